@@ -1,0 +1,102 @@
+"""The synthetic workloads: meshes, problem configurations and function-set parameters.
+
+1. manufactured p=1: [0,40000]^2 m, 20x20 quads -> 800 triangles, b = 2 m, g = 9.81,
+   ze = 0.1 sin(2 pi x/L) cos(2 pi y/L) cos(w t), function BC on all sides, SSP-RK2, dt = 1 s, 1000 steps
+2. manufactured p=2 at scale: 512x512 quads -> 524,288 triangles, interior nodes jittered by +-20% of the
+   cell size (seed 2), Dunavant degree 4 / 3-point Gauss-Legendre, SSP-RK3, 200 steps
+3. Thacker bowl with wetting/drying + slope limiter: +-4000 m, 256x256 quads -> 131,072 triangles,
+   h0 = 10 m, a = 3000 m, amplitude 2 m, p=1, SSP-RK2, h_o = 0.01 m, two periods
+4. learned troubled-cell indicator on bowl meshes with random Gaussian humps
+5. ensemble of p=1 members with random smooth bathymetry and wet/dry
+"""
+import math
+
+import numpy as np
+
+from . import meshgen
+from .types import (FN_GAUSSIAN_HUMPS, FN_MANUFACTURED_SINE, FN_THACKER_BOWL, FUNCTION, LAND, ProblemConfig)
+
+L_MMS = 40000.0
+
+
+def sine_params(L=L_MMS, A=0.1, H=2.0, g=9.81, w=0.0):
+    p = [0.0] * 16
+    p[0], p[1], p[2], p[3], p[4] = L, A, H, w, g
+    return p
+
+
+def manufactured(nq=20, p=1, rk=(2, 2), dt=1.0, jitter=0.0, seed=2, H=2.0, g=9.81, precision="fp64"):
+    mesh = meshgen.quad_mesh(nq, nq, corners=((0, 0), (L_MMS, 0), (L_MMS, L_MMS), (0, L_MMS)),
+                             bc=(FUNCTION,) * 4, jitter=jitter, seed=seed, bathymetry=meshgen.bath_flat(H),
+                             name="manufactured_%d" % nq)
+    cfg = ProblemConfig(p=p, rk_nstages=rk[0], rk_order=rk[1], dt=dt, g=g, function_source=True, ic_type=1,
+                        function_set=FN_MANUFACTURED_SINE, fn_params=sine_params(H=H, g=g), precision=precision)
+    return mesh, cfg
+
+
+def config1(precision="fp64"):
+    return manufactured(20, p=1, rk=(2, 2), dt=1.0, precision=precision)
+
+
+def config2(nq=512, precision="fp64"):
+    return manufactured(nq, p=2, rk=(3, 3), dt=1.0, jitter=0.2, seed=2, precision=precision)
+
+
+def thacker_params(h0=10.0, a=3000.0, eta0=2.0, g=9.81):
+    p = [0.0] * 16
+    p[0], p[1], p[2], p[3] = h0, a, eta0, g
+    return p
+
+
+def thacker_period(h0=10.0, a=3000.0, g=9.81):
+    return 2 * math.pi / (math.sqrt(8 * g * h0) / a)
+
+
+def config3(nq=256, dt=0.25, limiter=True, precision="fp64", extent=4000.0):
+    mesh = meshgen.quad_mesh(nq, nq, corners=((-extent, -extent), (extent, -extent), (extent, extent), (-extent, extent)),
+                             bc=(LAND,) * 4, bathymetry=meshgen.bath_thacker(10.0, 3000.0), name="bowl_%d" % nq)
+    cfg = ProblemConfig(p=1, rk_nstages=2, rk_order=2, dt=dt, g=9.81, wetting_drying=True, h_o=0.01,
+                        slope_limiting=limiter, sl_M=1.0e-8, sl_nu=1.5, ic_type=1, function_set=FN_THACKER_BOWL,
+                        fn_params=thacker_params(), precision=precision)
+    return mesh, cfg
+
+
+def humps_params(humps, ze0=0.0):
+    p = [0.0] * 16
+    p[0] = ze0
+    for i, (amp, xc, yc, w) in enumerate(humps[:3]):
+        p[1 + 4 * i], p[2 + 4 * i], p[3 + 4 * i], p[4 + 4 * i] = amp, xc, yc, w
+    return p
+
+
+def random_humps(rng, extent=2500.0, n=None):
+    n = n if n is not None else int(rng.integers(1, 4))
+    out = []
+    for _ in range(n):
+        r = rng.uniform(0, extent * 0.7)
+        th = rng.uniform(0, 2 * math.pi)
+        out.append((rng.uniform(0.5, 3.0), r * math.cos(th), r * math.sin(th), rng.uniform(200.0, 1500.0)))
+    return out
+
+
+def bowl_humps(nq=256, seed=0, dt=0.25, precision="fp64", extent=4000.0, limiter=True):
+    """Config-3 bowl bathymetry with random Gaussian humps on still water (config 4 training data)."""
+    rng = np.random.default_rng(seed)
+    mesh = meshgen.quad_mesh(nq, nq, corners=((-extent, -extent), (extent, -extent), (extent, extent), (-extent, extent)),
+                             bc=(LAND,) * 4, bathymetry=meshgen.bath_thacker(10.0, 3000.0), name="bowl_humps_%d" % nq)
+    cfg = ProblemConfig(p=1, rk_nstages=2, rk_order=2, dt=dt, g=9.81, wetting_drying=True, h_o=0.01,
+                        slope_limiting=limiter, sl_M=1.0e-8, sl_nu=1.5, ic_type=1, function_set=FN_GAUSSIAN_HUMPS,
+                        fn_params=humps_params(random_humps(rng)), precision=precision)
+    return mesh, cfg
+
+
+def ensemble_member(n, seed, extent=10000.0, dt=0.5, precision="fp32"):
+    rng = np.random.default_rng(seed)
+    bath = meshgen.bath_gaussians(seed, ((0, extent), (0, extent)))
+    mesh = meshgen.quad_mesh(n, n, corners=((0, 0), (extent, 0), (extent, extent), (0, extent)), bc=(LAND,) * 4,
+                             bathymetry=bath, name="member_%d" % seed)
+    hump = [(rng.uniform(0.5, 2.0), rng.uniform(0.3, 0.7) * extent, rng.uniform(0.3, 0.7) * extent,
+             rng.uniform(0.03, 0.1) * extent)]
+    cfg = ProblemConfig(p=1, rk_nstages=2, rk_order=2, dt=dt, g=9.81, wetting_drying=True, h_o=0.01, ic_type=1,
+                        function_set=FN_GAUSSIAN_HUMPS, fn_params=humps_params(hump), precision=precision)
+    return mesh, cfg

@@ -1,0 +1,129 @@
+"""Structured quadrilateral -> triangle mesh generator.
+
+Follows the reference's mesh_generators/quad_mesh_generator.cpp: a bilinear map of the index grid
+onto the quadrilateral (x1,y1)..(x4,y4) (:101-130), node numbering j*(m+1)+i, element patterns
+simple/zigzag/checker (:464-541), and four boundary node chains bottom, right, top, left (:144-160).
+Two additions the reference lacks: seeded jitter of interior nodes (uniform in +-frac of the local
+cell size, boundary nodes fixed) and a choice of bathymetry functions evaluated at the nodes.
+"""
+import numpy as np
+
+from .types import MeshArrays, LAND
+
+SIMPLE, ZIGZAG, CHECKER = 0, 1, 2
+
+
+def _triangles(m, n, pattern):
+    j, i = np.meshgrid(np.arange(n), np.arange(m), indexing="ij")
+    i = i.ravel()
+    j = j.ravel()
+    sw = i + (m + 1) * j
+    se = sw + 1
+    nw = i + m + 1 + (m + 1) * j
+    ne = i + m + 2 + (m + 1) * j
+    a = np.stack([sw, ne, nw], 1)  # element 2i + 2mj   (simple pattern)
+    b = np.stack([sw, se, ne], 1)  # element 2i + 2mj + 1
+    if pattern == SIMPLE:
+        alt = np.zeros_like(i, bool)
+    elif pattern == ZIGZAG:
+        alt = (j % 2) == 1
+    elif pattern == CHECKER:
+        alt = ((i + j) % 2) == 1
+    else:
+        raise ValueError("unknown pattern")
+    a2 = np.stack([sw, se, nw], 1)
+    b2 = np.stack([se, ne, nw], 1)
+    a = np.where(alt[:, None], a2, a)
+    b = np.where(alt[:, None], b2, b)
+    tri = np.empty((2 * m * n, 3), np.int32)
+    idx = 2 * i + 2 * m * j
+    tri[idx] = a
+    tri[idx + 1] = b
+    return tri
+
+
+def bath_flat(depth):
+    return lambda x, y: np.full_like(x, depth)
+
+
+def bath_thacker(h0, a, xc=0.0, yc=0.0):
+    return lambda x, y: h0 * (1.0 - ((x - xc) ** 2 + (y - yc) ** 2) / (a * a))
+
+
+def bath_gaussians(seed, extent, n=8, dmin=1.0, dmax=20.0):
+    """Sum of n seeded Gaussians scaled to depths in [dmin, dmax]."""
+    rng = np.random.default_rng(seed)
+    (x0, x1), (y0, y1) = extent
+    cx = rng.uniform(x0, x1, n)
+    cy = rng.uniform(y0, y1, n)
+    s = rng.uniform(0.1, 0.3, n) * max(x1 - x0, y1 - y0)
+    amp = rng.uniform(0.2, 1.0, n)
+
+    def f(x, y):
+        acc = np.zeros_like(x)
+        for k in range(n):
+            acc += amp[k] * np.exp(-((x - cx[k]) ** 2 + (y - cy[k]) ** 2) / (2 * s[k] ** 2))
+        return dmin + (dmax - dmin) * acc / amp.sum()
+
+    return f
+
+
+def quad_mesh(m, n, corners=((0, 0), (1, 0), (1, 1), (0, 1)), bc=(LAND, LAND, LAND, LAND), pattern=SIMPLE,
+              jitter=0.0, seed=0, bathymetry=None, name="quadrilateral"):
+    """m x n quads -> 2mn triangles. corners = (x1,y1),(x2,y2),(x3,y3),(x4,y4) counter-clockwise.
+    bc = boundary types of the chains bottom (1-2), right (2-3), top (4-3), left (1-4)."""
+    (x1, y1), (x2, y2), (x3, y3), (x4, y4) = corners
+    i = np.arange(m + 1)
+    j = np.arange(n + 1)
+    J, I = np.meshgrid(j, i, indexing="ij")
+    xi = -1.0 + (2.0 / m) * I
+    eta = -1.0 + (2.0 / n) * J
+    N1 = (1.0 - xi) * (1.0 - eta) / 4.0
+    N2 = (1.0 + xi) * (1.0 - eta) / 4.0
+    N3 = (1.0 + xi) * (1.0 + eta) / 4.0
+    N4 = (1.0 - xi) * (1.0 + eta) / 4.0
+    x = x1 * N1 + x2 * N2 + x3 * N3 + x4 * N4
+    y = y1 * N1 + y2 * N2 + y3 * N3 + y4 * N4
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        hx = np.hypot(x2 - x1, y2 - y1) / m
+        hy = np.hypot(x4 - x1, y4 - y1) / n
+        dx = rng.uniform(-jitter * hx, jitter * hx, x.shape)
+        dy = rng.uniform(-jitter * hy, jitter * hy, y.shape)
+        interior = (I > 0) & (I < m) & (J > 0) & (J < n)
+        x = np.where(interior, x + dx, x)
+        y = np.where(interior, y + dy, y)
+    x = x.ravel()
+    y = y.ravel()
+    z = bathymetry(x, y) if bathymetry is not None else np.zeros_like(x)
+    nodes = np.stack([x, y, z], 1).astype(np.float64)
+    tri = _triangles(m, n, pattern)
+    chains = [np.arange(m + 1), m + np.arange(n + 1) * (m + 1), np.arange(m + 1) + (m + 1) * n, np.arange(n + 1) * (m + 1)]
+    seg_type = np.array(bc, np.int32)
+    seg_offsets = np.concatenate([[0], np.cumsum([len(c) for c in chains])]).astype(np.int64)
+    seg_nodes = np.concatenate(chains).astype(np.int32)
+    return MeshArrays(nodes, tri, seg_type, seg_offsets, seg_nodes, None, name)
+
+
+def write_adcirc(mesh, path):
+    """Write the mesh as ADCIRC fort.14 (+ nothing for .bcis: land/function/outflow need no data).
+    Boundary chains become land-boundary segments with IBTYPE 0 (land), 77 (function), 88 (outflow)."""
+    ib = {0: 0, 3: 77, 4: 88}
+    with open(path, "w") as f:
+        f.write(mesh.name + "\n")
+        f.write("%d    %d\n" % (mesh.n_elems, mesh.n_nodes))
+        for k, (x, y, z) in enumerate(mesh.node_xyz):
+            f.write("%d %.17g %.17g %.17g\n" % (k, x, y, z))
+        ids = mesh.elem_ids if mesh.elem_ids is not None else np.arange(mesh.n_elems)
+        for k, (a, b, c) in enumerate(mesh.elem_nodes):
+            f.write("%d 3 %d %d %d\n" % (ids[k], a, b, c))
+        f.write("0 = Number of open boundaries\n0 = Total number of open boundary nodes\n")
+        nseg = len(mesh.seg_type)
+        f.write("%d = Number of land boundaries\n" % nseg)
+        f.write("%d = Total number of land boundary nodes\n" % int(mesh.seg_offsets[-1]))
+        for s in range(nseg):
+            chain = mesh.seg_nodes[mesh.seg_offsets[s]:mesh.seg_offsets[s + 1]]
+            f.write("%d %d = Number of nodes for land boundary %d\n" % (len(chain), ib[int(mesh.seg_type[s])], s + 1))
+            for nd in chain:
+                f.write("%d\n" % nd)
+        f.write("0 = Number of generic boundaries\n0 = Total number of generic boundary nodes\n")
