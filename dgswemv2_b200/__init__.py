@@ -1,0 +1,204 @@
+"""B200-native RKDG shallow-water step with dgswemv2's problem/stepper interface.
+
+Python host side of the drop-in. `Problem` wraps one library handle and exposes the reference's
+SWE::RKDG::Problem / Serial::Simulation operations (preprocessor_serial, step_serial, stage_serial,
+compute_residual_L2); all arithmetic runs in libdgsw_rkdg.so on the GPU.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import DGSW_FP32, DGSW_FP64, DgswError  # noqa: F401
+from .types import MeshArrays, ProblemConfig  # noqa: F401
+
+__all__ = ["Problem", "ProblemConfig", "MeshArrays", "DgswError", "mesh_topology"]
+
+
+def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True):
+    lib = _lib.load()
+    c = _lib.Config()
+    lib.dgsw_config_default(C.byref(c))
+    c.p = cfg.p
+    c.rk_nstages = cfg.rk_nstages
+    c.rk_order = cfg.rk_order
+    c.dt = cfg.dt
+    c.g = cfg.g
+    c.wetting_drying = int(cfg.wetting_drying)
+    c.h_o = cfg.h_o
+    c.slope_limiting = int(cfg.slope_limiting)
+    c.sl_M = cfg.sl_M
+    c.sl_nu = cfg.sl_nu
+    c.function_source = int(cfg.function_source)
+    c.ic_type = cfg.ic_type
+    for i in range(3):
+        c.ic_const[i] = cfg.ic_const[i]
+    c.function_set = cfg.function_set
+    for i, v in enumerate(list(cfg.fn_params)[:16]):
+        c.fn_params[i] = v
+    c.spherical = int(cfg.spherical)
+    c.sp_lat0_deg = cfg.sp_lat0_deg
+    c.sp_R = cfg.sp_R
+    c.precision = DGSW_FP32 if cfg.precision == "fp32" else DGSW_FP64
+    c.device = device
+    c.tile = tile
+    c.renumber = int(renumber)
+    c.use_graphs = int(use_graphs)
+    return c
+
+
+def _mesh_struct(mesh):
+    keep = [
+        np.ascontiguousarray(mesh.node_xyz, np.float64),
+        np.ascontiguousarray(mesh.elem_nodes, np.int32),
+        None if mesh.elem_ids is None else np.ascontiguousarray(mesh.elem_ids, np.uint32),
+        np.ascontiguousarray(mesh.seg_type, np.int32),
+        np.ascontiguousarray(mesh.seg_offsets, np.int64),
+        np.ascontiguousarray(mesh.seg_nodes, np.int32),
+    ]
+    m = _lib.Mesh()
+    m.n_nodes = keep[0].shape[0]
+    m.node_xyz = _lib.ptr(keep[0], C.c_double)
+    m.n_elems = keep[1].shape[0]
+    m.elem_nodes = _lib.ptr(keep[1], C.c_int32)
+    m.elem_ids = _lib.ptr(keep[2], C.c_uint32)
+    m.n_segments = keep[3].shape[0]
+    m.seg_type = _lib.ptr(keep[3], C.c_int32)
+    m.seg_offsets = _lib.ptr(keep[4], C.c_int64)
+    m.seg_nodes = _lib.ptr(keep[5], C.c_int32)
+    return m, keep
+
+
+def mesh_topology(mesh):
+    """Host-only topology (MeshMetaData + interface/boundary creation), in ascending element-ID order:
+    neighbours, boundary type per face, interfaces (in, ex, face_in, face_ex), boundaries (elem, face, type)."""
+    lib = _lib.load()
+    m, keep = _mesh_struct(mesh)
+    ni, nb = C.c_int64(), C.c_int64()
+    _lib.check(lib.dgsw_mesh_topology(C.byref(m), None, None, C.byref(ni), None, C.byref(nb), None))
+    ne = mesh.n_elems
+    nbr = np.empty((ne, 3), np.int32)
+    bt = np.empty((ne, 3), np.uint8)
+    intf = np.empty((ni.value, 4), np.int32)
+    bnd = np.empty((nb.value, 3), np.int32)
+    _lib.check(lib.dgsw_mesh_topology(C.byref(m), _lib.ptr(nbr, C.c_int32), _lib.ptr(bt, C.c_uint8), C.byref(ni),
+                                      _lib.ptr(intf, C.c_int32), C.byref(nb), _lib.ptr(bnd, C.c_int32)))
+    return nbr, bt, intf, bnd
+
+
+class Problem:
+    """One RKDG problem on one GPU (SWE::RKDG::Problem + Serial::Simulation, rkdg_swe_problem.hpp:34-194,
+    simulation.hpp:14-93)."""
+
+    def __init__(self, cfg, mesh, device=0, tile=0, renumber=True, use_graphs=True, init=True):
+        lib = _lib.load()
+        self.cfg = cfg
+        self._c = _make_config(cfg, device, tile, renumber, use_graphs)
+        m, self._keep = _mesh_struct(mesh)
+        h = C.c_void_p()
+        _lib.check(lib.dgsw_rkdg_create(C.byref(self._c), C.byref(m), C.byref(h)))
+        self._h = h
+        self.info = _lib.Info()
+        _lib.check(lib.dgsw_rkdg_info(h, C.byref(self.info)))
+        self.ne = self.info.n_elems
+        self.nd = self.info.ndof
+        if init:
+            self.preprocessor_serial()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().dgsw_rkdg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # reference interface ---------------------------------------------------------------------
+    def preprocessor_serial(self):
+        """Problem::preprocessor_serial: initial projections, wet/dry and limiter initialisation."""
+        _lib.check(_lib.load().dgsw_rkdg_init_state(self._h))
+
+    def step_serial(self, nsteps=1):
+        """Problem::step_serial, nsteps times."""
+        _lib.check(_lib.load().dgsw_rkdg_step(self._h, int(nsteps)))
+
+    def stage_serial(self):
+        """Problem::stage_serial: one RK stage."""
+        _lib.check(_lib.load().dgsw_rkdg_stage(self._h))
+
+    def compute_residual_L2(self):
+        """Simulation::ComputeL2Residual: sqrt of the summed per-element squared L2 error."""
+        out = C.c_double()
+        _lib.check(_lib.load().dgsw_rkdg_l2_error(self._h, C.byref(out)))
+        return out.value
+
+    # state access ----------------------------------------------------------------------------
+    def get_state(self):
+        q = np.empty((self.ne, 3, self.nd), np.float64)
+        _lib.check(_lib.load().dgsw_rkdg_get_state(self._h, _lib.ptr(q, C.c_double)))
+        return q
+
+    def set_state(self, q):
+        q = np.ascontiguousarray(q, np.float64)
+        assert q.shape == (self.ne, 3, self.nd)
+        _lib.check(_lib.load().dgsw_rkdg_set_state(self._h, _lib.ptr(q, C.c_double)))
+
+    def get_wet(self):
+        w = np.empty(self.ne, np.uint8)
+        _lib.check(_lib.load().dgsw_rkdg_get_wet(self._h, _lib.ptr(w, C.c_uint8)))
+        return w
+
+    def set_wet(self, w):
+        w = np.ascontiguousarray(w, np.uint8)
+        _lib.check(_lib.load().dgsw_rkdg_set_wet(self._h, _lib.ptr(w, C.c_uint8)))
+
+    def get_limited(self):
+        w = np.empty(self.ne, np.uint8)
+        _lib.check(_lib.load().dgsw_rkdg_get_limited(self._h, _lib.ptr(w, C.c_uint8)))
+        return w
+
+    def set_state_device(self, dptr):
+        _lib.check(_lib.load().dgsw_rkdg_set_state_device(self._h, C.c_void_p(dptr)))
+
+    def get_state_device(self, dptr):
+        _lib.check(_lib.load().dgsw_rkdg_get_state_device(self._h, C.c_void_p(dptr)))
+
+    def time(self):
+        t = C.c_double()
+        st = C.c_int64()
+        sg = C.c_int32()
+        _lib.check(_lib.load().dgsw_rkdg_get_time(self._h, C.byref(t), C.byref(st), C.byref(sg)))
+        return t.value, st.value, sg.value
+
+    def mass(self):
+        out = C.c_double()
+        _lib.check(_lib.load().dgsw_rkdg_mass(self._h, C.byref(out)))
+        return out.value
+
+    def topology(self):
+        lib = _lib.load()
+        ni, nb = C.c_int64(), C.c_int64()
+        _lib.check(lib.dgsw_rkdg_topology(self._h, None, None, C.byref(ni), None, C.byref(nb), None))
+        nbr = np.empty((self.ne, 3), np.int32)
+        bt = np.empty((self.ne, 3), np.uint8)
+        intf = np.empty((ni.value, 4), np.int32)
+        bnd = np.empty((nb.value, 3), np.int32)
+        _lib.check(lib.dgsw_rkdg_topology(self._h, _lib.ptr(nbr, C.c_int32), _lib.ptr(bt, C.c_uint8), C.byref(ni),
+                                          _lib.ptr(intf, C.c_int32), C.byref(nb), _lib.ptr(bnd, C.c_int32)))
+        return nbr, bt, intf, bnd
+
+    def synchronize(self):
+        _lib.check(_lib.load().dgsw_rkdg_synchronize(self._h))
+
+    def last_step_timing(self):
+        ms = C.c_double()
+        n = C.c_int64()
+        _lib.check(_lib.load().dgsw_rkdg_last_step_timing(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value

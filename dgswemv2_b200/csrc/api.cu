@@ -1,0 +1,908 @@
+// C ABI of the RKDG library: handle lifecycle, uploads, the stage/step driver and reductions.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dgsw_rkdg.h"
+#include "host_setup.h"
+#include "limiter_kernel.cuh"
+#include "quadrature.h"
+#include "reduce_kernels.cuh"
+#include "stage_kernel.cuh"
+
+using namespace dgsw;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(call)                                                                                     \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess)                                                                             \
+            return fail(DGSW_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+    } while (0)
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        n = count;
+        return cudaMalloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// host copies of the per-order tables in both precisions
+int make_dev_tables(int p, DevTables<double>& d, DevTables<float>& f, std::string& err) {
+    Tables t;
+    int rc = build_tables(p, t, err);
+    if (rc) return rc;
+    std::memset(&d, 0, sizeof(d));
+    std::memset(&f, 0, sizeof(f));
+    for (int k = 0; k < t.nd; ++k)
+        for (int gp = 0; gp < t.nq; ++gp) {
+            d.phi[k * t.nq + gp] = t.phi[k * t.nq + gp];
+            d.dphi[0][k * t.nq + gp] = t.dphi[0][k * t.nq + gp];
+            d.dphi[1][k * t.nq + gp] = t.dphi[1][k * t.nq + gp];
+            d.mz[0][gp * t.nd + k] = t.mz[0][gp * t.nd + k];
+            d.mz[1][gp * t.nd + k] = t.mz[1][gp * t.nd + k];
+            d.phiw[gp * t.nd + k] = t.phiw[gp * t.nd + k];
+        }
+    for (int n = 0; n < 3; ++n)
+        for (int gp = 0; gp < t.nq; ++gp) d.psi[n][gp] = t.psi[n][gp];
+    for (int fc = 0; fc < 3; ++fc) {
+        for (int i = 0; i < t.nd * t.ng; ++i) d.fphi[fc][i] = t.fphi[fc][i];
+        for (int n = 0; n < 3; ++n)
+            for (int g = 0; g < t.ng; ++g) d.fpsi[fc][n][g] = t.fpsi[fc][n][g];
+    }
+    for (int g = 0; g < t.ng; ++g) d.gw[g] = t.gw[g];
+    for (int k = 0; k < t.nd; ++k) d.minv[k] = t.minv[k];
+    for (int i = 0; i < 36; ++i) {
+        f.phi[i] = (float)d.phi[i];
+        f.dphi[0][i] = (float)d.dphi[0][i];
+        f.dphi[1][i] = (float)d.dphi[1][i];
+        f.mz[0][i] = (float)d.mz[0][i];
+        f.mz[1][i] = (float)d.mz[1][i];
+        f.phiw[i] = (float)d.phiw[i];
+    }
+    std::memcpy(f.psi, d.psi, sizeof(d.psi));
+    std::memcpy(f.fpsi, d.fpsi, sizeof(d.fpsi));
+    for (int fc = 0; fc < 3; ++fc)
+        for (int i = 0; i < 18; ++i) f.fphi[fc][i] = (float)d.fphi[fc][i];
+    for (int g = 0; g < 3; ++g) f.gw[g] = (float)d.gw[g];
+    std::memcpy(f.minv, d.minv, sizeof(d.minv));
+    return DGSW_OK;
+}
+
+int make_l2_rule(L2Rule& R, std::string& err) {
+    Rule2D r = triangle_rule(20);
+    if ((int)r.w.size() != L2_NPT) {
+        err = "unexpected L2 rule size";
+        return DGSW_ERR_UNSUPPORTED;
+    }
+    std::memset(&R, 0, sizeof(R));
+    for (int i = 0; i < L2_NPT; ++i) {
+        R.w[i] = r.w[i];
+        R.psi[0][i] = -(r.z1[i] + r.z2[i]) / 2;
+        R.psi[1][i] = (1 + r.z1[i]) / 2;
+        R.psi[2][i] = (1 + r.z2[i]) / 2;
+    }
+    eval_basis(1, r.z1.data(), r.z2.data(), L2_NPT, R.phi[0]);
+    eval_basis(2, r.z1.data(), r.z2.data(), L2_NPT, R.phi[1]);
+    return DGSW_OK;
+}
+
+__global__ void advance_clock_kernel(DevClock* c, double dt) {
+    c->t += dt;  // ESSPRKStepper::operator++ (explicit_ssp_rk_stepper.hpp:55-58)
+    c->step += 1;
+}
+
+}  // namespace
+
+struct dgsw_rkdg_s {
+    dgsw_config cfg;
+    Tables tb;
+    Topology topo;
+    Tiling tiling;
+    dgsw_rk_table rk;
+    int device = 0;
+    int ns = 0, nd = 0;
+    int64_t ne = 0, ne_pad = 0, nn = 0;
+    bool fp32 = false;
+    double h_o_thr = 1.0e-6;
+    std::vector<double> node_xyz;
+    std::vector<bool> need_sol;  // sol_k kept for later stages
+    // device buffers
+    size_t real_size = 8;
+    std::vector<void*> Q;    // ns+1 stage states
+    std::vector<void*> SOL;  // stored stage solutions (only where needed)
+    void* bath = nullptr;
+    DBuf<int> enodes, tile_edge_off, ref_of_dev;
+    DBuf<int2> eslot;
+    DBuf<int4> edges;
+    DBuf<double2> xy;
+    DBuf<double> nz;
+    DBuf<unsigned char> wet[2];
+    int wet_cur = 0;
+    DBuf<DevStatus> status;
+    DBuf<DevClock> clock;
+    DBuf<double> red;  // reduction partials
+    DBuf<unsigned char> limited;
+    DBuf<int> nbr;     // neighbours per face, device order (limiter)
+    DBuf<double> baryctr;  // barycentre values of the newest state (limiter)
+    int64_t device_bytes = 0;
+    // stepper mirror on the host (ESSPRKStepper state)
+    double t = 0.0;
+    int64_t step = 0;
+    int stage = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    int qswap = 0;  // parity of the q_0 <-> q_ns swaps so far
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevTables<double> tab_d;
+    DevTables<float> tab_f;
+    DBuf<L2Rule> l2rule;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    size_t smem_bytes = 0;
+    int tile = 256;
+};
+
+namespace {
+
+template <typename Real>
+void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
+    std::memset(&A, 0, sizeof(A));
+    int n = 0;
+    for (int k = 0; k < s; ++k) {
+        if (h->rk.ark[s][k] != 0.0 || h->rk.brk[s][k] != 0.0) {
+            A.qk[n] = (const Real*)h->Q[k];
+            A.solk[n] = (const Real*)h->SOL[k];
+            A.a[n] = h->rk.ark[s][k];
+            A.bdt[n] = h->cfg.dt * h->rk.brk[s][k];
+            ++n;
+        }
+    }
+    A.qk[n] = (const Real*)h->Q[s];
+    A.solk[n] = nullptr;
+    A.a[n] = h->rk.ark[s][s];
+    A.bdt[n] = h->cfg.dt * h->rk.brk[s][s];
+    ++n;
+    A.nterms = n;
+    A.store_sol = h->need_sol[s] ? 1 : 0;
+    A.sol_out = (Real*)h->SOL[s];
+    A.q_out = (Real*)h->Q[s + 1];
+    A.bath = (const Real*)h->bath;
+    A.enodes = h->enodes.p;
+    A.eslot = h->eslot.p;
+    A.edges = h->edges.p;
+    A.tile_edge_off = h->tile_edge_off.p;
+    A.xy = h->xy.p;
+    A.nz = h->nz.p;
+    A.ref_of_dev = h->ref_of_dev.p;
+    A.baryctr = h->cfg.slope_limiting ? h->baryctr.p : nullptr;
+    A.status = h->status.p;
+    A.clock = h->clock.p;
+    A.drk_s = h->cfg.dt * h->rk.drk[s];
+    A.ne = (int)h->ne;
+    A.ne_pad = (int)h->ne_pad;
+    A.g = h->cfg.g;
+    A.h_o = h->cfg.h_o;
+    A.h_o_thr = h->h_o_thr;
+    A.fn_set = h->cfg.function_set;
+    for (int i = 0; i < 16; ++i) A.fn_params[i] = h->cfg.fn_params[i];
+    A.spherical = h->cfg.spherical;
+    A.sp_cos_lat0 = std::cos(h->cfg.sp_lat0_deg * M_PI / 180.0);
+    A.sp_R = h->cfg.sp_R;
+}
+
+void set_tables(dgsw_rkdg_s* h, StageArgs<double>& A) { A.T = h->tab_d; }
+void set_tables(dgsw_rkdg_s* h, StageArgs<float>& A) { A.T = h->tab_f; }
+
+cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, bool wd, bool fs) {
+    const int nt = (int)h->tiling.ntiles, me = h->tiling.max_edges;
+    return h->cfg.p == 1 ? launch_stage_p1_f64(A, h->tile, nt, me, wd, fs, h->stream)
+                         : launch_stage_p2_f64(A, h->tile, nt, me, wd, fs, h->stream);
+}
+cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<float>& A, bool wd, bool fs) {
+    const int nt = (int)h->tiling.ntiles, me = h->tiling.max_edges;
+    return h->cfg.p == 1 ? launch_stage_p1_f32(A, h->tile, nt, me, wd, fs, h->stream)
+                         : launch_stage_p2_f32(A, h->tile, nt, me, wd, fs, h->stream);
+}
+
+template <typename Real>
+cudaError_t launch_stage(dgsw_rkdg_s* h, int s) {
+    StageArgs<Real> A;
+    fill_stage_args<Real>(h, s, A);
+    set_tables(h, A);
+    A.wet_in = h->wet[h->wet_cur].p;
+    A.wet_out = h->wet[1 - h->wet_cur].p;
+    return launch_stage_any(h, A, h->cfg.wetting_drying != 0, h->cfg.function_source != 0);
+}
+
+template <typename Real>
+cudaError_t launch_limiter(dgsw_rkdg_s* h, int s_out) {
+    LimiterArgs<Real> L;
+    std::memset(&L, 0, sizeof(L));
+    L.q = (Real*)h->Q[s_out];
+    L.baryctr = h->baryctr.p;
+    L.wet = h->wet[h->wet_cur].p;
+    L.nbr = h->nbr.p;
+    L.enodes = h->enodes.p;
+    L.xy = h->xy.p;
+    L.nz = h->nz.p;
+    L.limited = h->limited.p;
+    L.ne = (int)h->ne;
+    L.ne_pad = (int)h->ne_pad;
+    L.g = h->cfg.g;
+    L.M = h->cfg.sl_M;
+    L.nu = h->cfg.sl_nu;
+    L.status = h->status.p;
+    L.ref_of_dev = h->ref_of_dev.p;
+    return launch_limiter_kernel<Real>(L, h->cfg.p, h->stream);
+}
+
+// one RK stage: stage kernel, (clock on the last stage), limiter, wet flag buffer flip
+cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches) {
+    cudaError_t e = h->fp32 ? launch_stage<float>(h, s) : launch_stage<double>(h, s);
+    if (e != cudaSuccess) return e;
+    ++launches;
+    h->wet_cur = 1 - h->wet_cur;
+    int s_out = s + 1;
+    if (s + 1 == h->ns) {
+        advance_clock_kernel<<<1, 1, 0, h->stream>>>(h->clock.p, h->cfg.dt);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        std::swap(h->Q[0], h->Q[h->ns]);  // UpdateState's swap of q_0 and q_ns
+        h->qswap ^= 1;
+        s_out = 0;
+    }
+    if (h->cfg.slope_limiting) {
+        e = h->fp32 ? launch_limiter<float>(h, s_out) : launch_limiter<double>(h, s_out);
+        if (e != cudaSuccess) return e;
+        ++launches;
+    }
+    return cudaSuccess;
+}
+
+void advance_host_stepper(dgsw_rkdg_s* h) {
+    h->stage = (h->stage + 1) % h->ns;
+    if (h->stage == 0) {
+        h->t += h->cfg.dt;
+        h->step += 1;
+    }
+}
+
+int check_status(dgsw_rkdg_s* h) {
+    DevStatus st;
+    CUDA_TRY(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (st.nan_flag) {
+        uint32_t id = st.nan_ref_elem < h->topo.ids.size() ? h->topo.ids[st.nan_ref_elem] : 0;
+        DevStatus z;
+        std::memset(&z, 0, sizeof(z));
+        z.nan_ref_elem = 0xffffffffu;
+        cudaMemcpyAsync(h->status.p, &z, sizeof(z), cudaMemcpyHostToDevice, h->stream);
+        return fail(DGSW_ERR_NAN, "Fatal Error: NaN found at element " + std::to_string(id));
+    }
+    return DGSW_OK;
+}
+
+void destroy_graphs(dgsw_rkdg_s* h) {
+    for (int i = 0; i < 4; ++i)
+        if (h->graph[i]) {
+            cudaGraphExecDestroy(h->graph[i]);
+            h->graph[i] = nullptr;
+        }
+}
+
+// element-major host state [ref][var][dof] <-> device component-major SoA in device order
+template <typename Real>
+void host_to_dev_layout(dgsw_rkdg_s* h, const double* q, std::vector<Real>& out) {
+    const int nd = h->nd;
+    out.assign((size_t)3 * nd * h->ne_pad, Real(0));
+    for (int64_t d = 0; d < h->ne; ++d) {
+        int64_t r = h->tiling.ref_of_dev[d];
+        for (int c = 0; c < 3 * nd; ++c) out[(size_t)c * h->ne_pad + d] = (Real)q[r * 3 * nd + c];
+    }
+}
+
+template <typename Real>
+void dev_to_host_layout(dgsw_rkdg_s* h, const std::vector<Real>& in, double* q) {
+    const int nd = h->nd;
+    for (int64_t d = 0; d < h->ne; ++d) {
+        int64_t r = h->tiling.ref_of_dev[d];
+        for (int c = 0; c < 3 * nd; ++c) q[r * 3 * nd + c] = (double)in[(size_t)c * h->ne_pad + d];
+    }
+}
+
+int upload_state(dgsw_rkdg_s* h, const double* q) {
+    const size_t n = (size_t)3 * h->nd * h->ne_pad;
+    if (h->fp32) {
+        std::vector<float> buf;
+        host_to_dev_layout<float>(h, q, buf);
+        CUDA_TRY(cudaMemcpyAsync(h->Q[h->stage], buf.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    } else {
+        std::vector<double> buf;
+        host_to_dev_layout<double>(h, q, buf);
+        CUDA_TRY(cudaMemcpyAsync(h->Q[h->stage], buf.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    return DGSW_OK;
+}
+
+int upload_wet(dgsw_rkdg_s* h, const uint8_t* wet_ref) {
+    std::vector<unsigned char> w(h->ne_pad, 0);
+    for (int64_t d = 0; d < h->ne; ++d) w[d] = wet_ref[h->tiling.ref_of_dev[d]] ? 1 : 0;
+    CUDA_TRY(cudaMemcpyAsync(h->wet[h->wet_cur].p, w.data(), h->ne_pad, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DGSW_OK;
+}
+
+template <typename Real>
+int run_reduction(dgsw_rkdg_s* h, int what, double* out) {
+    ReduceArgs<Real> R;
+    std::memset(&R, 0, sizeof(R));
+    // the L2 error reads state[0] (swe_post_comp_res_l2.hpp:12), the mass the current stage state
+    R.q = (const Real*)h->Q[what == 0 ? 0 : h->stage];
+    R.bath = (const Real*)h->bath;
+    R.enodes = h->enodes.p;
+    R.xy = h->xy.p;
+    R.ne = (int)h->ne;
+    R.ne_pad = (int)h->ne_pad;
+    R.t = h->t + h->cfg.dt * h->rk.drk[h->stage];
+    R.fn_set = h->cfg.function_set;
+    for (int i = 0; i < 16; ++i) R.fn_params[i] = h->cfg.fn_params[i];
+    R.partial = h->red.p;
+    R.rule = h->l2rule.p;
+    R.npartial = (int)h->red.n;
+    cudaError_t e = launch_reduction<Real>(R, h->cfg.p, what, h->stream);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("reduction: ") + cudaGetErrorString(e));
+    std::vector<double> part(h->red.n);
+    CUDA_TRY(cudaMemcpyAsync(part.data(), h->red.p, h->red.n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    double s = 0.0;
+    for (double v : part) s += v;  // fixed order: deterministic
+    *out = s;
+    return DGSW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t dgsw_abi_version(void) { return DGSW_ABI_VERSION; }
+
+const char* dgsw_last_error(void) { return g_last_error.c_str(); }
+
+const char* dgsw_status_string(int32_t s) {
+    switch (s) {
+        case DGSW_OK:
+            return "ok";
+        case DGSW_ERR_INVALID_ARGUMENT:
+            return "invalid argument";
+        case DGSW_ERR_MESH:
+            return "mesh error";
+        case DGSW_ERR_CUDA:
+            return "CUDA error";
+        case DGSW_ERR_NAN:
+            return "NaN in solution";
+        case DGSW_ERR_UNSUPPORTED:
+            return "unsupported";
+        case DGSW_ERR_NO_DEVICE:
+            return "no CUDA device";
+        case DGSW_ERR_IO:
+            return "I/O error";
+        default:
+            return "unknown status";
+    }
+}
+
+void dgsw_config_default(dgsw_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->p = 1;
+    c->rk_nstages = 2;
+    c->rk_order = 2;
+    c->dt = 1.0;
+    c->g = 9.81;
+    c->h_o = 0.1;
+    c->sl_M = 1.0e-8;
+    c->sl_nu = 1.5;
+    c->sp_R = 6378200.0;
+    c->precision = DGSW_FP64;
+    c->tile = 0;
+    c->renumber = 1;
+    c->use_graphs = 1;
+}
+
+int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_handle* out) {
+    if (!cfg || !mesh || !out) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(DGSW_ERR_NO_DEVICE, "no CUDA device available");
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(DGSW_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    if (!(cfg->dt > 0)) return fail(DGSW_ERR_INVALID_ARGUMENT, "dt must be positive");
+    if (cfg->precision != DGSW_FP64 && cfg->precision != DGSW_FP32)
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "precision must be DGSW_FP64 or DGSW_FP32");
+    if (cfg->function_set < 0 || cfg->function_set >= DGSW_FN_COUNT)
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "unknown function set");
+    auto* h = new dgsw_rkdg_s();
+    h->cfg = *cfg;
+    h->device = cfg->device;
+    std::string err;
+    int rc = build_tables(cfg->p, h->tb, err);
+    if (rc) {
+        delete h;
+        return fail(rc, err);
+    }
+    if (dgsw_rk_table_init(cfg->rk_nstages, cfg->rk_order, &h->rk) != 0) {
+        delete h;
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "Fatal Error: invalid Runge-Kutta method entered!");
+    }
+    h->ns = cfg->rk_nstages;
+    h->nd = h->tb.nd;
+    rc = build_topology(mesh, h->topo, err);
+    if (rc) {
+        delete h;
+        return fail(rc, err);
+    }
+    h->ne = h->topo.ne;
+    h->nn = mesh->n_nodes;
+    h->ne_pad = (h->ne + 31) / 32 * 32;
+    h->fp32 = cfg->precision == DGSW_FP32;
+    h->real_size = h->fp32 ? sizeof(float) : sizeof(double);
+    if (cfg->wetting_drying) h->h_o_thr = 1.0e6 * cfg->h_o * std::numeric_limits<double>::epsilon();
+    h->node_xyz.assign(mesh->node_xyz, mesh->node_xyz + 3 * mesh->n_nodes);
+    int tile = cfg->tile;
+    if (tile == 0) tile = (cfg->p == 1) ? 256 : 128;
+    if (tile != 128 && tile != 256) {
+        delete h;
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "tile must be 0 (automatic), 128 or 256");
+    }
+    h->tile = tile;
+    rc = build_tiling(h->topo, h->node_xyz.data(), tile, cfg->renumber != 0, h->tiling, err);
+    if (rc) {
+        delete h;
+        return fail(rc, err);
+    }
+    // which stage solutions are read by later stages (off-diagonal brk)
+    h->need_sol.assign(h->ns, false);
+    for (int i = 0; i < h->ns; ++i)
+        for (int k = 0; k < i; ++k)
+            if (h->rk.brk[i][k] != 0.0) h->need_sol[k] = true;
+
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(DGSW_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+    rc = make_dev_tables(cfg->p, h->tab_d, h->tab_f, err);
+    if (rc) {
+        delete h;
+        return fail(rc, err);
+    }
+    auto cleanup_fail = [&](const std::string& what, cudaError_t ce) {
+        dgsw_rkdg_destroy(h);
+        return fail(DGSW_ERR_CUDA, what + ": " + cudaGetErrorString(ce));
+    };
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cleanup_fail("stream", e);
+    h->own_stream = true;
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    const size_t state_bytes = (size_t)3 * h->nd * h->ne_pad * h->real_size;
+    h->Q.assign(h->ns + 1, nullptr);
+    h->SOL.assign(h->ns, nullptr);
+    for (int s = 0; s <= h->ns; ++s) {
+        if ((e = cudaMalloc(&h->Q[s], state_bytes)) != cudaSuccess) return cleanup_fail("state alloc", e);
+        cudaMemset(h->Q[s], 0, state_bytes);
+        h->device_bytes += state_bytes;
+    }
+    for (int s = 0; s < h->ns; ++s)
+        if (h->need_sol[s]) {
+            if ((e = cudaMalloc(&h->SOL[s], state_bytes)) != cudaSuccess) return cleanup_fail("sol alloc", e);
+            h->device_bytes += state_bytes;
+        }
+    const size_t bath_bytes = (size_t)h->nd * h->ne_pad * h->real_size;
+    if ((e = cudaMalloc(&h->bath, bath_bytes)) != cudaSuccess) return cleanup_fail("bath alloc", e);
+    h->device_bytes += bath_bytes;
+    // static mesh data in device order
+    {
+        std::vector<int> en((size_t)3 * h->ne_pad, 0);
+        std::vector<double> bathm;
+        project_bathymetry(h->topo, h->node_xyz.data(), h->tb, bathm);
+        std::vector<double> bdev((size_t)h->nd * h->ne_pad, 0.0);
+        std::vector<int> nb((size_t)3 * h->ne_pad, -1);
+        for (int64_t d = 0; d < h->ne; ++d) {
+            int64_t r = h->tiling.ref_of_dev[d];
+            for (int v = 0; v < 3; ++v) {
+                en[(size_t)v * h->ne_pad + d] = h->topo.enodes[3 * r + v];
+                int32_t n = h->topo.nbr[3 * r + v];
+                // limiter neighbours: device index, -2 - type for faces without a neighbour
+                nb[(size_t)v * h->ne_pad + d] =
+                    n >= 0 ? h->tiling.dev_of_ref[n] : -2 - (int)h->topo.btype[3 * r + v];
+            }
+            for (int k = 0; k < h->nd; ++k) bdev[(size_t)k * h->ne_pad + d] = bathm[r * h->nd + k];
+        }
+        if ((e = h->enodes.alloc(en.size())) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->enodes.p, en.data(), en.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if ((e = h->nbr.alloc(nb.size())) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->nbr.p, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (h->fp32) {
+            std::vector<float> bf(bdev.begin(), bdev.end());
+            cudaMemcpy(h->bath, bf.data(), bath_bytes, cudaMemcpyHostToDevice);
+        } else {
+            cudaMemcpy(h->bath, bdev.data(), bath_bytes, cudaMemcpyHostToDevice);
+        }
+        std::vector<double2> xy(h->nn);
+        std::vector<double> nz(h->nn);
+        for (int64_t i = 0; i < h->nn; ++i) {
+            xy[i] = make_double2(h->node_xyz[3 * i], h->node_xyz[3 * i + 1]);
+            nz[i] = h->node_xyz[3 * i + 2];
+        }
+        if ((e = h->xy.alloc(h->nn)) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->xy.p, xy.data(), h->nn * sizeof(double2), cudaMemcpyHostToDevice);
+        if ((e = h->nz.alloc(h->nn)) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->nz.p, nz.data(), h->nn * sizeof(double), cudaMemcpyHostToDevice);
+        const size_t nedges = h->tiling.edges.size() / 4;
+        if ((e = h->edges.alloc(nedges)) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->edges.p, h->tiling.edges.data(), nedges * sizeof(int4), cudaMemcpyHostToDevice);
+        if ((e = h->tile_edge_off.alloc(h->tiling.tile_edge_off.size())) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->tile_edge_off.p, h->tiling.tile_edge_off.data(), h->tiling.tile_edge_off.size() * sizeof(int),
+                   cudaMemcpyHostToDevice);
+        if ((e = h->eslot.alloc(h->ne)) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->eslot.p, h->tiling.eslot.data(), h->ne * sizeof(int2), cudaMemcpyHostToDevice);
+        if ((e = h->ref_of_dev.alloc(h->ne)) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->ref_of_dev.p, h->tiling.ref_of_dev.data(), h->ne * sizeof(int), cudaMemcpyHostToDevice);
+        for (int i = 0; i < 2; ++i) {
+            if ((e = h->wet[i].alloc(h->ne_pad)) != cudaSuccess) return cleanup_fail("alloc", e);
+            cudaMemset(h->wet[i].p, 1, h->ne_pad);
+        }
+        if ((e = h->limited.alloc(h->ne_pad)) != cudaSuccess) return cleanup_fail("alloc", e);
+        if (cfg->slope_limiting) {
+            if ((e = h->baryctr.alloc((size_t)3 * h->ne_pad)) != cudaSuccess) return cleanup_fail("alloc", e);
+            cudaMemset(h->baryctr.p, 0, (size_t)3 * h->ne_pad * sizeof(double));
+            h->device_bytes += (int64_t)3 * h->ne_pad * 8;
+        }
+        cudaMemset(h->limited.p, 0, h->ne_pad);
+        if ((e = h->status.alloc(1)) != cudaSuccess) return cleanup_fail("alloc", e);
+        DevStatus z;
+        std::memset(&z, 0, sizeof(z));
+        z.nan_ref_elem = 0xffffffffu;
+        cudaMemcpy(h->status.p, &z, sizeof(z), cudaMemcpyHostToDevice);
+        if ((e = h->clock.alloc(1)) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemset(h->clock.p, 0, sizeof(DevClock));
+        if ((e = h->red.alloc(reduction_partials(h->ne))) != cudaSuccess) return cleanup_fail("alloc", e);
+        {
+            static L2Rule Rh;
+            std::string e2;
+            if (make_l2_rule(Rh, e2) != DGSW_OK) {
+                dgsw_rkdg_destroy(h);
+                return fail(DGSW_ERR_UNSUPPORTED, e2);
+            }
+            if ((e = h->l2rule.alloc(1)) != cudaSuccess) return cleanup_fail("alloc", e);
+            cudaMemcpy(h->l2rule.p, &Rh, sizeof(L2Rule), cudaMemcpyHostToDevice);
+        }
+        h->device_bytes += en.size() * 4 + nb.size() * 4 + h->nn * 24 + nedges * 16 + h->ne * 12 + 3 * h->ne_pad;
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return cleanup_fail("setup", e);
+    *out = h;
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_destroy(dgsw_handle h) {
+    if (!h) return DGSW_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    destroy_graphs(h);
+    for (void* p : h->Q)
+        if (p) cudaFree(p);
+    for (void* p : h->SOL)
+        if (p) cudaFree(p);
+    if (h->bath) cudaFree(h->bath);
+    h->enodes.release();
+    h->tile_edge_off.release();
+    h->ref_of_dev.release();
+    h->eslot.release();
+    h->edges.release();
+    h->xy.release();
+    h->nz.release();
+    h->wet[0].release();
+    h->wet[1].release();
+    h->status.release();
+    h->clock.release();
+    h->red.release();
+    h->l2rule.release();
+    h->limited.release();
+    h->nbr.release();
+    h->baryctr.release();
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_info(dgsw_handle h, dgsw_info* o) {
+    if (!h || !o) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    std::memset(o, 0, sizeof(*o));
+    o->n_elems = h->ne;
+    o->n_nodes = h->nn;
+    o->n_interfaces = (int64_t)h->topo.intf.size() / 4;
+    o->n_boundaries = (int64_t)h->topo.bnd.size() / 3;
+    o->n_tiles = h->tiling.ntiles;
+    o->n_tile_edges = (int64_t)h->tiling.edges.size() / 4;
+    o->p = h->cfg.p;
+    o->ndof = h->nd;
+    o->ngp_volume = h->tb.nq;
+    o->ngp_edge = h->tb.ng;
+    o->nstages = h->ns;
+    o->precision = h->cfg.precision;
+    o->tile = h->tile;
+    o->device_bytes = h->device_bytes;
+    o->state_bytes = (int64_t)3 * h->nd * h->ne_pad * h->real_size;
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_init_state(dgsw_handle h) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    cudaSetDevice(h->device);
+    std::vector<double> q;
+    project_initial_condition(h->topo, h->node_xyz.data(), h->tb, h->cfg, q);
+    std::vector<uint8_t> wet;
+    init_wet_dry(h->topo, h->node_xyz.data(), h->tb, h->cfg, q, wet);
+    h->t = 0.0;
+    h->step = 0;
+    h->stage = 0;
+    DevClock c = {0.0, 0};
+    CUDA_TRY(cudaMemcpyAsync(h->clock.p, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
+    int rc = upload_state(h, q.data());
+    if (rc) return rc;
+    return upload_wet(h, wet.data());
+}
+
+int32_t dgsw_rkdg_set_state(dgsw_handle h, const double* q) {
+    if (!h || !q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    return upload_state(h, q);
+}
+
+int32_t dgsw_rkdg_get_state(dgsw_handle h, double* q) {
+    if (!h || !q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    const size_t n = (size_t)3 * h->nd * h->ne_pad;
+    if (h->fp32) {
+        std::vector<float> buf(n);
+        CUDA_TRY(cudaMemcpyAsync(buf.data(), h->Q[h->stage], n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        dev_to_host_layout<float>(h, buf, q);
+    } else {
+        std::vector<double> buf(n);
+        CUDA_TRY(cudaMemcpyAsync(buf.data(), h->Q[h->stage], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        dev_to_host_layout<double>(h, buf, q);
+    }
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_set_wet(dgsw_handle h, const uint8_t* wet) {
+    if (!h || !wet) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    return upload_wet(h, wet);
+}
+
+int32_t dgsw_rkdg_get_wet(dgsw_handle h, uint8_t* wet) {
+    if (!h || !wet) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    std::vector<unsigned char> w(h->ne_pad);
+    CUDA_TRY(cudaMemcpyAsync(w.data(), h->wet[h->wet_cur].p, h->ne_pad, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int64_t d = 0; d < h->ne; ++d) wet[h->tiling.ref_of_dev[d]] = w[d];
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_get_limited(dgsw_handle h, uint8_t* flags) {
+    if (!h || !flags) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    std::vector<unsigned char> w(h->ne_pad);
+    CUDA_TRY(cudaMemcpyAsync(w.data(), h->limited.p, h->ne_pad, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int64_t d = 0; d < h->ne; ++d) flags[h->tiling.ref_of_dev[d]] = w[d];
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
+    if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    cudaError_t e = h->fp32 ? launch_permute_in<float>((const float*)d_q, (float*)h->Q[h->stage], h->ref_of_dev.p,
+                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream)
+                            : launch_permute_in<double>((const double*)d_q, (double*)h->Q[h->stage], h->ref_of_dev.p,
+                                                        (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("set_state_device: ") + cudaGetErrorString(e));
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_get_state_device(dgsw_handle h, void* d_q) {
+    if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    cudaError_t e = h->fp32 ? launch_permute_out<float>((const float*)h->Q[h->stage], (float*)d_q, h->ref_of_dev.p,
+                                                        (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream)
+                            : launch_permute_out<double>((const double*)h->Q[h->stage], (double*)d_q, h->ref_of_dev.p,
+                                                         (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("get_state_device: ") + cudaGetErrorString(e));
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_stage(dgsw_handle h) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    cudaSetDevice(h->device);
+    int64_t launches = 0;
+    cudaError_t e = enqueue_stage(h, h->stage, launches);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("stage: ") + cudaGetErrorString(e));
+    advance_host_stepper(h);
+    return check_status(h);
+}
+
+int32_t dgsw_rkdg_step(dgsw_handle h, int32_t nsteps) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (nsteps < 0) return fail(DGSW_ERR_INVALID_ARGUMENT, "negative step count");
+    cudaSetDevice(h->device);
+    int64_t launches = 0;
+    CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+    // finish a partially advanced step stage by stage
+    while (h->stage != 0 && nsteps > 0) {
+        cudaError_t e = enqueue_stage(h, h->stage, launches);
+        if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("stage: ") + cudaGetErrorString(e));
+        advance_host_stepper(h);
+        if (h->stage == 0) --nsteps;
+    }
+    for (int32_t n = 0; n < nsteps; ++n) {
+        // a captured step bakes in the buffer pointers: key the graphs by the parity of the
+        // q_0 <-> q_ns swaps and by which wet-flag buffer is current
+        const int key = h->qswap + 2 * h->wet_cur;
+        if (h->cfg.use_graphs) {
+            if (!h->graph[key]) {
+                cudaGraph_t g;
+                std::vector<void*> Qsave = h->Q;
+                const int wsave = h->wet_cur, qsave = h->qswap;
+                CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+                int64_t l2 = 0;
+                cudaError_t ce = cudaSuccess;
+                for (int s = 0; s < h->ns && ce == cudaSuccess; ++s) ce = enqueue_stage(h, s, l2);
+                cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
+                h->Q = Qsave;
+                h->wet_cur = wsave;
+                h->qswap = qsave;
+                if (ce != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+                if (ee != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("capture end: ") + cudaGetErrorString(ee));
+                CUDA_TRY(cudaGraphInstantiate(&h->graph[key], g, 0));
+                cudaGraphDestroy(g);
+            }
+            CUDA_TRY(cudaGraphLaunch(h->graph[key], h->stream));
+            // replay the host-side buffer rotation of one step
+            for (int s = 0; s < h->ns; ++s) {
+                h->wet_cur = 1 - h->wet_cur;
+                if (s + 1 == h->ns) {
+                    std::swap(h->Q[0], h->Q[h->ns]);
+                    h->qswap ^= 1;
+                }
+                ++launches;
+                if (h->cfg.slope_limiting) ++launches;
+            }
+        } else {
+            for (int s = 0; s < h->ns; ++s) {
+                cudaError_t e = enqueue_stage(h, s, launches);
+                if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("stage: ") + cudaGetErrorString(e));
+            }
+        }
+        for (int s = 0; s < h->ns; ++s) advance_host_stepper(h);
+    }
+    CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+    int rc = check_status(h);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_ms = ms;
+    h->last_launches = launches;
+    return rc;
+}
+
+int32_t dgsw_rkdg_get_time(dgsw_handle h, double* t, int64_t* step, int32_t* stage) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (t) *t = h->t + h->cfg.dt * h->rk.drk[h->stage];
+    if (step) *step = h->step;
+    if (stage) *stage = h->stage;
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_l2_error(dgsw_handle h, double* out) {
+    if (!h || !out) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    double s = 0;
+    int rc = h->fp32 ? run_reduction<float>(h, 0, &s) : run_reduction<double>(h, 0, &s);
+    if (rc) return rc;
+    *out = std::sqrt(s);
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_mass(dgsw_handle h, double* out) {
+    if (!h || !out) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    return h->fp32 ? run_reduction<float>(h, 1, out) : run_reduction<double>(h, 1, out);
+}
+
+int32_t dgsw_rkdg_topology(dgsw_handle h, int32_t* neighbors, uint8_t* btype, int64_t* n_interfaces,
+                           int32_t* interfaces, int64_t* n_boundaries, int32_t* boundaries) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    const Topology& T = h->topo;
+    if (neighbors) std::memcpy(neighbors, T.nbr.data(), T.nbr.size() * sizeof(int32_t));
+    if (btype) std::memcpy(btype, T.btype.data(), T.btype.size());
+    if (n_interfaces) *n_interfaces = (int64_t)T.intf.size() / 4;
+    if (interfaces) std::memcpy(interfaces, T.intf.data(), T.intf.size() * sizeof(int32_t));
+    if (n_boundaries) *n_boundaries = (int64_t)T.bnd.size() / 3;
+    if (boundaries) std::memcpy(boundaries, T.bnd.data(), T.bnd.size() * sizeof(int32_t));
+    return DGSW_OK;
+}
+
+int32_t dgsw_mesh_topology(const dgsw_mesh* mesh, int32_t* neighbors, uint8_t* btype, int64_t* n_interfaces,
+                           int32_t* interfaces, int64_t* n_boundaries, int32_t* boundaries) {
+    if (!mesh) return fail(DGSW_ERR_INVALID_ARGUMENT, "null mesh");
+    Topology T;
+    std::string err;
+    int rc = build_topology(mesh, T, err);
+    if (rc) return fail(rc, err);
+    if (neighbors) std::memcpy(neighbors, T.nbr.data(), T.nbr.size() * sizeof(int32_t));
+    if (btype) std::memcpy(btype, T.btype.data(), T.btype.size());
+    if (n_interfaces) *n_interfaces = (int64_t)T.intf.size() / 4;
+    if (interfaces) std::memcpy(interfaces, T.intf.data(), T.intf.size() * sizeof(int32_t));
+    if (n_boundaries) *n_boundaries = (int64_t)T.bnd.size() / 3;
+    if (boundaries) std::memcpy(boundaries, T.bnd.data(), T.bnd.size() * sizeof(int32_t));
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_set_stream(dgsw_handle h, void* s) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)s;
+    h->own_stream = false;
+    destroy_graphs(h);
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_synchronize(dgsw_handle h) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    cudaSetDevice(h->device);
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_last_step_timing(dgsw_handle h, double* ms, int64_t* launches) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (ms) *ms = h->last_ms;
+    if (launches) *launches = h->last_launches;
+    return DGSW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,590 @@
+// Host-side preprocessing of the RKDG library (see host_setup.h).
+#include "host_setup.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <unordered_map>
+
+#include "function_sets.h"
+#include "quadrature.h"
+
+namespace dgsw {
+
+// ------------------------------------------------------------------------------------------------
+// Dubiner modal basis on the master triangle (source/basis/bases_2D/basis_dubiner_2D.cpp):
+// phi_(p,q) = P_p^(0,0)(n1) ((1-n2)/2)^p P_q^(2p+1,0)(n2),  n1 = 2(1+z1)/(1-z2) - 1, n2 = z2,
+// with the reference's values at the collapsed vertex (-1, 1). Modes are numbered along the
+// anti-diagonals p+q = 0, 1, 2, ... with q descending, matching the reference's dof -> (p,q) map.
+// ------------------------------------------------------------------------------------------------
+static void mode_pq(int dof, int& p, int& q) {
+    int d = 0;
+    while ((d + 1) * (d + 2) / 2 <= dof) ++d;  // anti-diagonal index
+    p = dof - d * (d + 1) / 2;
+    q = d - p;
+}
+
+// P_n^(a,b)(x) by the standard three-term recurrence
+static double jacobi(int n, int a, int b, double x) {
+    if (n == 0) return 1.0;
+    double pm = 1.0, pc = (a - b + (a + b + 2) * x) / 2;
+    for (int i = 1; i < n; ++i) {
+        double c1 = 2.0 * (i + 1) * (i + a + b + 1) * (2 * i + a + b);
+        double c2 = (2.0 * i + a + b + 1) * (double)(a * a - b * b);
+        double c3 = (2.0 * i + a + b) * (2.0 * i + a + b + 1) * (2.0 * i + a + b + 2);
+        double c4 = 2.0 * (i + a) * (i + b) * (2 * i + a + b + 2);
+        double pn = ((c2 + c3 * x) * pc - c4 * pm) / c1;
+        pm = pc;
+        pc = pn;
+    }
+    return pc;
+}
+
+static double djacobi(int n, int a, int b, double x) {
+    if (n == 0) return 0.0;
+    if (n == 1) return (a + b + n + 1) / 2.0;
+    return jacobi(n - 1, a + 1, b + 1, x) * ((a + b + n + 1) / 2.0);
+}
+
+// values at the singular vertex (-1, 1): the reference's recursions (basis_dubiner_2D.cpp:177-211)
+static double sing_dz1(int q) {
+    double a = 3.0, b = 1.0;
+    for (int k = 1; k <= q; ++k) {
+        double na = a + k + 2, nb = a + b;
+        a = na;
+        b = nb;
+    }
+    return b;
+}
+static double sing_dz2(int q) {
+    double a = 0.5, b = 0.0;
+    for (int k = 1; k <= q; ++k) {
+        double na = a + 0.5 * (k + 1), nb = a + b;
+        a = na;
+        b = nb;
+    }
+    return b;
+}
+
+static void dubiner_eval(int dof, double z1, double z2, double& phi, double& d1, double& d2) {
+    int p, q;
+    mode_pq(dof, p, q);
+    const double n1 = 2 * (1 + z1) / (1 - z2) - 1;
+    const double n2 = z2;
+    const double s = (1 - n2) / 2;
+    const double sp = std::pow(s, p);
+    const double Pp = jacobi(p, 0, 0, n1), Pq = jacobi(q, 2 * p + 1, 0, n2);
+    const double dPp = djacobi(p, 0, 0, n1), dPq = djacobi(q, 2 * p + 1, 0, n2);
+    phi = Pp * sp * Pq;
+    d1 = (2.0 / (1.0 - n2)) * dPp * sp * Pq;
+    d2 = ((1 + n1) / (1.0 - n2)) * dPp * sp * Pq + Pp * (sp * dPq - (p / 2.0) * std::pow(s, p - 1) * Pq);
+    if (std::isnan(n1)) {
+        phi = (p == 0) ? q + 1.0 : 0.0;
+        d1 = (p == 1) ? sing_dz1(q) : 0.0;
+        d2 = (p == 0) ? 3 * sing_dz2(q) : (p == 1 ? sing_dz2(q + 1) : 0.0);
+    }
+}
+
+static void face_to_master(int f, double z, double& z1, double& z2) {
+    // master_triangle.tpp:89-122
+    if (f == 0) {
+        z1 = -z;
+        z2 = z;
+    } else if (f == 1) {
+        z1 = -1.0;
+        z2 = -z;
+    } else {
+        z1 = z;
+        z2 = -1.0;
+    }
+}
+
+void eval_basis(int p, const double* z1, const double* z2, int n, double* phi) {
+    const int nd = (p + 1) * (p + 2) / 2;
+    for (int k = 0; k < nd; ++k)
+        for (int i = 0; i < n; ++i) {
+            double d1, d2;
+            dubiner_eval(k, z1[i], z2[i], phi[k * n + i], d1, d2);
+        }
+}
+
+int build_tables(int p, Tables& t, std::string& err) {
+    if (p < 1 || p > 2) {
+        err = "polynomial_order must be 1 or 2";
+        return DGSW_ERR_UNSUPPORTED;
+    }
+    std::memset(&t, 0, sizeof(Tables));
+    t.p = p;
+    t.nd = (p + 1) * (p + 2) / 2;
+    Rule2D r = triangle_rule(2 * p);
+    Rule1D gl = gauss_legendre_degree(2 * p + 1);
+    t.nq = (int)r.w.size();
+    t.ng = (int)gl.w.size();
+    if (t.nq > MAX_NQ || t.ng > MAX_NG) {
+        err = "quadrature larger than the compiled tables";
+        return DGSW_ERR_UNSUPPORTED;
+    }
+    for (int gp = 0; gp < t.nq; ++gp) {
+        t.w[gp] = r.w[gp];
+        t.psi[0][gp] = -(r.z1[gp] + r.z2[gp]) / 2;
+        t.psi[1][gp] = (1 + r.z1[gp]) / 2;
+        t.psi[2][gp] = (1 + r.z2[gp]) / 2;
+        for (int k = 0; k < t.nd; ++k) {
+            double ph, d1, d2;
+            dubiner_eval(k, r.z1[gp], r.z2[gp], ph, d1, d2);
+            t.phi[k * t.nq + gp] = ph;
+            t.dphi[0][k * t.nq + gp] = d1;
+            t.dphi[1][k * t.nq + gp] = d2;
+            t.mz[0][gp * t.nd + k] = d1 * r.w[gp];
+            t.mz[1][gp * t.nd + k] = d2 * r.w[gp];
+            t.phiw[gp * t.nd + k] = ph * r.w[gp];
+        }
+    }
+    for (int g = 0; g < t.ng; ++g) t.gw[g] = gl.w[g];
+    for (int f = 0; f < 3; ++f)
+        for (int g = 0; g < t.ng; ++g) {
+            double z1, z2;
+            face_to_master(f, gl.z[g], z1, z2);
+            t.fpsi[f][0][g] = -(z1 + z2) / 2;
+            t.fpsi[f][1][g] = (1 + z1) / 2;
+            t.fpsi[f][2][g] = (1 + z2) / 2;
+            for (int k = 0; k < t.nd; ++k) {
+                double ph, d1, d2;
+                dubiner_eval(k, z1, z2, ph, d1, d2);
+                t.fphi[f][k * t.ng + g] = ph;
+            }
+        }
+    for (int k = 0; k < t.nd; ++k) {
+        int pp, qq;
+        mode_pq(k, pp, qq);
+        t.minv[k] = (2 * pp + 1) * (pp + qq + 1) / 2.0;  // diagonal of the inverse master mass matrix
+    }
+    return DGSW_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Topology. Same results as MeshMetaData (mesh_metadata.cpp:3-85): faces are matched by their
+// unordered node pair; here by sorting the 3*ne face keys instead of a hash dictionary. Boundary
+// faces take the type of the first boundary chain that contains the node pair as neighbours of the
+// first occurrence of the face's first node (AdcircFormat::has_edge semantics).
+// ------------------------------------------------------------------------------------------------
+int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
+    const int64_t ne = m->n_elems;
+    if (ne <= 0 || m->n_nodes <= 0 || !m->node_xyz || !m->elem_nodes) {
+        err = "empty mesh";
+        return DGSW_ERR_INVALID_ARGUMENT;
+    }
+    if (ne > (int64_t)std::numeric_limits<int32_t>::max() / 4) {
+        err = "too many elements";
+        return DGSW_ERR_UNSUPPORTED;
+    }
+    T.ne = ne;
+    T.nn = m->n_nodes;
+    std::vector<std::pair<uint32_t, int32_t>> ord(ne);
+    for (int64_t i = 0; i < ne; ++i) ord[i] = {m->elem_ids ? m->elem_ids[i] : (uint32_t)i, (int32_t)i};
+    std::sort(ord.begin(), ord.end());
+    T.ids.resize(ne);
+    T.src.resize(ne);
+    T.enodes.resize(3 * ne);
+    for (int64_t r = 0; r < ne; ++r) {
+        if (r > 0 && ord[r].first == ord[r - 1].first) {
+            err = "Fatal Error: duplicate element ID " + std::to_string(ord[r].first);
+            return DGSW_ERR_MESH;
+        }
+        T.ids[r] = ord[r].first;
+        T.src[r] = ord[r].second;
+        for (int v = 0; v < 3; ++v) {
+            int32_t n = m->elem_nodes[3 * (int64_t)ord[r].second + v];
+            if (n < 0 || n >= m->n_nodes) {
+                err = "Fatal Error: element node index out of range";
+                return DGSW_ERR_MESH;
+            }
+            T.enodes[3 * r + v] = n;
+        }
+        const double* X = m->node_xyz;
+        const int32_t* nd = &T.enodes[3 * r];
+        double det = (X[3 * nd[1]] - X[3 * nd[0]]) * (X[3 * nd[2] + 1] - X[3 * nd[0] + 1]) -
+                     (X[3 * nd[1] + 1] - X[3 * nd[0] + 1]) * (X[3 * nd[2]] - X[3 * nd[0]]);
+        if (!(det > 0)) {
+            err = "element " + std::to_string(T.ids[r]) +
+                  " is not counter-clockwise (or degenerate); reorder its nodes (the reference swaps coordinates "
+                  "but not node IDs for such elements, which this library does not reproduce)";
+            return DGSW_ERR_UNSUPPORTED;
+        }
+    }
+    // face keys
+    struct FK {
+        uint64_t key;
+        int32_t r;
+        int8_t f;
+    };
+    std::vector<FK> fk(3 * ne);
+    for (int64_t r = 0; r < ne; ++r)
+        for (int f = 0; f < 3; ++f) {
+            uint32_t a = (uint32_t)T.enodes[3 * r + (f + 1) % 3], b = (uint32_t)T.enodes[3 * r + (f + 2) % 3];
+            fk[3 * r + f] = {(uint64_t)std::min(a, b) << 32 | std::max(a, b), (int32_t)r, (int8_t)f};
+        }
+    std::sort(fk.begin(), fk.end(), [](const FK& x, const FK& y) {
+        return x.key != y.key ? x.key < y.key : (x.r != y.r ? x.r < y.r : x.f < y.f);
+    });
+    T.nbr.assign(3 * ne, -1);
+    T.nbr_face.assign(3 * ne, -1);
+    T.btype.assign(3 * ne, 255);
+    // boundary chain lookup: first occurrence of each node in each chain
+    std::unordered_map<uint64_t, int64_t> first_pos;
+    for (int32_t s = 0; s < m->n_segments; ++s)
+        for (int64_t i = m->seg_offsets[s]; i < m->seg_offsets[s + 1]; ++i) {
+            uint64_t k = (uint64_t)(uint32_t)s << 32 | (uint32_t)m->seg_nodes[i];
+            if (!first_pos.count(k)) first_pos[k] = i;
+        }
+    auto lookup_type = [&](int32_t n0, int32_t n1) -> int {
+        for (int32_t s = 0; s < m->n_segments; ++s) {
+            auto it = first_pos.find((uint64_t)(uint32_t)s << 32 | (uint32_t)n0);
+            if (it == first_pos.end()) continue;
+            int64_t i = it->second;
+            if (i + 1 < m->seg_offsets[s + 1] && m->seg_nodes[i + 1] == n1) return m->seg_type[s];
+            if (i > m->seg_offsets[s] && m->seg_nodes[i - 1] == n1) return m->seg_type[s];
+        }
+        return -1;
+    };
+    for (size_t i = 0; i < fk.size();) {
+        size_t j = i + 1;
+        while (j < fk.size() && fk[j].key == fk[i].key) ++j;
+        if (j - i > 2) {
+            err = "Fatal Error: edge shared by more than two elements";
+            return DGSW_ERR_MESH;
+        }
+        if (j - i == 2) {
+            const FK& A = fk[i];
+            const FK& B = fk[i + 1];
+            if (A.r == B.r) {
+                err = "Fatal Error: degenerate element";
+                return DGSW_ERR_MESH;
+            }
+            T.nbr[3 * A.r + A.f] = B.r;
+            T.nbr_face[3 * A.r + A.f] = B.f;
+            T.btype[3 * A.r + A.f] = DGSW_BC_INTERNAL;
+            T.nbr[3 * B.r + B.f] = A.r;
+            T.nbr_face[3 * B.r + B.f] = A.f;
+            T.btype[3 * B.r + B.f] = DGSW_BC_INTERNAL;
+        } else {
+            const FK& A = fk[i];
+            int32_t n0 = T.enodes[3 * A.r + (A.f + 1) % 3], n1 = T.enodes[3 * A.r + (A.f + 2) % 3];
+            int bt = lookup_type(n0, n1);
+            if (bt < 0) {
+                err = "Fatal Error: boundary not found, unable to assign BOUNDARY_TYPE to given node_pair (" +
+                      std::to_string(n0) + ", " + std::to_string(n1) + ")!";
+                return DGSW_ERR_MESH;
+            }
+            if (bt == DGSW_BC_TIDE || bt == DGSW_BC_FLOW) {
+                err = "tide and flow boundaries need .bcis forcing data, which this build does not support";
+                return DGSW_ERR_UNSUPPORTED;
+            }
+            if (bt != DGSW_BC_LAND && bt != DGSW_BC_FUNCTION && bt != DGSW_BC_OUTFLOW) {
+                err = "unsupported boundary type " + std::to_string(bt);
+                return DGSW_ERR_UNSUPPORTED;
+            }
+            T.btype[3 * A.r + A.f] = (uint8_t)bt;
+        }
+        i = j;
+    }
+    // two faces of one element against the same neighbour would collide in the reference's
+    // (element, neighbour) keyed map; reject such meshes
+    for (int64_t r = 0; r < ne; ++r)
+        for (int f = 0; f < 3; ++f)
+            for (int g = f + 1; g < 3; ++g)
+                if (T.nbr[3 * r + f] >= 0 && T.nbr[3 * r + f] == T.nbr[3 * r + g]) {
+                    err = "Fatal Error: two elements share more than one edge";
+                    return DGSW_ERR_MESH;
+                }
+    // interfaces in (in, ex) order, in = smaller reference ID (swe_pre_create_intface.hpp:14-34)
+    T.intf.clear();
+    std::vector<int64_t> intf_of_face(3 * ne, -1);
+    for (int64_t r = 0; r < ne; ++r) {
+        // faces of r with a larger neighbour, ordered by the neighbour
+        int fs[3], n = 0;
+        for (int f = 0; f < 3; ++f)
+            if (T.nbr[3 * r + f] > r) fs[n++] = f;
+        std::sort(fs, fs + n, [&](int a, int b) { return T.nbr[3 * r + a] < T.nbr[3 * r + b]; });
+        for (int k = 0; k < n; ++k) {
+            int f = fs[k];
+            int32_t e = T.nbr[3 * r + f];
+            int fe = T.nbr_face[3 * r + f];
+            int64_t idx = (int64_t)T.intf.size() / 4;
+            T.intf.push_back((int32_t)r);
+            T.intf.push_back(e);
+            T.intf.push_back(f);
+            T.intf.push_back(fe);
+            intf_of_face[3 * r + f] = idx;
+            intf_of_face[3 * (int64_t)e + fe] = idx;
+        }
+    }
+    // boundaries grouped by type (Land, Tide, Flow, Function tuple order), each by (element, face)
+    T.bnd.clear();
+    std::vector<int64_t> bnd_of_face(3 * ne, -1);
+    for (int bt : {DGSW_BC_LAND, DGSW_BC_FUNCTION}) {
+        for (int64_t r = 0; r < ne; ++r)
+            for (int f = 0; f < 3; ++f)
+                if (T.btype[3 * r + f] == bt) {
+                    bnd_of_face[3 * r + f] = (int64_t)T.bnd.size() / 3;
+                    T.bnd.push_back((int32_t)r);
+                    T.bnd.push_back(f);
+                    T.bnd.push_back(bt);
+                }
+    }
+    // per element accumulation order: its interfaces by creation index, then its boundaries
+    T.order_count.assign(ne, 0);
+    T.order_face.assign(3 * ne, 0);
+    T.is_in.assign(3 * ne, 0);
+    for (int64_t r = 0; r < ne; ++r) {
+        std::pair<int64_t, int> items[3];
+        int n = 0;
+        for (int f = 0; f < 3; ++f)
+            if (intf_of_face[3 * r + f] >= 0) items[n++] = {intf_of_face[3 * r + f], f};
+        std::sort(items, items + n);
+        int ni = n;
+        for (int f = 0; f < 3; ++f)
+            if (bnd_of_face[3 * r + f] >= 0) items[n++] = {bnd_of_face[3 * r + f], f};
+        std::sort(items + ni, items + n);
+        T.order_count[r] = (uint8_t)n;
+        for (int k = 0; k < n; ++k) T.order_face[3 * r + k] = (uint8_t)items[k].second;
+        // the element owns the flux evaluation of its boundary faces and of interfaces to larger IDs
+        for (int f = 0; f < 3; ++f) T.is_in[3 * r + f] = (T.nbr[3 * r + f] > r || T.nbr[3 * r + f] < 0) ? 1 : 0;
+    }
+    return DGSW_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Device order and tiles: Morton order of element centroids, cut into tiles of `tile` elements.
+// Each tile lists the edges its elements need: interior edges once per tile (an edge between two
+// tiles appears in both lists and is evaluated by both CTAs with the same code), boundary edges
+// with a boundary object (land, function). Outflow faces have no object and contribute nothing.
+// ------------------------------------------------------------------------------------------------
+static uint64_t spread21(uint64_t v) {
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffULL;
+    v = (v | v << 16) & 0x1f0000ff0000ffULL;
+    v = (v | v << 8) & 0x100f00f00f00f00fULL;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+    v = (v | v << 2) & 0x1249249249249249ULL;
+    return v;
+}
+
+int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tiling& out, std::string& err) {
+    const int64_t ne = T.ne;
+    if (tile != 64 && tile != 128 && tile != 256) {
+        err = "tile must be 64, 128 or 256";
+        return DGSW_ERR_INVALID_ARGUMENT;
+    }
+    out.tile = tile;
+    out.ref_of_dev.resize(ne);
+    std::iota(out.ref_of_dev.begin(), out.ref_of_dev.end(), 0);
+    if (morton) {
+        double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+        std::vector<double> cx(ne), cy(ne);
+        for (int64_t r = 0; r < ne; ++r) {
+            const int32_t* nd = &T.enodes[3 * r];
+            cx[r] = (X[3 * nd[0]] + X[3 * nd[1]] + X[3 * nd[2]]) / 3.0;
+            cy[r] = (X[3 * nd[0] + 1] + X[3 * nd[1] + 1] + X[3 * nd[2] + 1]) / 3.0;
+            xmin = std::min(xmin, cx[r]);
+            xmax = std::max(xmax, cx[r]);
+            ymin = std::min(ymin, cy[r]);
+            ymax = std::max(ymax, cy[r]);
+        }
+        double span = std::max(xmax - xmin, ymax - ymin);
+        if (span <= 0) span = 1;
+        std::vector<uint64_t> key(ne);
+        for (int64_t r = 0; r < ne; ++r) {
+            uint64_t ix = (uint64_t)std::min(2097151.0, std::floor((cx[r] - xmin) / span * 2097151.0));
+            uint64_t iy = (uint64_t)std::min(2097151.0, std::floor((cy[r] - ymin) / span * 2097151.0));
+            key[r] = spread21(ix) | spread21(iy) << 1;
+        }
+        std::stable_sort(out.ref_of_dev.begin(), out.ref_of_dev.end(),
+                         [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    }
+    out.dev_of_ref.resize(ne);
+    for (int64_t d = 0; d < ne; ++d) out.dev_of_ref[out.ref_of_dev[d]] = (int32_t)d;
+    out.ntiles = (ne + tile - 1) / tile;
+    out.tile_edge_off.assign(out.ntiles + 1, 0);
+    out.edges.clear();
+    out.eslot.assign(2 * ne, 0);
+    out.max_edges = 0;
+    // interface index of each interior face (for de-duplication inside a tile)
+    std::vector<int64_t> iface(3 * ne, -1);
+    for (size_t i = 0; i < T.intf.size() / 4; ++i) {
+        iface[3 * (int64_t)T.intf[4 * i] + T.intf[4 * i + 2]] = (int64_t)i;
+        iface[3 * (int64_t)T.intf[4 * i + 1] + T.intf[4 * i + 3]] = (int64_t)i;
+    }
+    std::vector<int64_t> bface(3 * ne, -1);
+    for (size_t i = 0; i < T.bnd.size() / 3; ++i) bface[3 * (int64_t)T.bnd[3 * i] + T.bnd[3 * i + 1]] = (int64_t)i;
+    std::unordered_map<int64_t, int> local;
+    for (int64_t t = 0; t < out.ntiles; ++t) {
+        local.clear();
+        int64_t base = (int64_t)out.edges.size() / 4;
+        out.tile_edge_off[t] = (int32_t)base;
+        int64_t d0 = t * tile, d1 = std::min(ne, d0 + tile);
+        for (int64_t d = d0; d < d1; ++d) {
+            int32_t r = out.ref_of_dev[d];
+            uint32_t slots[3] = {1023, 1023, 1023};
+            for (int f = 0; f < 3; ++f) {
+                int64_t ii = iface[3 * (int64_t)r + f];
+                int64_t bi = bface[3 * (int64_t)r + f];
+                if (ii >= 0) {
+                    auto it = local.find(ii);
+                    if (it != local.end()) {
+                        slots[f] = (uint32_t)it->second;
+                    } else {
+                        int idx = (int)((int64_t)out.edges.size() / 4 - base);
+                        local[ii] = idx;
+                        slots[f] = (uint32_t)idx;
+                        int32_t in = T.intf[4 * ii], ex = T.intf[4 * ii + 1];
+                        out.edges.push_back(out.dev_of_ref[in]);
+                        out.edges.push_back(out.dev_of_ref[ex]);
+                        out.edges.push_back(T.intf[4 * ii + 2] | T.intf[4 * ii + 3] << 2 | EK_INTERIOR << 4);
+                        out.edges.push_back((int32_t)ii);
+                    }
+                } else if (bi >= 0) {
+                    int idx = (int)((int64_t)out.edges.size() / 4 - base);
+                    slots[f] = (uint32_t)idx;
+                    int kind = T.bnd[3 * bi + 2] == DGSW_BC_LAND ? EK_LAND : EK_FUNCTION;
+                    out.edges.push_back((int32_t)d);
+                    out.edges.push_back(-1);
+                    out.edges.push_back(f | kind << 4);
+                    out.edges.push_back((int32_t)(-1 - bi));
+                }
+            }
+            int32_t roles = 0;
+            for (int f = 0; f < 3; ++f) roles |= (T.is_in[3 * r + f] ? 1 : 0) << f;
+            int32_t ord = T.order_count[r];
+            for (int k = 0; k < T.order_count[r]; ++k) ord |= T.order_face[3 * r + k] << (2 + 2 * k);
+            out.eslot[2 * d] = (int32_t)(slots[0] | slots[1] << 10 | slots[2] << 20);
+            out.eslot[2 * d + 1] = roles | ord << 3;
+        }
+        int n = (int)((int64_t)out.edges.size() / 4 - base);
+        if (n > 1022) {
+            err = "tile edge list overflow";
+            return DGSW_ERR_INVALID_ARGUMENT;
+        }
+        out.max_edges = std::max(out.max_edges, n);
+    }
+    out.tile_edge_off[out.ntiles] = (int32_t)((int64_t)out.edges.size() / 4);
+    return DGSW_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// FP64 projections (initialize_data_serial, swe_pre_init_data.hpp:9-64) and wet/dry initialisation
+// ------------------------------------------------------------------------------------------------
+static void elem_geom(const double* X, const int32_t* nd, double& aJ) {
+    double J00 = (X[3 * nd[1]] - X[3 * nd[0]]) / 2.0, J01 = (X[3 * nd[2]] - X[3 * nd[0]]) / 2.0;
+    double J10 = (X[3 * nd[1] + 1] - X[3 * nd[0] + 1]) / 2.0, J11 = (X[3 * nd[2] + 1] - X[3 * nd[0] + 1]) / 2.0;
+    aJ = std::abs(J00 * J11 - J10 * J01);
+}
+
+// L2ProjectionNode: ((nodal * psi_gp) * int_phi_fact) * m_inv
+static void l2_node(const Tables& tb, double aJ, const double nodal[3], double* out) {
+    double a[MAX_NQ];
+    for (int gp = 0; gp < tb.nq; ++gp) {
+        double s = 0;
+        for (int n = 0; n < 3; ++n) s += nodal[n] * tb.psi[n][gp];
+        a[gp] = s;
+    }
+    for (int k = 0; k < tb.nd; ++k) {
+        double s = 0;
+        for (int gp = 0; gp < tb.nq; ++gp) s += a[gp] * (tb.phiw[gp * tb.nd + k] * aJ);
+        out[k] = s * (tb.minv[k] / aJ);
+    }
+}
+
+void project_bathymetry(const Topology& T, const double* X, const Tables& tb, std::vector<double>& bath) {
+    bath.assign(T.ne * tb.nd, 0.0);
+    for (int64_t r = 0; r < T.ne; ++r) {
+        const int32_t* nd = &T.enodes[3 * r];
+        double aJ;
+        elem_geom(X, nd, aJ);
+        double z[3] = {X[3 * nd[0] + 2], X[3 * nd[1] + 2], X[3 * nd[2] + 2]};
+        l2_node(tb, aJ, z, &bath[r * tb.nd]);
+    }
+}
+
+void project_initial_condition(const Topology& T, const double* X, const Tables& tb, const dgsw_config& cfg,
+                               std::vector<double>& q) {
+    const int nd = tb.nd;
+    q.assign(T.ne * 3 * nd, 0.0);
+    for (int64_t r = 0; r < T.ne; ++r) {
+        const int32_t* no = &T.enodes[3 * r];
+        double aJ;
+        elem_geom(X, no, aJ);
+        double* qe = &q[r * 3 * nd];
+        if (cfg.ic_type == 0) {
+            for (int v = 0; v < 3; ++v) {
+                double nodal[3] = {cfg.ic_const[v], cfg.ic_const[v], cfg.ic_const[v]};
+                l2_node(tb, aJ, nodal, qe + v * nd);
+            }
+        } else {
+            double fg[3][MAX_NQ];
+            for (int gp = 0; gp < tb.nq; ++gp) {
+                double x = X[3 * no[0]] * tb.psi[0][gp] + X[3 * no[1]] * tb.psi[1][gp] + X[3 * no[2]] * tb.psi[2][gp];
+                double y = X[3 * no[0] + 1] * tb.psi[0][gp] + X[3 * no[1] + 1] * tb.psi[1][gp] +
+                           X[3 * no[2] + 1] * tb.psi[2][gp];
+                dgsw_fn3 f = dgsw_fn_ic(cfg.function_set, cfg.fn_params, 0.0, x, y);
+                fg[0][gp] = f.ze;
+                fg[1][gp] = f.qx;
+                fg[2][gp] = f.qy;
+            }
+            for (int v = 0; v < 3; ++v)
+                for (int k = 0; k < nd; ++k) {
+                    double s = 0;
+                    for (int gp = 0; gp < tb.nq; ++gp) s += fg[v][gp] * (tb.phiw[gp * nd + k] * aJ);
+                    qe[v * nd + k] = s * (tb.minv[k] / aJ);
+                }
+        }
+    }
+}
+
+// basis -> vertex values through T_basis_linear (first three modes, basis_dubiner_2D.cpp:213-234)
+static inline void to_vertices(const double* qv, double out[3]) {
+    out[0] = qv[0] - qv[1] - qv[2];
+    out[1] = qv[0] - qv[1] + qv[2];
+    out[2] = qv[0] + 2.0 * qv[1];
+}
+// vertex values -> basis through T_linear_basis (:236-257); higher modes become zero
+static inline void from_vertices(const double v[3], double* qv, int nd) {
+    qv[0] = v[0] * (1.0 / 3.0) + v[1] * (1.0 / 3.0) + v[2] * (1.0 / 3.0);
+    qv[1] = v[0] * (-1.0 / 6.0) + v[1] * (-1.0 / 6.0) + v[2] * (1.0 / 3.0);
+    qv[2] = v[0] * (-1.0 / 2.0) + v[1] * (1.0 / 2.0);
+    for (int k = 3; k < nd; ++k) qv[k] = 0.0;
+}
+
+void init_wet_dry(const Topology& T, const double* X, const Tables& tb, const dgsw_config& cfg, std::vector<double>& q,
+                  std::vector<uint8_t>& wet) {
+    wet.assign(T.ne, 1);
+    if (!cfg.wetting_drying) return;
+    const double thr = 1.0e6 * cfg.h_o * std::numeric_limits<double>::epsilon();
+    const int nd = tb.nd;
+    for (int64_t r = 0; r < T.ne; ++r) {
+        const int32_t* no = &T.enodes[3 * r];
+        double* qe = &q[r * 3 * nd];
+        double b[3] = {X[3 * no[0] + 2], X[3 * no[1] + 2], X[3 * no[2] + 2]};
+        double ze[3], qx[3], qy[3];
+        to_vertices(qe, ze);
+        to_vertices(qe + nd, qx);
+        to_vertices(qe + 2 * nd, qy);
+        bool set_wet = true;
+        for (int v = 0; v < 3; ++v)
+            if (ze[v] + b[v] <= cfg.h_o + thr) {
+                ze[v] = cfg.h_o - b[v];
+                set_wet = false;
+            }
+        if (!set_wet) {
+            wet[r] = 0;
+            for (int v = 0; v < 3; ++v) qx[v] = qy[v] = 0.0;
+            from_vertices(ze, qe, nd);
+            from_vertices(qx, qe + nd, nd);
+            from_vertices(qy, qe + 2 * nd, nd);
+        }
+    }
+}
+
+}  // namespace dgsw

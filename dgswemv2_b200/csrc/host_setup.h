@@ -1,0 +1,85 @@
+// Host-side preprocessing of the RKDG library: mesh topology in the reference's order, the element
+// permutation and CTA tiling used on the device, per-tile edge lists, master tables and the FP64
+// initial projections. Host C++ only.
+#ifndef DGSW_HOST_SETUP_H
+#define DGSW_HOST_SETUP_H
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dgsw_rkdg.h"
+
+namespace dgsw {
+
+constexpr int MAX_ND = 6;  // p <= 2
+constexpr int MAX_NQ = 6;
+constexpr int MAX_NG = 3;
+
+// Edge kinds in the per-tile edge lists
+enum EdgeKind { EK_INTERIOR = 0, EK_LAND = 1, EK_FUNCTION = 2 };
+
+struct Topology {
+    int64_t ne = 0, nn = 0;
+    std::vector<uint32_t> ids;      // reference element IDs, ascending
+    std::vector<int32_t> src;       // caller index of element r
+    std::vector<int32_t> enodes;    // [3*ne] node indices of element r
+    std::vector<int32_t> nbr;       // [3*ne] neighbor element (reference order) or -1
+    std::vector<int8_t> nbr_face;   // [3*ne] neighbor's local face or -1
+    std::vector<uint8_t> btype;     // [3*ne] DGSW_BC_* (128 interior)
+    std::vector<int32_t> intf;      // [4*n_intf] in, ex, face_in, face_ex in creation order
+    std::vector<int32_t> bnd;       // [3*n_bnd] elem, face, type in traversal order
+    // per element: faces in accumulation order (interfaces by creation order, then boundaries)
+    std::vector<uint8_t> order_count;  // [ne]
+    std::vector<uint8_t> order_face;   // [3*ne]
+    std::vector<uint8_t> is_in;        // [3*ne] element is the "in" side of the interface on this face
+};
+
+// reference MeshMetaData + create_interfaces/create_boundaries semantics
+int build_topology(const dgsw_mesh* m, Topology& T, std::string& err);
+
+struct Tiling {
+    int tile = 256;
+    int64_t ntiles = 0;
+    std::vector<int32_t> dev_of_ref;  // [ne]
+    std::vector<int32_t> ref_of_dev;  // [ne]
+    std::vector<int32_t> tile_edge_off;  // [ntiles+1]
+    std::vector<int32_t> edges;          // [4 * n_edges]: A dev, B dev (-1), meta, interface/boundary index
+    std::vector<int32_t> eslot;          // [2 * ne] per element (dev order): packed slots, roles + order
+    int max_edges = 0;
+};
+
+int build_tiling(const Topology& T, const double* node_xyz, int tile, bool morton, Tiling& out, std::string& err);
+
+// Master-element tables in the layouts the kernels read
+struct Tables {
+    int p = 1, nd = 3, nq = 3, ng = 2;
+    double phi[MAX_ND * MAX_NQ];         // [dof][gp]
+    double dphi[2][MAX_ND * MAX_NQ];     // [z][dof][gp]
+    double mz[2][MAX_NQ * MAX_ND];       // [z][gp][dof] = dphi_z(dof,gp) * w(gp)
+    double phiw[MAX_NQ * MAX_ND];        // [gp][dof]   = phi(dof,gp) * w(gp)
+    double psi[3][MAX_NQ];               // nodal (linear) shape functions at the volume points
+    double w[MAX_NQ];
+    double fphi[3][MAX_ND * MAX_NG];     // [face][dof][gp]
+    double fpsi[3][3][MAX_NG];           // [face][node][gp]
+    double gw[MAX_NG];
+    double minv[MAX_ND];
+};
+
+int build_tables(int p, Tables& t, std::string& err);
+
+// Dubiner modes of order p at n master points: phi[dof * n + pt]
+void eval_basis(int p, const double* z1, const double* z2, int n, double* phi);
+
+// FP64 host projections of initialize_data_serial: bathymetry modes per element (reference order)
+void project_bathymetry(const Topology& T, const double* node_xyz, const Tables& tb, std::vector<double>& bath);
+// initial condition modes [ne][3][nd] (reference order)
+void project_initial_condition(const Topology& T, const double* node_xyz, const Tables& tb, const dgsw_config& cfg,
+                               std::vector<double>& q);
+// wetting/drying initialisation on the projected state (swe_pre_init_data.hpp:213-250); returns wet flags
+void init_wet_dry(const Topology& T, const double* node_xyz, const Tables& tb, const dgsw_config& cfg,
+                  std::vector<double>& q, std::vector<uint8_t>& wet);
+
+}  // namespace dgsw
+
+#endif

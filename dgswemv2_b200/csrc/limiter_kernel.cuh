@@ -1,0 +1,204 @@
+// Cockburn-Shu TVB slope limiter in characteristic variables (CS_slope_limiter_serial,
+// source/problem/SWE/problem_slope_limiter/swe_CS_sl_serial.hpp:9-23; kernels in
+// swe_CS_slope_limiter.hpp:9-189; eigenvectors R, R^-1 in problem_jacobian/swe_jacobian.hpp:462-550;
+// limiter geometry from problem_preprocessor/swe_pre_init_data.hpp:252-326).
+//
+// One thread per element, after the stage kernel has written the new state, the new wet flags and
+// the barycentre values of every element. The limiter arithmetic runs in FP64 in both precisions:
+// its write-back test compares a relative change against 1e-12. The geometry (centroids, medians,
+// alpha = A^-1 b, r^2) is rebuilt from the FP64 node coordinates instead of being stored.
+// The KXRCF trouble indicator the reference evaluates in the same pass (swe_trouble_check.hpp) does
+// not feed the limiter there and is not evaluated here.
+#ifndef DGSW_LIMITER_KERNEL_CUH
+#define DGSW_LIMITER_KERNEL_CUH
+
+#include <cuda_runtime.h>
+
+namespace dgsw {
+
+template <typename Real>
+struct LimiterArgs {
+    Real* q;                    // state to limit in place [(var*ND+dof)][ne_pad]
+    const double* baryctr;      // [3][ne_pad]
+    const unsigned char* wet;   // new wet flags
+    const int* nbr;             // [3][ne_pad] neighbour (device index) or -2 - boundary type
+    const int* enodes;          // [3][ne_pad]
+    const double2* xy;
+    const double* nz;
+    unsigned char* limited;     // per element: 1 if its state was changed
+    int ne, ne_pad;
+    double g, M, nu;
+    void* status;
+    const int* ref_of_dev;
+};
+
+template <int ND, typename Real>
+__global__ void __launch_bounds__(256) cs_limiter_kernel(const LimiterArgs<Real> L) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= L.ne) return;
+    const size_t P = (size_t)L.ne_pad;
+    unsigned char lim = 0;
+    bool ok = L.wet[e] != 0;
+    int nb[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        nb[f] = L.nbr[f * P + e];
+        if (nb[f] >= 0) {
+            ok = ok && (L.wet[nb[f]] != 0);
+        } else {
+            const int bt = -2 - nb[f];
+            // land / function boundaries set wet_neigh to the element's own flag; faces without a
+            // boundary object (outflow) never set it and keep its initial false
+            ok = ok && (bt == 0 || bt == 3);
+        }
+    }
+    if (!ok) {
+        L.limited[e] = 0;
+        return;
+    }
+    // own vertex values (T_basis_linear) and derived barycentre / midpoint values
+    double ql[3][3], qb[3], qm[3][3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const double a = (double)L.q[(v * ND + 0) * P + e], b = (double)L.q[(v * ND + 1) * P + e],
+                     c = (double)L.q[(v * ND + 2) * P + e];
+        ql[v][0] = a - b - c;
+        ql[v][1] = a - b + c;
+        ql[v][2] = a + 2.0 * b;
+        qb[v] = L.baryctr[v * P + e];
+        // chi_midpts (master_triangle.tpp:23-33): midpoint b is opposite vertex b
+        qm[v][0] = ql[v][1] * 0.5 + ql[v][2] * 0.5;
+        qm[v][1] = ql[v][0] * 0.5 + ql[v][2] * 0.5;
+        qm[v][2] = ql[v][0] * 0.5 + ql[v][1] * 0.5;
+    }
+    // geometry
+    const int n0 = L.enodes[e], n1 = L.enodes[P + e], n2 = L.enodes[2 * P + e];
+    const double2 X0 = L.xy[n0], X1 = L.xy[n1], X2 = L.xy[n2];
+    const double X[3][2] = {{X0.x, X0.y}, {X1.x, X1.y}, {X2.x, X2.y}};
+    const double cx = (X[0][0] + X[1][0] + X[2][0]) / 3.0, cy = (X[0][1] + X[1][1] + X[2][1]) / 3.0;
+    double mid[3][2], nbc[3][2], qnb[3][3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        mid[b][0] = (X[(b + 1) % 3][0] + X[(b + 2) % 3][0]) / 2.0;
+        mid[b][1] = (X[(b + 1) % 3][1] + X[(b + 2) % 3][1]) / 2.0;
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        if (nb[f] >= 0) {
+            const int m = nb[f];
+            const double2 Y0 = L.xy[L.enodes[m]], Y1 = L.xy[L.enodes[P + m]], Y2 = L.xy[L.enodes[2 * P + m]];
+            nbc[f][0] = (Y0.x + Y1.x + Y2.x) / 3.0;
+            nbc[f][1] = (Y0.y + Y1.y + Y2.y) / 3.0;
+#pragma unroll
+            for (int v = 0; v < 3; ++v) qnb[f][v] = L.baryctr[v * P + m];
+        } else {
+            // mirrored centroid across the boundary edge, own barycentre state
+            nbc[f][0] = 2.0 * mid[f][0] - cx;
+            nbc[f][1] = 2.0 * mid[f][1] - cy;
+#pragma unroll
+            for (int v = 0; v < 3; ++v) qnb[f][v] = qb[v];
+        }
+    }
+    const double zb = L.nz[n0] * (1.0 / 3.0) + L.nz[n1] * (1.0 / 3.0) + L.nz[n2] * (1.0 / 3.0);
+    const double h = qb[0] + zb;
+    const double u = qb[1] / h, vv = qb[2] / h;
+    const double c = sqrt(L.g * h);
+    double delta[3][3];  // [var][bound]
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const int e1 = b, e2 = (b + 1) % 3;
+        const double bx = mid[b][0] - cx, by = mid[b][1] - cy;
+        const double nrm = sqrt(bx * bx + by * by);
+        const double nx = bx / nrm, ny = by / nrm;  // normalised median
+        const double A00 = nbc[e1][0] - cx, A10 = nbc[e1][1] - cy, A01 = nbc[e2][0] - cx, A11 = nbc[e2][1] - cy;
+        const double idet = 1.0 / (A00 * A11 - A10 * A01);
+        const double al0 = (A11 * idet) * bx + (-A01 * idet) * by;
+        const double al1 = (-A10 * idet) * bx + (A00 * idet) * by;
+        const double rsq = bx * bx + by * by;
+        const double un = u * nx + vv * ny;
+        const double iR[3][3] = {{(c + un) / (2 * c), -nx / (2 * c), -ny / (2 * c)},
+                                 {u * ny - vv * nx, -ny, nx},
+                                 {(c - un) / (2 * c), nx / (2 * c), ny / (2 * c)}};
+        const double R[3][3] = {{1.0, 0.0, 1.0}, {u - c * nx, -ny, u + c * nx}, {vv - c * ny, nx, vv + c * ny}};
+        double dch[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double wm = 0, w0 = 0, w1 = 0, w2 = 0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                wm += iR[i][j] * qm[j][b];
+                w0 += iR[i][j] * qb[j];
+                w1 += iR[i][j] * qnb[e1][j];
+                w2 += iR[i][j] * qnb[e2][j];
+            }
+            const double wt = wm - w0;
+            const double wd = al0 * (w1 - w0) + al1 * (w2 - w0);
+            if (fabs(wt) <= L.M * rsq)
+                dch[i] = wt;
+            else if (signbit(wt) == signbit(wd))
+                dch[i] = copysign(1.0, wt) * fmin(fabs(wt), fabs(L.nu * wd));
+            else
+                dch[i] = 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) s += R[i][j] * dch[j];
+            delta[i][b] = s;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const double dsum = delta[v][0] + delta[v][1] + delta[v][2];
+        if (dsum != 0.0) {
+            double pos = 0.0, neg = 0.0;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                pos += fmax(0.0, delta[v][b]);
+                neg += fmax(0.0, -delta[v][b]);
+            }
+            const double tp = fmin(1.0, neg / pos), tn = fmin(1.0, pos / neg);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) delta[v][b] = tp * fmax(0.0, delta[v][b]) - tn * fmax(0.0, -delta[v][b]);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        // vertex values = barycentre + delta * T, T = ones - 2 I (swe_data_slope_limit.hpp)
+        double qv[3];
+        qv[0] = qb[v] + (-delta[v][0] + delta[v][1] + delta[v][2]);
+        qv[1] = qb[v] + (delta[v][0] - delta[v][1] + delta[v][2]);
+        qv[2] = qb[v] + (delta[v][0] + delta[v][1] - delta[v][2]);
+        double d2 = 0, n2 = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double dd = qv[k] - ql[v][k];
+            d2 += dd * dd;
+            n2 += ql[v][k] * ql[v][k];
+        }
+        if (sqrt(d2) / sqrt(n2) > 1.0e-12) {
+            lim = 1;
+            L.q[(v * ND + 0) * P + e] = (Real)(qv[0] * (1.0 / 3.0) + qv[1] * (1.0 / 3.0) + qv[2] * (1.0 / 3.0));
+            L.q[(v * ND + 1) * P + e] = (Real)(qv[0] * (-1.0 / 6.0) + qv[1] * (-1.0 / 6.0) + qv[2] * (1.0 / 3.0));
+            L.q[(v * ND + 2) * P + e] = (Real)(qv[0] * (-1.0 / 2.0) + qv[1] * (1.0 / 2.0));
+#pragma unroll
+            for (int k = 3; k < ND; ++k) L.q[(v * ND + k) * P + e] = Real(0);
+        }
+    }
+    L.limited[e] = lim;
+}
+
+template <typename Real>
+cudaError_t launch_limiter_kernel(const LimiterArgs<Real>& L, int p, cudaStream_t s) {
+    const int blocks = (L.ne + 255) / 256;
+    if (p == 1)
+        cs_limiter_kernel<3, Real><<<blocks, 256, 0, s>>>(L);
+    else
+        cs_limiter_kernel<6, Real><<<blocks, 256, 0, s>>>(L);
+    return cudaGetLastError();
+}
+
+}  // namespace dgsw
+
+#endif

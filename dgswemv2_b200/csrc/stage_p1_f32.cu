@@ -1,0 +1,9 @@
+// Stage-kernel instantiations for polynomial order 1, float state (compiled as a separate unit).
+#include "stage_kernel.cuh"
+
+namespace dgsw {
+cudaError_t launch_stage_p1_f32(const StageArgs<float>& A, int tile, int ntiles, int max_edges, bool wd, bool fsrc,
+                                cudaStream_t s) {
+    return launch_stage_dispatch<1, float>(A, tile, ntiles, max_edges, wd, fsrc, s);
+}
+}  // namespace dgsw

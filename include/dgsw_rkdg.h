@@ -1,0 +1,166 @@
+/* dgsw_rkdg.h - C ABI of the B200 RKDG shallow-water library (libdgsw_rkdg.so).
+ *
+ * The library replaces the serial RKDG step of dgswemv2 behind the reference's problem/stepper
+ * interface SWE::RKDG::Problem (source/problem/SWE/discretization_RKDG/rkdg_swe_problem.hpp:34-194).
+ * Each entry point below names the reference interface it stands in for. Plain C types only: the
+ * caller owns every host array (copied in at create/set, copied out at get); the library owns the
+ * device buffers, its CUDA stream and its CUDA graphs.
+ *
+ * Errors: every function returns a dgsw_status; 0 is success. A failing call leaves a message that
+ * dgsw_last_error() returns (per host thread). Nothing aborts or traps: the reference's abort() on a
+ * NaN (rkdg_swe_proc_serial_step.hpp:59-65) becomes DGSW_ERR_NAN from dgsw_rkdg_step.
+ * Threading: one host thread per handle at a time; all work is ordered on the handle's stream.
+ */
+#ifndef DGSW_RKDG_H
+#define DGSW_RKDG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGSW_ABI_VERSION 1
+
+typedef enum {
+    DGSW_OK = 0,
+    DGSW_ERR_INVALID_ARGUMENT = 1,
+    DGSW_ERR_MESH = 2,          /* topology / boundary lookup errors (std::logic_error in the reference) */
+    DGSW_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+    DGSW_ERR_NAN = 4,           /* NaN in the modal state after a stage (scrutinize_solution) */
+    DGSW_ERR_UNSUPPORTED = 5,   /* a feature of the input this build does not implement */
+    DGSW_ERR_NO_DEVICE = 6,     /* no CUDA device visible */
+    DGSW_ERR_IO = 7             /* input file could not be read or parsed */
+} dgsw_status;
+
+typedef enum { DGSW_FP64 = 0, DGSW_FP32 = 1 } dgsw_precision;
+
+/* Boundary condition / edge types, source/problem/SWE/swe_definitions.hpp:61-69 */
+enum { DGSW_BC_LAND = 0, DGSW_BC_TIDE = 1, DGSW_BC_FLOW = 2, DGSW_BC_FUNCTION = 3, DGSW_BC_OUTFLOW = 4,
+       DGSW_BC_INTERNAL = 128 };
+
+/* Problem configuration: the `.15` input surface read by InputParameters
+ * (source/preprocessor/input_parameters.hpp:95-261) and SWE::Inputs (problem_input/swe_inputs.cpp:4-205)
+ * that the RKDG step consumes, plus the B200-specific execution options at the end. */
+typedef struct {
+    int32_t p;                 /* polynomial_order (1 or 2) */
+    int32_t rk_nstages;        /* timestepping.nstages */
+    int32_t rk_order;          /* timestepping.order */
+    double dt;                 /* timestepping.dt */
+    double g;                  /* problem.gravity */
+    int32_t wetting_drying;    /* problem.wetting_drying present */
+    double h_o;                /* problem.wetting_drying.h_o */
+    int32_t slope_limiting;    /* problem.slope_limiting.type == Cockburn-Shu */
+    double sl_M, sl_nu;        /* problem.slope_limiting.{M,nu} */
+    int32_t function_source;   /* problem.function_source: Enable */
+    int32_t ic_type;           /* problem.initial_conditions.type: 0 Default/Constant, 1 Function */
+    double ic_const[3];        /* initial_surface_height, initial_momentum_x, initial_momentum_y */
+    int32_t function_set;      /* which ic_q/source_q/true_q set (function_sets.h) */
+    double fn_params[16];      /* parameters of that set */
+    int32_t spherical;         /* problem.spherical_projection present */
+    double sp_lat0_deg, sp_R;  /* spherical_projection.{latitude_o, R} */
+    /* execution options (no reference counterpart) */
+    int32_t precision;         /* dgsw_precision: FP64, or FP32 bulk with FP64 wet/dry tests and reductions */
+    int32_t device;            /* CUDA device ordinal */
+    int32_t tile;              /* elements per CTA tile: 0 = autotune, else 64/128/256 */
+    int32_t renumber;          /* 0 keep input order, 1 Morton order of element centroids (default 1) */
+    int32_t use_graphs;        /* capture each RK step in a CUDA graph (default 1) */
+    int32_t reserved[8];
+} dgsw_config;
+
+/* Mesh: node coordinates (x, y, bathymetry depth), element node triples (0-based node indices), the
+ * reference element IDs (the order the reference iterates elements in; NULL = 0..n-1), and ADCIRC-style
+ * boundary node chains with their types, searched in the given order like AdcircFormat::get_ibtype
+ * (source/preprocessor/ADCIRC_reader/adcirc_format.cpp). */
+typedef struct {
+    int64_t n_nodes;
+    const double* node_xyz;     /* [3*n_nodes] */
+    int64_t n_elems;
+    const int32_t* elem_nodes;  /* [3*n_elems] */
+    const uint32_t* elem_ids;   /* [n_elems] or NULL */
+    int32_t n_segments;
+    const int32_t* seg_type;    /* [n_segments], DGSW_BC_* */
+    const int64_t* seg_offsets; /* [n_segments+1] */
+    const int32_t* seg_nodes;   /* [seg_offsets[n_segments]] */
+} dgsw_mesh;
+
+typedef struct {
+    int64_t n_elems, n_nodes, n_interfaces, n_boundaries, n_tiles, n_tile_edges;
+    int32_t p, ndof, ngp_volume, ngp_edge, nstages, precision, tile;
+    int64_t device_bytes;      /* bytes of device memory held by the handle */
+    int64_t state_bytes;       /* bytes of one stage state array */
+} dgsw_info;
+
+typedef struct dgsw_rkdg_s* dgsw_handle;
+
+/* library -------------------------------------------------------------------------------------- */
+int32_t dgsw_abi_version(void);
+const char* dgsw_last_error(void);
+const char* dgsw_status_string(int32_t status);
+void dgsw_config_default(dgsw_config* cfg);
+
+/* Problem::initialize_problem_parameters + preprocess_mesh_data + create_interfaces/boundaries +
+ * Simulation ctor (rkdg_swe_problem.hpp:55-92, simulation.hpp:36-65, initialize_mesh.hpp:19-77):
+ * builds topology, interface/boundary order and device geometry. Does not set the state. */
+int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_handle* out);
+int32_t dgsw_rkdg_destroy(dgsw_handle h);
+int32_t dgsw_rkdg_info(dgsw_handle h, dgsw_info* out);
+
+/* Problem::preprocessor_serial -> initialize_data_serial (swe_pre_init_data.hpp:9-327): bathymetry and
+ * initial-condition L2 projections, wetting/drying and limiter initialisation; resets time to 0. */
+int32_t dgsw_rkdg_init_state(dgsw_handle h);
+
+/* modal state of the current stage in ascending element-ID order, layout [elem][var(ze,qx,qy)][dof],
+ * FP64 on the host (elt.data.state[stage].q, swe_data_state.hpp:5-17). set_state leaves wet flags as
+ * they are; call dgsw_rkdg_set_wet to change them. */
+int32_t dgsw_rkdg_set_state(dgsw_handle h, const double* q);
+int32_t dgsw_rkdg_get_state(dgsw_handle h, double* q);
+int32_t dgsw_rkdg_set_wet(dgsw_handle h, const uint8_t* wet);
+int32_t dgsw_rkdg_get_wet(dgsw_handle h, uint8_t* wet);
+/* the same on device buffers of the library's device (layout [elem][var][dof], precision of the handle:
+ * double for FP64, float for FP32); ordered on the handle's stream */
+int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q);
+int32_t dgsw_rkdg_get_state_device(dgsw_handle h, void* d_q);
+
+/* Problem::step_serial / stage_serial (rkdg_swe_proc_serial_step.hpp:10-67): advance nsteps full RK
+ * steps (or one stage). Returns DGSW_ERR_NAN if a NaN appeared (checked once at the end of the call). */
+int32_t dgsw_rkdg_step(dgsw_handle h, int32_t nsteps);
+int32_t dgsw_rkdg_stage(dgsw_handle h);
+/* ESSPRKStepper::GetTimeAtCurrentStage / GetStep / GetStage (explicit_ssp_rk_stepper.hpp:42-46) */
+int32_t dgsw_rkdg_get_time(dgsw_handle h, double* t, int64_t* step, int32_t* stage);
+
+/* Simulation::ComputeL2Residual (simulation.hpp:85-93): sqrt of the sum over elements of
+ * int (true_q(t) - q_h)^2 over ze, qx, qy, on the device in FP64 */
+int32_t dgsw_rkdg_l2_error(dgsw_handle h, double* out);
+/* total water volume sum_e int_e (ze_h + b_h) dA, FP64 device reduction (no reference counterpart;
+ * the global mass balance check of the FP32 path) */
+int32_t dgsw_rkdg_mass(dgsw_handle h, double* out);
+
+/* integer topology in ascending element-ID order, for bit-exact comparison with the reference's
+ * MeshMetaData (mesh_metadata.cpp:3-85) and interface/boundary creation (swe_pre_create_intface.hpp,
+ * swe_pre_create_bound.hpp): neighbor element index per face (-1 none), boundary type per face
+ * (DGSW_BC_INTERNAL for interior faces), interfaces (in, ex, face_in, face_ex) in creation order,
+ * boundaries (elem, face, type) in traversal order. Pass NULL arrays to query the counts. */
+int32_t dgsw_rkdg_topology(dgsw_handle h, int32_t* neighbors, uint8_t* btype, int64_t* n_interfaces,
+                           int32_t* interfaces, int64_t* n_boundaries, int32_t* boundaries);
+
+/* The same topology computed on the host only (no device needed): MeshMetaData + interface and
+ * boundary creation for a mesh. Arrays as for dgsw_rkdg_topology; pass NULL to query counts. */
+int32_t dgsw_mesh_topology(const dgsw_mesh* mesh, int32_t* neighbors, uint8_t* btype, int64_t* n_interfaces,
+                           int32_t* interfaces, int64_t* n_boundaries, int32_t* boundaries);
+
+/* per element 1 if the last slope-limiter pass changed its state (the plain limiter's decision) */
+int32_t dgsw_rkdg_get_limited(dgsw_handle h, uint8_t* flags);
+
+/* execution control */
+int32_t dgsw_rkdg_set_stream(dgsw_handle h, void* cuda_stream);
+int32_t dgsw_rkdg_synchronize(dgsw_handle h);
+/* device time of the most recent dgsw_rkdg_step call's stage kernels, from CUDA events recorded on the
+ * handle's stream around it: total milliseconds and number of stage-kernel launches */
+int32_t dgsw_rkdg_last_step_timing(dgsw_handle h, double* ms, int64_t* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGSW_RKDG_H */

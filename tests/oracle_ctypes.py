@@ -3,7 +3,7 @@ import ctypes as C
 
 import numpy as np
 
-from dgswemv2_b200.types import ProblemConfig, MeshArrays  # noqa: F401  (shared plain-data containers)
+
 
 
 class OrcConfig(C.Structure):

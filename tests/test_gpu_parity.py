@@ -1,0 +1,131 @@
+"""CUDA path against the CPU oracle on the same meshes, initial conditions and step counts.
+
+Tolerances (written per test):
+  FP64, no wet/dry: per variable max |q_gpu - q_oracle| <= 1e-12 * max |q_oracle| (relative to the
+  variable's scale), L2 errors equal to 1e-12 relative.
+  FP32 bulk: the L2 error against the analytic solution within 1.05x of the FP64 oracle's.
+  Wet/dry + limiter (threshold branches can flip on last-bit differences): wet-cell counts within
+  0.5 %, state within 1e-9 of the variable scale after a short run.
+"""
+import numpy as np
+import pytest
+
+from dgswemv2_b200 import Problem, configs, meshgen
+from dgswemv2_b200.types import FUNCTION, LAND
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(a, b):
+    """max over variables of max|a-b| / max|b| (per-variable scale)."""
+    out = 0.0
+    for v in range(3):
+        scale = max(np.max(np.abs(b[:, v, :])), 1e-300)
+        out = max(out, np.max(np.abs(a[:, v, :] - b[:, v, :])) / scale)
+    return out
+
+
+def run_pair(oracle, mesh, cfg, nsteps, **kw):
+    P = Problem(cfg, mesh, **kw)
+    O = oracle.problem(cfg, mesh, n_threads=8)
+    q0g, q0o = P.get_state(), O.get_state()
+    assert rel_err(q0g, q0o) <= 1e-13, "initial projection"
+    P.step_serial(nsteps)
+    O.step(nsteps)
+    return P, O
+
+
+def test_config1_manufactured_p1_1000_steps(oracle):
+    """Config 1: 800 triangles, p=1, SSP-RK2, dt=1 s, 1000 steps, FP64."""
+    mesh, cfg = configs.config1()
+    P, O = run_pair(oracle, mesh, cfg, 1000)
+    e = rel_err(P.get_state(), O.get_state())
+    assert e <= 1e-12, e
+    lg, lo = P.compute_residual_L2(), O.l2_error()
+    assert abs(lg - lo) <= 1e-12 * lo, (lg, lo)
+    assert P.time()[0] == O.time() == 1000.0
+
+
+@pytest.mark.parametrize("tile", [128, 256])
+def test_p2_rk3_jittered(oracle, tile):
+    """p=2, SSP-RK3, jittered mesh (config-2 discretisation on a small mesh), 100 steps, FP64."""
+    mesh, cfg = configs.manufactured(24, p=2, rk=(3, 3), dt=2.0, jitter=0.2, seed=2)
+    P, O = run_pair(oracle, mesh, cfg, 100, tile=tile)
+    e = rel_err(P.get_state(), O.get_state())
+    assert e <= 1e-12, e
+    assert abs(P.compute_residual_L2() - O.l2_error()) <= 1e-12 * O.l2_error()
+
+
+def test_stage_by_stage_and_graphs_agree(oracle):
+    """stage_serial calls, graph-captured steps and plain launches give the same bits."""
+    mesh, cfg = configs.manufactured(10, p=1, rk=(3, 3), dt=5.0)
+    A = Problem(cfg, mesh, use_graphs=True)
+    B = Problem(cfg, mesh, use_graphs=False)
+    C = Problem(cfg, mesh)
+    A.step_serial(7)
+    B.step_serial(7)
+    for _ in range(21):
+        C.stage_serial()
+    assert np.array_equal(A.get_state(), B.get_state())
+    assert np.array_equal(A.get_state(), C.get_state())
+
+
+def test_renumbering_does_not_change_results(oracle):
+    mesh, cfg = configs.manufactured(12, p=2, rk=(2, 2), dt=5.0, jitter=0.15)
+    A = Problem(cfg, mesh, renumber=True)
+    B = Problem(cfg, mesh, renumber=False)
+    A.step_serial(20)
+    B.step_serial(20)
+    assert np.array_equal(A.get_state(), B.get_state())
+
+
+def test_fp32_bulk_l2_within_5_percent(oracle):
+    """FP32 bulk path: L2 error vs the analytic solution within 1.05x of the FP64 oracle's."""
+    mesh, cfg = configs.manufactured(20, p=2, rk=(3, 3), dt=2.0, jitter=0.2, precision="fp32")
+    P = Problem(cfg, mesh)
+    cfg64 = configs.manufactured(20, p=2, rk=(3, 3), dt=2.0, jitter=0.2)[1]
+    O = oracle.problem(cfg64, mesh, n_threads=8)
+    P.step_serial(200)
+    O.step(200)
+    lg, lo = P.compute_residual_L2(), O.l2_error()
+    assert lg <= 1.05 * lo, (lg, lo)
+    assert rel_err(P.get_state(), O.get_state()) < 1e-4
+
+
+def test_land_boundaries_conserve_mass(oracle):
+    """Closed basin with land boundaries: FP64 mass is conserved to rounding."""
+    mesh = meshgen.quad_mesh(16, 16, corners=((0, 0), (1000, 0), (1000, 1000), (0, 1000)), bc=(LAND,) * 4,
+                             jitter=0.2, seed=5, bathymetry=meshgen.bath_flat(5.0))
+    cfg = configs.ProblemConfig(p=2, rk_nstages=3, rk_order=3, dt=0.5, ic_type=1,
+                                function_set=configs.FN_GAUSSIAN_HUMPS,
+                                fn_params=configs.humps_params([(0.3, 500.0, 400.0, 120.0)]))
+    P, O = run_pair(oracle, mesh, cfg, 200)
+    assert rel_err(P.get_state(), O.get_state()) <= 1e-12
+    m0 = O.mass()
+    assert abs(P.mass() - m0) <= 1e-12 * m0
+
+
+def test_wet_dry_and_limiter_bowl(oracle):
+    """Thacker bowl with wetting/drying and the Cockburn-Shu limiter (config-3 physics, 48x48 quads)."""
+    mesh, cfg = configs.config3(nq=48, dt=1.0)
+    P, O = run_pair(oracle, mesh, cfg, 50)
+    wg, wo = P.get_wet(), O.get_wet()
+    assert abs(int(wg.sum()) - int(wo.sum())) <= max(2, 0.005 * mesh.n_elems)
+    assert rel_err(P.get_state(), O.get_state()) <= 1e-9
+    lim_g, lim_o = P.get_limited(), O.limited_flags()
+    assert np.mean(lim_g != lim_o) <= 0.005
+
+
+def test_nan_is_reported_not_aborted(oracle):
+    """A NaN injected into the host state comes back as DGSW_ERR_NAN with the element ID."""
+    from dgswemv2_b200._lib import DgswError
+
+    mesh, cfg = configs.manufactured(6, p=1)
+    P = Problem(cfg, mesh)
+    q = P.get_state()
+    q[5, 1, 0] = np.nan
+    P.set_state(q)
+    with pytest.raises(DgswError) as ei:
+        P.step_serial(1)
+    assert ei.value.status == 4
+    assert "element" in str(ei.value)
