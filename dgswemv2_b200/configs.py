@@ -3,7 +3,7 @@
 1. manufactured p=1: [0,40000]^2 m, 20x20 quads -> 800 triangles, b = 2 m, g = 9.81,
    ze = 0.1 sin(2 pi x/L) cos(2 pi y/L) cos(w t), function BC on all sides, SSP-RK2, dt = 1 s, 1000 steps
 2. manufactured p=2 at scale: 512x512 quads -> 524,288 triangles, interior nodes jittered by +-20% of the
-   cell size (seed 2), Dunavant degree 4 / 3-point Gauss-Legendre, SSP-RK3, 200 steps
+   cell size (seed 2), Dunavant degree 4 / 3-point Gauss-Legendre, SSP-RK3, 200 steps of dt = 0.5 s
 3. Thacker bowl with wetting/drying + slope limiter: +-4000 m, 256x256 quads -> 131,072 triangles,
    h0 = 10 m, a = 3000 m, amplitude 2 m, p=1, SSP-RK2, h_o = 0.01 m, two periods
 4. learned troubled-cell indicator on bowl meshes with random Gaussian humps
@@ -38,8 +38,10 @@ def config1(precision="fp64"):
     return manufactured(20, p=1, rk=(2, 2), dt=1.0, precision=precision)
 
 
-def config2(nq=512, precision="fp64"):
-    return manufactured(nq, p=2, rk=(3, 3), dt=1.0, jitter=0.2, seed=2, precision=precision)
+def config2(nq=512, precision="fp64", dt=0.5):
+    """dt is not part of the configuration; 0.5 s keeps the Courant number near 0.1 on the thinnest
+    jittered triangles of the 512x512 mesh (dt = 1 s is unstable there, on the CPU oracle too)."""
+    return manufactured(nq, p=2, rk=(3, 3), dt=dt, jitter=0.2, seed=2, precision=precision)
 
 
 def thacker_params(h0=10.0, a=3000.0, eta0=2.0, g=9.81):

@@ -161,6 +161,7 @@ struct dgsw_rkdg_s {
     DevTables<double> tab_d;
     DevTables<float> tab_f;
     DBuf<L2Rule> l2rule;
+    DBuf<double> staging;  // FP64 host-layout state for the host API (allocated on first use)
     double last_ms = 0.0;
     int64_t last_launches = 0;
     size_t smem_bytes = 0;
@@ -272,6 +273,7 @@ cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches) {
         advance_clock_kernel<<<1, 1, 0, h->stream>>>(h->clock.p, h->cfg.dt);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
+        ++launches;
         std::swap(h->Q[0], h->Q[h->ns]);  // UpdateState's swap of q_0 and q_ns
         h->qswap ^= 1;
         s_out = 0;
@@ -315,39 +317,42 @@ void destroy_graphs(dgsw_rkdg_s* h) {
         }
 }
 
-// element-major host state [ref][var][dof] <-> device component-major SoA in device order
-template <typename Real>
-void host_to_dev_layout(dgsw_rkdg_s* h, const double* q, std::vector<Real>& out) {
-    const int nd = h->nd;
-    out.assign((size_t)3 * nd * h->ne_pad, Real(0));
-    for (int64_t d = 0; d < h->ne; ++d) {
-        int64_t r = h->tiling.ref_of_dev[d];
-        for (int c = 0; c < 3 * nd; ++c) out[(size_t)c * h->ne_pad + d] = (Real)q[r * 3 * nd + c];
-    }
+int ensure_staging(dgsw_rkdg_s* h) {
+    if (h->staging.p) return DGSW_OK;
+    cudaError_t e = h->staging.alloc((size_t)h->ne * 3 * h->nd);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("staging alloc: ") + cudaGetErrorString(e));
+    h->device_bytes += (int64_t)h->ne * 3 * h->nd * 8;
+    return DGSW_OK;
 }
 
-template <typename Real>
-void dev_to_host_layout(dgsw_rkdg_s* h, const std::vector<Real>& in, double* q) {
-    const int nd = h->nd;
-    for (int64_t d = 0; d < h->ne; ++d) {
-        int64_t r = h->tiling.ref_of_dev[d];
-        for (int c = 0; c < 3 * nd; ++c) q[r * 3 * nd + c] = (double)in[(size_t)c * h->ne_pad + d];
-    }
-}
-
+// host FP64 [ref][var][dof] -> one DMA into the staging buffer -> device permute + convert
 int upload_state(dgsw_rkdg_s* h, const double* q) {
-    const size_t n = (size_t)3 * h->nd * h->ne_pad;
-    if (h->fp32) {
-        std::vector<float> buf;
-        host_to_dev_layout<float>(h, q, buf);
-        CUDA_TRY(cudaMemcpyAsync(h->Q[h->stage], buf.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-        CUDA_TRY(cudaStreamSynchronize(h->stream));
-    } else {
-        std::vector<double> buf;
-        host_to_dev_layout<double>(h, q, buf);
-        CUDA_TRY(cudaMemcpyAsync(h->Q[h->stage], buf.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        CUDA_TRY(cudaStreamSynchronize(h->stream));
-    }
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    const size_t bytes = (size_t)h->ne * 3 * h->nd * sizeof(double);
+    CUDA_TRY(cudaMemcpyAsync(h->staging.p, q, bytes, cudaMemcpyHostToDevice, h->stream));
+    cudaError_t e = h->fp32 ? launch_permute_in<double, float>(h->staging.p, (float*)h->Q[h->stage], h->ref_of_dev.p,
+                                                               (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream)
+                            : launch_permute_in<double, double>(h->staging.p, (double*)h->Q[h->stage], h->ref_of_dev.p,
+                                                                (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("set_state: ") + cudaGetErrorString(e));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DGSW_OK;
+}
+
+int download_state(dgsw_rkdg_s* h, double* q) {
+    int rc = ensure_staging(h);
+    if (rc) return rc;
+    cudaError_t e = h->fp32 ? launch_permute_out<float, double>((const float*)h->Q[h->stage], h->staging.p,
+                                                                h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
+                                                                h->stream)
+                            : launch_permute_out<double, double>((const double*)h->Q[h->stage], h->staging.p,
+                                                                 h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
+                                                                 h->stream);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("get_state: ") + cudaGetErrorString(e));
+    const size_t bytes = (size_t)h->ne * 3 * h->nd * sizeof(double);
+    CUDA_TRY(cudaMemcpyAsync(q, h->staging.p, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
     return DGSW_OK;
 }
 
@@ -470,6 +475,10 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
     h->ne = h->topo.ne;
     h->nn = mesh->n_nodes;
     h->ne_pad = (h->ne + 31) / 32 * 32;
+    if ((int64_t)3 * h->nd * h->ne_pad >= ((int64_t)1 << 31)) {
+        delete h;
+        return fail(DGSW_ERR_UNSUPPORTED, "mesh too large for 32-bit state indexing on one handle");
+    }
     h->fp32 = cfg->precision == DGSW_FP32;
     h->real_size = h->fp32 ? sizeof(float) : sizeof(double);
     if (cfg->wetting_drying) h->h_o_thr = 1.0e6 * cfg->h_o * std::numeric_limits<double>::epsilon();
@@ -634,6 +643,7 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     h->clock.release();
     h->red.release();
     h->l2rule.release();
+    h->staging.release();
     h->limited.release();
     h->nbr.release();
     h->baryctr.release();
@@ -691,19 +701,7 @@ int32_t dgsw_rkdg_set_state(dgsw_handle h, const double* q) {
 int32_t dgsw_rkdg_get_state(dgsw_handle h, double* q) {
     if (!h || !q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
-    const size_t n = (size_t)3 * h->nd * h->ne_pad;
-    if (h->fp32) {
-        std::vector<float> buf(n);
-        CUDA_TRY(cudaMemcpyAsync(buf.data(), h->Q[h->stage], n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-        CUDA_TRY(cudaStreamSynchronize(h->stream));
-        dev_to_host_layout<float>(h, buf, q);
-    } else {
-        std::vector<double> buf(n);
-        CUDA_TRY(cudaMemcpyAsync(buf.data(), h->Q[h->stage], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        CUDA_TRY(cudaStreamSynchronize(h->stream));
-        dev_to_host_layout<double>(h, buf, q);
-    }
-    return DGSW_OK;
+    return download_state(h, q);
 }
 
 int32_t dgsw_rkdg_set_wet(dgsw_handle h, const uint8_t* wet) {
@@ -735,10 +733,12 @@ int32_t dgsw_rkdg_get_limited(dgsw_handle h, uint8_t* flags) {
 int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
     if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
-    cudaError_t e = h->fp32 ? launch_permute_in<float>((const float*)d_q, (float*)h->Q[h->stage], h->ref_of_dev.p,
-                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream)
-                            : launch_permute_in<double>((const double*)d_q, (double*)h->Q[h->stage], h->ref_of_dev.p,
-                                                        (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    cudaError_t e = h->fp32 ? launch_permute_in<float, float>((const float*)d_q, (float*)h->Q[h->stage],
+                                                              h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
+                                                              h->stream)
+                            : launch_permute_in<double, double>((const double*)d_q, (double*)h->Q[h->stage],
+                                                                h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
+                                                                h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("set_state_device: ") + cudaGetErrorString(e));
     return DGSW_OK;
 }
@@ -746,10 +746,12 @@ int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
 int32_t dgsw_rkdg_get_state_device(dgsw_handle h, void* d_q) {
     if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
-    cudaError_t e = h->fp32 ? launch_permute_out<float>((const float*)h->Q[h->stage], (float*)d_q, h->ref_of_dev.p,
-                                                        (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream)
-                            : launch_permute_out<double>((const double*)h->Q[h->stage], (double*)d_q, h->ref_of_dev.p,
-                                                         (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    cudaError_t e = h->fp32 ? launch_permute_out<float, float>((const float*)h->Q[h->stage], (float*)d_q,
+                                                               h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
+                                                               h->stream)
+                            : launch_permute_out<double, double>((const double*)h->Q[h->stage], (double*)d_q,
+                                                                 h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad,
+                                                                 3 * h->nd, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("get_state_device: ") + cudaGetErrorString(e));
     return DGSW_OK;
 }
@@ -806,6 +808,7 @@ int32_t dgsw_rkdg_step(dgsw_handle h, int32_t nsteps) {
                 if (s + 1 == h->ns) {
                     std::swap(h->Q[0], h->Q[h->ns]);
                     h->qswap ^= 1;
+                    ++launches;  // clock update
                 }
                 ++launches;
                 if (h->cfg.slope_limiting) ++launches;

@@ -231,4 +231,128 @@ DGSW_HD dgsw_fn3 dgsw_fn_source(int id, const double* P, double t, double x, dou
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Split evaluation for the device: the time-only factors of a set are computed once per stage
+// (dgsw_fn_prepare), the space-dependent part per point in the kernel's precision (dgsw_fn_eval).
+// Same formulas as above; only the time factors are hoisted out of the point loop.
+// ---------------------------------------------------------------------------------------------
+struct dgsw_fn_time {
+    double t;
+    double s[6];
+};
+
+DGSW_HD dgsw_fn_time dgsw_fn_prepare(int id, const double* P, double t) {
+    dgsw_fn_time T;
+    T.t = t;
+    for (int i = 0; i < 6; ++i) T.s[i] = 0.0;
+    if (id == DGSW_FN_MANUFACTURED_SINE) {
+        const double w = fn_sine_omega(P);
+        T.s[0] = sin(w * t);
+        T.s[1] = cos(w * t);
+        T.s[2] = w;
+    } else if (id == DGSW_FN_THACKER_BOWL) {
+        const double h0 = P[0], eta0 = P[2];
+        const double hp = (h0 + eta0) * (h0 + eta0);
+        const double A = (hp - h0 * h0) / (hp + h0 * h0);
+        const double w = fn_thacker_omega(P);
+        T.s[0] = 1.0 - A * cos(w * t);  // den
+        T.s[1] = sin(w * t);
+        T.s[2] = A;
+        T.s[3] = w;
+    }
+    return T;
+}
+
+DGSW_HD void dgsw_sincos(double a, double* s, double* c) {
+#if defined(__CUDA_ARCH__)
+    sincos(a, s, c);
+#else
+    *s = sin(a);
+    *c = cos(a);
+#endif
+}
+DGSW_HD void dgsw_sincos(float a, float* s, float* c) {
+#if defined(__CUDA_ARCH__)
+    sincosf(a, s, c);
+#else
+    *s = sinf(a);
+    *c = cosf(a);
+#endif
+}
+
+// source = 0: ic_q / true_q;  source = 1: source_q.  R = double or float.
+template <typename R>
+DGSW_HD void dgsw_fn_eval(int id, const double* P, const dgsw_fn_time& T, int source, R x, R y, R out[3]) {
+    out[0] = out[1] = out[2] = R(0);
+    if (id == DGSW_FN_MANUFACTURED_SINE) {
+        const R k = (R)(2.0 * M_PI / P[0]);
+        const R A = (R)P[1], w = (R)T.s[2];
+        const R B = (R)(P[1] * T.s[2] / (2.0 * (2.0 * M_PI / P[0])));
+        const R st = (R)T.s[0], ct = (R)T.s[1];
+        R sx, cx, sy, cy;
+        dgsw_sincos(k * x, &sx, &cx);
+        dgsw_sincos(k * y, &sy, &cy);
+        const R ze = A * sx * cy * ct;
+        const R qx = -B * cx * cy * st;
+        const R qy = B * sx * sy * st;
+        if (!source) {
+            out[0] = ze;
+            out[1] = qx;
+            out[2] = qy;
+            return;
+        }
+        const R zex = A * k * cx * cy * ct, zey = -A * k * sx * sy * ct, zet = -A * w * sx * cy * st;
+        const R qxx = B * k * sx * cy * st, qxy = B * k * cx * sy * st, qxt = -B * w * cx * cy * ct;
+        const R qyx = B * k * cx * sy * st, qyy = B * k * sx * cy * st, qyt = B * w * sx * sy * ct;
+        const R g = (R)P[4];
+        const R h = ze + (R)P[2];
+        const R ih = R(1) / h;
+        const R ih2 = ih * ih;
+        out[0] = zet + qxx + qyy;
+        out[1] = qxt + (R(2) * qx * qxx * ih - qx * qx * zex * ih2) + ((qxy * qy + qx * qyy) * ih - qx * qy * zey * ih2) +
+                 g * h * zex;
+        out[2] = qyt + ((qxx * qy + qx * qyx) * ih - qx * qy * zex * ih2) + (R(2) * qy * qyy * ih - qy * qy * zey * ih2) +
+                 g * h * zey;
+        return;
+    }
+    if (id == DGSW_FN_THACKER_BOWL) {
+        if (source) return;
+        const R h0 = (R)P[0], a = (R)P[1];
+        const R dx = x - (R)P[4], dy = y - (R)P[5];
+        const R r2 = dx * dx + dy * dy;
+        const R den = (R)T.s[0], A = (R)T.s[2];
+        const R ze = h0 * ((R)sqrt(1.0 - T.s[2] * T.s[2]) / den - R(1) - r2 / (a * a) * ((R(1) - A * A) / (den * den) - R(1)));
+        const R b = h0 * (R(1) - r2 / (a * a));
+        if (ze + b > R(0)) {
+            const R fac = (R)T.s[3] * A * (R)T.s[1] / (R(2) * den);
+            out[0] = ze;
+            out[1] = (ze + b) * dx * fac;
+            out[2] = (ze + b) * dy * fac;
+        } else {
+            out[0] = -b;
+        }
+        return;
+    }
+    if (id == DGSW_FN_GAUSSIAN_HUMPS) {
+        if (source) return;
+        R ze = (R)P[0];
+        for (int i = 0; i < 3; ++i) {
+            const R wd = (R)P[4 + 4 * i];
+            if (wd > R(0)) {
+                const R dx = x - (R)P[2 + 4 * i], dy = y - (R)P[3 + 4 * i];
+                ze += (R)P[1 + 4 * i] * (R)exp((double)(-(dx * dx + dy * dy) / (R(2) * wd * wd)));
+            }
+        }
+        out[0] = ze;
+        return;
+    }
+    if (id == DGSW_FN_REFERENCE_MANUFACTURED) {
+        const dgsw_fn3 f = source ? fn_refmms_source(T.t, (double)x, (double)y) : fn_refmms_true(T.t, (double)x, (double)y);
+        out[0] = (R)f.ze;
+        out[1] = (R)f.qx;
+        out[2] = (R)f.qy;
+    }
+}
+
+
 #endif

@@ -126,36 +126,37 @@ cudaError_t launch_reduction(const ReduceArgs<Real>& R, int p, int what, cudaStr
     return cudaGetLastError();
 }
 
-// element-major [ref][comp] <-> component-major [comp][ne_pad] in device order
-template <typename Real>
-__global__ void permute_in_kernel(const Real* __restrict__ src, Real* __restrict__ dst, const int* __restrict__ ref_of_dev,
+// element-major [ref][comp] <-> component-major [comp][ne_pad] in device order, with a precision
+// conversion (the host-facing state is FP64 in every precision)
+template <typename Src, typename Dst>
+__global__ void permute_in_kernel(const Src* __restrict__ src, Dst* __restrict__ dst, const int* __restrict__ ref_of_dev,
                                   int ne, int ne_pad, int ncomp) {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= ne) return;
     const int r = ref_of_dev[d];
-    for (int c = 0; c < ncomp; ++c) dst[(size_t)c * ne_pad + d] = src[(size_t)r * ncomp + c];
+    for (int c = 0; c < ncomp; ++c) dst[c * ne_pad + d] = (Dst)src[(size_t)r * ncomp + c];
 }
 
-template <typename Real>
-__global__ void permute_out_kernel(const Real* __restrict__ src, Real* __restrict__ dst,
+template <typename Src, typename Dst>
+__global__ void permute_out_kernel(const Src* __restrict__ src, Dst* __restrict__ dst,
                                    const int* __restrict__ ref_of_dev, int ne, int ne_pad, int ncomp) {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= ne) return;
     const int r = ref_of_dev[d];
-    for (int c = 0; c < ncomp; ++c) dst[(size_t)r * ncomp + c] = src[(size_t)c * ne_pad + d];
+    for (int c = 0; c < ncomp; ++c) dst[(size_t)r * ncomp + c] = (Dst)src[c * ne_pad + d];
 }
 
-template <typename Real>
-cudaError_t launch_permute_in(const Real* src, Real* dst, const int* ref_of_dev, int ne, int ne_pad, int ncomp,
+template <typename Src, typename Dst>
+cudaError_t launch_permute_in(const Src* src, Dst* dst, const int* ref_of_dev, int ne, int ne_pad, int ncomp,
                               cudaStream_t s) {
-    permute_in_kernel<Real><<<(ne + 255) / 256, 256, 0, s>>>(src, dst, ref_of_dev, ne, ne_pad, ncomp);
+    permute_in_kernel<Src, Dst><<<(ne + 255) / 256, 256, 0, s>>>(src, dst, ref_of_dev, ne, ne_pad, ncomp);
     return cudaGetLastError();
 }
 
-template <typename Real>
-cudaError_t launch_permute_out(const Real* src, Real* dst, const int* ref_of_dev, int ne, int ne_pad, int ncomp,
+template <typename Src, typename Dst>
+cudaError_t launch_permute_out(const Src* src, Dst* dst, const int* ref_of_dev, int ne, int ne_pad, int ncomp,
                                cudaStream_t s) {
-    permute_out_kernel<Real><<<(ne + 255) / 256, 256, 0, s>>>(src, dst, ref_of_dev, ne, ne_pad, ncomp);
+    permute_out_kernel<Src, Dst><<<(ne + 255) / 256, 256, 0, s>>>(src, dst, ref_of_dev, ne, ne_pad, ncomp);
     return cudaGetLastError();
 }
 

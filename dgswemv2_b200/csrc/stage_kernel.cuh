@@ -136,6 +136,37 @@ __device__ __forceinline__ void land_flux(Real g, Real nx, Real ny, const Real q
     llf_flux<Real>(g, qin, qex, bath, sp, nx, ny, F);
 }
 
+// Wet/dry fix-ups of ISP::Internal (rkdg_swe_is_internal.hpp:47-90) for an interface whose LLF
+// ze-flux exceeds 1e-12 in magnitude with one side dry. Out of line: taken on few edges only.
+template <typename Real>
+__device__ __noinline__ void wd_fixup(Real g, const Real* qi, const Real* qe, Real bi, Real be, Real sp, Real nx, Real ny,
+                                      bool wa, bool wb, Real* Fi, Real* Fe) {
+    if (Fi[0] > Real(1e-12)) {
+        if (!wa) {  // water flowing from the dry in-side: zero flux there, reflective wall on the ex side
+            Fi[0] = Fi[1] = Fi[2] = Real(0);
+            land_flux<Real>(g, -nx, -ny, qe, be, sp, Fe);
+        } else if (!wb) {  // water flowing into the dry ex-side: gravity-free LLF there
+            llf_flux<Real>(Real(0), qe, qi, be, sp, -nx, -ny, Fe);
+            Fe[0] = -Fi[0];
+        }
+    } else if (Fi[0] < Real(-1e-12)) {
+        if (!wb) {
+            Fe[0] = Fe[1] = Fe[2] = Real(0);
+            land_flux<Real>(g, nx, ny, qi, bi, sp, Fi);
+        } else if (!wa) {
+            llf_flux<Real>(Real(0), qi, qe, bi, sp, nx, ny, Fi);
+            Fi[0] = -Fe[0];
+        }
+    }
+}
+
+// analytic function sets evaluated out of line (one copy per kernel)
+template <typename Real>
+__device__ __noinline__ void fn_eval_dev(int id, const double* P, const dgsw_fn_time* T, int source, Real x, Real y,
+                                         Real* out) {
+    dgsw_fn_eval<Real>(id, P, *T, source, x, y, out);
+}
+
 // ------------------------------------------------------------------------------------------------
 // wetting/drying of one p>=1 element on its vertex values, swe_post_wet_dry.hpp:6-145, in FP64.
 // qv: modal state (first three modes carry the linear part); returns the new wet flag and writes
@@ -280,10 +311,15 @@ struct Smem {
     static __host__ __device__ size_t bytes(int tile, int me) { return off_flag(tile, me) + al((size_t)me); }
 };
 
+// resident CTAs per SM the register budget is sized for
+template <int P, typename Real, int TILE>
+struct MinBlocks {
+    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? 4 : 2) : (TILE == 128 ? 3 : 1);
+};
+
 template <int P, typename Real, bool WD, bool FSRC, int TILE>
-__global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> A, int max_edges) {
+__global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_edges) {
     constexpr int ND = Dims<P>::ND, NQ = Dims<P>::NQ, NG = Dims<P>::NG;
-    constexpr int NFC = Smem<P, Real, WD>::NFC;
     const DevTables<Real>& T = A.T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using SM = Smem<P, Real, WD>;
@@ -306,6 +342,7 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
     const double t_stage = A.clock->t + A.drk_s;  // ESSPRKStepper::GetTimeAtCurrentStage
     const Real g = (Real)A.g;
     const Real* __restrict__ qs = A.qk[A.nterms - 1];  // this stage's state
+    const dgsw_fn_time FT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
 
     // face tables are indexed by per-thread face numbers: keep them in shared memory
     for (int i = tid; i < 3 * ND * NG; i += TILE) sfphi[i] = T.fphi[i / (ND * NG)][i % (ND * NG)];
@@ -337,18 +374,19 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
         Real q[3][ND], b[ND];
 #pragma unroll
         for (int c = 0; c < 3 * ND; ++c) {
-            const Real val = qs[(size_t)c * A.ne_pad + d];
+            const Real val = qs[c * A.ne_pad + d];
             q[c / ND][c % ND] = val;
             sq[c * TILE + tid] = val;
         }
 #pragma unroll
         for (int k = 0; k < ND; ++k) {
-            b[k] = A.bath[(size_t)k * A.ne_pad + d];
+            b[k] = A.bath[k * A.ne_pad + d];
             sbath[k * TILE + tid] = b[k];
         }
         wet = A.wet_in[d] != 0;
         swet[tid] = wet ? 1 : 0;
         if (wet) {
+            // unrolled: every table entry becomes an immediate constant-bank operand
 #pragma unroll
             for (int gp = 0; gp < NQ; ++gp) {
                 Real qg[3], bg = Real(0), db0 = Real(0), db1 = Real(0);
@@ -387,10 +425,11 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
                 const Real dby = db0 * Ji01 + db1 * Ji11;
                 Real S[3] = {Real(0), g * (dbx * qg[0]), g * (dby * qg[0])};
                 if (FSRC) {
-                    const dgsw_fn3 f = dgsw_fn_source(A.fn_set, A.fn_params, t_stage, xg, yg);
-                    S[0] += (Real)f.ze;
-                    S[1] += (Real)f.qx;
-                    S[2] += (Real)f.qy;
+                    Real fs[3];
+                    fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, (Real)xg, (Real)yg, fs);
+                    S[0] += fs[0];
+                    S[1] += fs[1];
+                    S[2] += fs[2];
                 }
                 // int F . grad(phi) = sum_gp sum_z (F_x J^-1(z,x) + F_y J^-1(z,y)) dphi_z w
 #pragma unroll
@@ -450,11 +489,11 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
         for (int k = 0; k < ND; ++k) {
 #pragma unroll
             for (int v = 0; v < 3; ++v) {
-                const Real c = a_loc ? sq[(v * ND + k) * TILE + la] : qs[(size_t)(v * ND + k) * A.ne_pad + ea];
+                const Real c = a_loc ? sq[(v * ND + k) * TILE + la] : qs[(v * ND + k) * A.ne_pad + ea];
 #pragma unroll
                 for (int gp = 0; gp < NG; ++gp) ti[v][gp] += c * fta[k * NG + gp];
             }
-            const Real c = a_loc ? sbath[k * TILE + la] : A.bath[(size_t)k * A.ne_pad + ea];
+            const Real c = a_loc ? sbath[k * TILE + la] : A.bath[k * A.ne_pad + ea];
 #pragma unroll
             for (int gp = 0; gp < NG; ++gp) bi[gp] += c * fta[k * NG + gp];
         }
@@ -463,12 +502,12 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
             for (int k = 0; k < ND; ++k) {
 #pragma unroll
                 for (int v = 0; v < 3; ++v) {
-                    const Real c = b_loc ? sq[(v * ND + k) * TILE + lb] : qs[(size_t)(v * ND + k) * A.ne_pad + eb];
+                    const Real c = b_loc ? sq[(v * ND + k) * TILE + lb] : qs[(v * ND + k) * A.ne_pad + eb];
 #pragma unroll
                     for (int gp = 0; gp < NG; ++gp) te[v][gp] += c * ftb[k * NG + (NG - 1 - gp)];
                 }
                 if (WD) {
-                    const Real c = b_loc ? sbath[k * TILE + lb] : A.bath[(size_t)k * A.ne_pad + eb];
+                    const Real c = b_loc ? sbath[k * TILE + lb] : A.bath[k * A.ne_pad + eb];
 #pragma unroll
                     for (int gp = 0; gp < NG; ++gp) be[gp] += c * ftb[k * NG + (NG - 1 - gp)];
                 }
@@ -491,39 +530,30 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
         for (int gp = 0; gp < NG; ++gp) {
             if (A.spherical) sp = (Real)(A.sp_cos_lat0 / cos(yg[gp] / A.sp_R));
             const Real qi[3] = {ti[0][gp], ti[1][gp], ti[2][gp]};
-            Real Fi[3];
+            Real qe[3];
             if (kind == 0) {
-                const Real qe[3] = {te[0][gp], te[1][gp], te[2][gp]};
-                llf_flux<Real>(g, qi, qe, bi[gp], sp, nx, ny, Fi);
-                if (WD) {
-                    Real Fe[3] = {-Fi[0], -Fi[1], -Fi[2]};
-                    // ISP::Internal wet/dry fix-ups (rkdg_swe_is_internal.hpp:47-90)
-                    if (Fi[0] > Real(1e-12)) {
-                        if (!wa) {
-                            Fi[0] = Fi[1] = Fi[2] = Real(0);
-                            land_flux<Real>(g, -nx, -ny, qe, be[gp], sp, Fe);
-                        } else if (!wb) {
-                            llf_flux<Real>(Real(0), qe, qi, be[gp], sp, -nx, -ny, Fe);
-                            Fe[0] = -Fi[0];
-                        }
-                    } else if (Fi[0] < Real(-1e-12)) {
-                        if (!wb) {
-                            Fe[0] = Fe[1] = Fe[2] = Real(0);
-                            land_flux<Real>(g, nx, ny, qi, bi[gp], sp, Fi);
-                        } else if (!wa) {
-                            llf_flux<Real>(Real(0), qi, qe, bi[gp], sp, nx, ny, Fi);
-                            Fi[0] = -Fe[0];
-                        }
-                    }
-#pragma unroll
-                    for (int v = 0; v < 3; ++v) sF[((3 + v) * NG + gp) * max_edges + le] = Fe[v];
-                }
+                qe[0] = te[0][gp];
+                qe[1] = te[1][gp];
+                qe[2] = te[2][gp];
             } else if (kind == 1) {
-                land_flux<Real>(g, nx, ny, qi, bi[gp], sp, Fi);
+                // BC::Land ghost state: normal momentum mirrored (rkdg_swe_bc_land.hpp:44-56)
+                const Real tx = -ny, ty = nx;
+                const Real qn_ex = -(qi[1] * nx + qi[2] * ny);
+                const Real qt_ex = qi[1] * tx + qi[2] * ty;
+                qe[0] = qi[0];
+                qe[1] = qn_ex * nx + qt_ex * tx;
+                qe[2] = qn_ex * ny + qt_ex * ty;
             } else {
-                const dgsw_fn3 f = dgsw_fn_ic(A.fn_set, A.fn_params, t_stage, xg[gp], yg[gp]);
-                const Real qe[3] = {(Real)f.ze, (Real)f.qx, (Real)f.qy};
-                llf_flux<Real>(g, qi, qe, bi[gp], sp, nx, ny, Fi);
+                // BC::Function ghost state: ic_q(t, x_gp) (rkdg_swe_bc_function.hpp:33-50)
+                fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 0, (Real)xg[gp], (Real)yg[gp], qe);
+            }
+            Real Fi[3];
+            llf_flux<Real>(g, qi, qe, bi[gp], sp, nx, ny, Fi);
+            if (WD && kind == 0) {
+                Real Fe[3] = {-Fi[0], -Fi[1], -Fi[2]};
+                if (!(wa && wb)) wd_fixup<Real>(g, qi, qe, bi[gp], be[gp], sp, nx, ny, wa, wb, Fi, Fe);
+#pragma unroll
+                for (int v = 0; v < 3; ++v) sF[((3 + v) * NG + gp) * max_edges + le] = Fe[v];
             }
 #pragma unroll
             for (int v = 0; v < 3; ++v) sF[(v * NG + gp) * max_edges + le] = Fi[v];
@@ -574,7 +604,7 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
 #pragma unroll
         for (int k = 0; k < ND; ++k) {
             const Real sol = rhs[v][k] * (Real)(T.minv[k] * iaJ);
-            const size_t idx = (size_t)(v * ND + k) * A.ne_pad + d;
+            const int idx = (v * ND + k) * A.ne_pad + d;
             if (A.store_sol) A.sol_out[idx] = sol;
             Real acc = Real(0);
             for (int j = 0; j < A.nterms - 1; ++j) {
@@ -597,7 +627,7 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
 #pragma unroll
         for (int k = 0; k < ND; ++k) {
             has_nan |= isnan((double)qn[v][k]);
-            A.q_out[(size_t)(v * ND + k) * A.ne_pad + d] = qn[v][k];
+            A.q_out[(v * ND + k) * A.ne_pad + d] = qn[v][k];
         }
     A.wet_out[d] = wet_new ? 1 : 0;
     if (A.baryctr) {
@@ -607,7 +637,7 @@ __global__ void __launch_bounds__(TILE) rkdg_stage_kernel(const StageArgs<Real> 
         for (int v = 0; v < 3; ++v) {
             const double a = qn[v][0], b = qn[v][1], c = qn[v][2];
             const double l0 = a - b - c, l1 = a - b + c, l2 = a + 2.0 * b;
-            A.baryctr[(size_t)v * A.ne_pad + d] = l0 * (1.0 / 3.0) + l1 * (1.0 / 3.0) + l2 * (1.0 / 3.0);
+            A.baryctr[v * A.ne_pad + d] = l0 * (1.0 / 3.0) + l1 * (1.0 / 3.0) + l2 * (1.0 / 3.0);
         }
     }
     if (has_nan) {
