@@ -50,48 +50,6 @@ struct DBuf {
     }
 };
 
-// host copies of the per-order tables in both precisions
-int make_dev_tables(int p, DevTables<double>& d, DevTables<float>& f, std::string& err) {
-    Tables t;
-    int rc = build_tables(p, t, err);
-    if (rc) return rc;
-    std::memset(&d, 0, sizeof(d));
-    std::memset(&f, 0, sizeof(f));
-    for (int k = 0; k < t.nd; ++k)
-        for (int gp = 0; gp < t.nq; ++gp) {
-            d.phi[k * t.nq + gp] = t.phi[k * t.nq + gp];
-            d.dphi[0][k * t.nq + gp] = t.dphi[0][k * t.nq + gp];
-            d.dphi[1][k * t.nq + gp] = t.dphi[1][k * t.nq + gp];
-            d.mz[0][gp * t.nd + k] = t.mz[0][gp * t.nd + k];
-            d.mz[1][gp * t.nd + k] = t.mz[1][gp * t.nd + k];
-            d.phiw[gp * t.nd + k] = t.phiw[gp * t.nd + k];
-        }
-    for (int n = 0; n < 3; ++n)
-        for (int gp = 0; gp < t.nq; ++gp) d.psi[n][gp] = t.psi[n][gp];
-    for (int fc = 0; fc < 3; ++fc) {
-        for (int i = 0; i < t.nd * t.ng; ++i) d.fphi[fc][i] = t.fphi[fc][i];
-        for (int n = 0; n < 3; ++n)
-            for (int g = 0; g < t.ng; ++g) d.fpsi[fc][n][g] = t.fpsi[fc][n][g];
-    }
-    for (int g = 0; g < t.ng; ++g) d.gw[g] = t.gw[g];
-    for (int k = 0; k < t.nd; ++k) d.minv[k] = t.minv[k];
-    for (int i = 0; i < 36; ++i) {
-        f.phi[i] = (float)d.phi[i];
-        f.dphi[0][i] = (float)d.dphi[0][i];
-        f.dphi[1][i] = (float)d.dphi[1][i];
-        f.mz[0][i] = (float)d.mz[0][i];
-        f.mz[1][i] = (float)d.mz[1][i];
-        f.phiw[i] = (float)d.phiw[i];
-    }
-    std::memcpy(f.psi, d.psi, sizeof(d.psi));
-    std::memcpy(f.fpsi, d.fpsi, sizeof(d.fpsi));
-    for (int fc = 0; fc < 3; ++fc)
-        for (int i = 0; i < 18; ++i) f.fphi[fc][i] = (float)d.fphi[fc][i];
-    for (int g = 0; g < 3; ++g) f.gw[g] = (float)d.gw[g];
-    std::memcpy(f.minv, d.minv, sizeof(d.minv));
-    return DGSW_OK;
-}
-
 int make_l2_rule(L2Rule& R, std::string& err) {
     Rule2D r = triangle_rule(20);
     if ((int)r.w.size() != L2_NPT) {
@@ -134,7 +92,11 @@ struct dgsw_rkdg_s {
     size_t real_size = 8;
     std::vector<void*> Q;    // ns+1 stage states
     std::vector<void*> SOL;  // stored stage solutions (only where needed)
-    void* bath = nullptr;
+    void* bath = nullptr;  // [3][ne_pad] bathymetry modes of the linear part
+    void* geo = nullptr;   // [5][ne_pad] J^-1 and |J|
+    void* egeo = nullptr;  // [3][n_edges] edge normal and half length
+    DBuf<int2> halo;
+    DBuf<int> tile_halo_off;
     DBuf<int> enodes, tile_edge_off, ref_of_dev;
     DBuf<int2> eslot;
     DBuf<int4> edges;
@@ -158,8 +120,6 @@ struct dgsw_rkdg_s {
     cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
     int qswap = 0;  // parity of the q_0 <-> q_ns swaps so far
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    DevTables<double> tab_d;
-    DevTables<float> tab_f;
     DBuf<L2Rule> l2rule;
     DBuf<double> staging;  // FP64 host-layout state for the host API (allocated on first use)
     double last_ms = 0.0;
@@ -193,10 +153,15 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.sol_out = (Real*)h->SOL[s];
     A.q_out = (Real*)h->Q[s + 1];
     A.bath = (const Real*)h->bath;
+    A.geo = (const Real*)h->geo;
     A.enodes = h->enodes.p;
     A.eslot = h->eslot.p;
     A.edges = h->edges.p;
+    A.egeo = (const Real*)h->egeo;
     A.tile_edge_off = h->tile_edge_off.p;
+    A.halo = h->halo.p;
+    A.tile_halo_off = h->tile_halo_off.p;
+    A.n_edges = (int)(h->tiling.edges.size() / 4);
     A.xy = h->xy.p;
     A.nz = h->nz.p;
     A.ref_of_dev = h->ref_of_dev.p;
@@ -216,25 +181,21 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.sp_R = h->cfg.sp_R;
 }
 
-void set_tables(dgsw_rkdg_s* h, StageArgs<double>& A) { A.T = h->tab_d; }
-void set_tables(dgsw_rkdg_s* h, StageArgs<float>& A) { A.T = h->tab_f; }
-
 cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, bool wd, bool fs) {
-    const int nt = (int)h->tiling.ntiles, me = h->tiling.max_edges;
-    return h->cfg.p == 1 ? launch_stage_p1_f64(A, h->tile, nt, me, wd, fs, h->stream)
-                         : launch_stage_p2_f64(A, h->tile, nt, me, wd, fs, h->stream);
+    const int nt = (int)h->tiling.ntiles, mh = h->tiling.max_halo, me = h->tiling.max_edges;
+    return h->cfg.p == 1 ? launch_stage_p1_f64(A, h->tile, nt, mh, me, wd, fs, h->stream)
+                         : launch_stage_p2_f64(A, h->tile, nt, mh, me, wd, fs, h->stream);
 }
 cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<float>& A, bool wd, bool fs) {
-    const int nt = (int)h->tiling.ntiles, me = h->tiling.max_edges;
-    return h->cfg.p == 1 ? launch_stage_p1_f32(A, h->tile, nt, me, wd, fs, h->stream)
-                         : launch_stage_p2_f32(A, h->tile, nt, me, wd, fs, h->stream);
+    const int nt = (int)h->tiling.ntiles, mh = h->tiling.max_halo, me = h->tiling.max_edges;
+    return h->cfg.p == 1 ? launch_stage_p1_f32(A, h->tile, nt, mh, me, wd, fs, h->stream)
+                         : launch_stage_p2_f32(A, h->tile, nt, mh, me, wd, fs, h->stream);
 }
 
 template <typename Real>
 cudaError_t launch_stage(dgsw_rkdg_s* h, int s) {
     StageArgs<Real> A;
     fill_stage_args<Real>(h, s, A);
-    set_tables(h, A);
     A.wet_in = h->wet[h->wet_cur].p;
     A.wet_out = h->wet[1 - h->wet_cur].p;
     return launch_stage_any(h, A, h->cfg.wetting_drying != 0, h->cfg.function_source != 0);
@@ -506,11 +467,6 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
         delete h;
         return fail(DGSW_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     }
-    rc = make_dev_tables(cfg->p, h->tab_d, h->tab_f, err);
-    if (rc) {
-        delete h;
-        return fail(rc, err);
-    }
     auto cleanup_fail = [&](const std::string& what, cudaError_t ce) {
         dgsw_rkdg_destroy(h);
         return fail(DGSW_ERR_CUDA, what + ": " + cudaGetErrorString(ce));
@@ -533,15 +489,23 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
             if ((e = cudaMalloc(&h->SOL[s], state_bytes)) != cudaSuccess) return cleanup_fail("sol alloc", e);
             h->device_bytes += state_bytes;
         }
-    const size_t bath_bytes = (size_t)h->nd * h->ne_pad * h->real_size;
+    const size_t bath_bytes = (size_t)3 * h->ne_pad * h->real_size;
     if ((e = cudaMalloc(&h->bath, bath_bytes)) != cudaSuccess) return cleanup_fail("bath alloc", e);
     h->device_bytes += bath_bytes;
+    const size_t geo_bytes = (size_t)5 * h->ne_pad * h->real_size;
+    if ((e = cudaMalloc(&h->geo, geo_bytes)) != cudaSuccess) return cleanup_fail("geometry alloc", e);
+    h->device_bytes += geo_bytes;
+    const size_t n_edges = h->tiling.edges.size() / 4;
+    const size_t egeo_bytes = (size_t)3 * std::max<size_t>(n_edges, 1) * h->real_size;
+    if ((e = cudaMalloc(&h->egeo, egeo_bytes)) != cudaSuccess) return cleanup_fail("edge geometry alloc", e);
+    h->device_bytes += egeo_bytes;
     // static mesh data in device order
     {
         std::vector<int> en((size_t)3 * h->ne_pad, 0);
         std::vector<double> bathm;
         project_bathymetry(h->topo, h->node_xyz.data(), h->tb, bathm);
-        std::vector<double> bdev((size_t)h->nd * h->ne_pad, 0.0);
+        std::vector<double> bdev((size_t)3 * h->ne_pad, 0.0);
+        std::vector<double> gdev((size_t)5 * h->ne_pad, 0.0);
         std::vector<int> nb((size_t)3 * h->ne_pad, -1);
         for (int64_t d = 0; d < h->ne; ++d) {
             int64_t r = h->tiling.ref_of_dev[d];
@@ -552,18 +516,36 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
                 nb[(size_t)v * h->ne_pad + d] =
                     n >= 0 ? h->tiling.dev_of_ref[n] : -2 - (int)h->topo.btype[3 * r + v];
             }
-            for (int k = 0; k < h->nd; ++k) bdev[(size_t)k * h->ne_pad + d] = bathm[r * h->nd + k];
+            // the projected bathymetry is linear: modes above the third are rounding residue
+            for (int k = 0; k < 3; ++k) bdev[(size_t)k * h->ne_pad + d] = bathm[r * h->nd + k];
+            double gg[5];
+            element_geometry(h->node_xyz.data(), &h->topo.enodes[3 * r], gg);
+            for (int c = 0; c < 5; ++c) gdev[(size_t)c * h->ne_pad + d] = gg[c];
         }
         if ((e = h->enodes.alloc(en.size())) != cudaSuccess) return cleanup_fail("alloc", e);
         cudaMemcpy(h->enodes.p, en.data(), en.size() * sizeof(int), cudaMemcpyHostToDevice);
         if ((e = h->nbr.alloc(nb.size())) != cudaSuccess) return cleanup_fail("alloc", e);
         cudaMemcpy(h->nbr.p, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice);
-        if (h->fp32) {
-            std::vector<float> bf(bdev.begin(), bdev.end());
-            cudaMemcpy(h->bath, bf.data(), bath_bytes, cudaMemcpyHostToDevice);
-        } else {
-            cudaMemcpy(h->bath, bdev.data(), bath_bytes, cudaMemcpyHostToDevice);
-        }
+        std::vector<double> edev((size_t)3 * std::max<size_t>(n_edges, 1), 0.0);
+        for (size_t i = 0; i < n_edges; ++i)
+            for (int c = 0; c < 3; ++c) edev[c * n_edges + i] = h->tiling.egeo[3 * i + c];
+        auto upload_real = [&](void* dst, const std::vector<double>& src) {
+            if (h->fp32) {
+                std::vector<float> f(src.begin(), src.end());
+                cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+            } else {
+                cudaMemcpy(dst, src.data(), src.size() * sizeof(double), cudaMemcpyHostToDevice);
+            }
+        };
+        upload_real(h->bath, bdev);
+        upload_real(h->geo, gdev);
+        upload_real(h->egeo, edev);
+        const size_t nhalo = h->tiling.halo.size() / 2;
+        if ((e = h->halo.alloc(std::max<size_t>(nhalo, 1))) != cudaSuccess) return cleanup_fail("alloc", e);
+        if (nhalo) cudaMemcpy(h->halo.p, h->tiling.halo.data(), nhalo * sizeof(int2), cudaMemcpyHostToDevice);
+        if ((e = h->tile_halo_off.alloc(h->tiling.tile_halo_off.size())) != cudaSuccess) return cleanup_fail("alloc", e);
+        cudaMemcpy(h->tile_halo_off.p, h->tiling.tile_halo_off.data(), h->tiling.tile_halo_off.size() * sizeof(int),
+                   cudaMemcpyHostToDevice);
         std::vector<double2> xy(h->nn);
         std::vector<double> nz(h->nn);
         for (int64_t i = 0; i < h->nn; ++i) {
@@ -574,9 +556,9 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
         cudaMemcpy(h->xy.p, xy.data(), h->nn * sizeof(double2), cudaMemcpyHostToDevice);
         if ((e = h->nz.alloc(h->nn)) != cudaSuccess) return cleanup_fail("alloc", e);
         cudaMemcpy(h->nz.p, nz.data(), h->nn * sizeof(double), cudaMemcpyHostToDevice);
-        const size_t nedges = h->tiling.edges.size() / 4;
-        if ((e = h->edges.alloc(nedges)) != cudaSuccess) return cleanup_fail("alloc", e);
-        cudaMemcpy(h->edges.p, h->tiling.edges.data(), nedges * sizeof(int4), cudaMemcpyHostToDevice);
+        const size_t nedges = n_edges;
+        if ((e = h->edges.alloc(std::max<size_t>(nedges, 1))) != cudaSuccess) return cleanup_fail("alloc", e);
+        if (nedges) cudaMemcpy(h->edges.p, h->tiling.edges.data(), nedges * sizeof(int4), cudaMemcpyHostToDevice);
         if ((e = h->tile_edge_off.alloc(h->tiling.tile_edge_off.size())) != cudaSuccess) return cleanup_fail("alloc", e);
         cudaMemcpy(h->tile_edge_off.p, h->tiling.tile_edge_off.data(), h->tiling.tile_edge_off.size() * sizeof(int),
                    cudaMemcpyHostToDevice);
@@ -630,6 +612,10 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     for (void* p : h->SOL)
         if (p) cudaFree(p);
     if (h->bath) cudaFree(h->bath);
+    if (h->geo) cudaFree(h->geo);
+    if (h->egeo) cudaFree(h->egeo);
+    h->halo.release();
+    h->tile_halo_off.release();
     h->enodes.release();
     h->tile_edge_off.release();
     h->ref_of_dev.release();

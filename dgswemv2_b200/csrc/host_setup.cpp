@@ -372,6 +372,31 @@ static uint64_t spread21(uint64_t v) {
     return v;
 }
 
+void element_geometry(const double* X, const int32_t* nd, double out[5]) {
+    const double J00 = (X[3 * nd[1]] - X[3 * nd[0]]) / 2.0, J01 = (X[3 * nd[2]] - X[3 * nd[0]]) / 2.0;
+    const double J10 = (X[3 * nd[1] + 1] - X[3 * nd[0] + 1]) / 2.0, J11 = (X[3 * nd[2] + 1] - X[3 * nd[0] + 1]) / 2.0;
+    const double det = J00 * J11 - J10 * J01;
+    const double invdet = 1.0 / det;  // 2x2 cofactor inverse
+    out[0] = J11 * invdet;
+    out[1] = -J01 * invdet;
+    out[2] = -J10 * invdet;
+    out[3] = J00 * invdet;
+    out[4] = std::abs(det);
+}
+
+void face_geometry(const double* X, const int32_t* nd, int f, double& nx, double& ny, double& sJ) {
+    const int a = nd[(f + 1) % 3], b = nd[(f + 2) % 3];
+    const double dx = X[3 * b] - X[3 * a], dy = X[3 * b + 1] - X[3 * a + 1];
+    double J00 = (X[3 * nd[1]] - X[3 * nd[0]]) / 2.0, J01 = (X[3 * nd[2]] - X[3 * nd[0]]) / 2.0;
+    double J10 = (X[3 * nd[1] + 1] - X[3 * nd[0] + 1]) / 2.0, J11 = (X[3 * nd[2] + 1] - X[3 * nd[0] + 1]) / 2.0;
+    const double det = J00 * J11 - J10 * J01;
+    const double cw = det / std::abs(det);
+    const double length = std::hypot(dx, dy);
+    nx = cw * dy / length;
+    ny = -cw * dx / length;
+    sJ = std::sqrt(std::pow(dx, 2.0) + std::pow(dy, 2.0)) / 2.0;
+}
+
 int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tiling& out, std::string& err) {
     const int64_t ne = T.ne;
     if (tile != 64 && tile != 128 && tile != 256) {
@@ -408,10 +433,13 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
     for (int64_t d = 0; d < ne; ++d) out.dev_of_ref[out.ref_of_dev[d]] = (int32_t)d;
     out.ntiles = (ne + tile - 1) / tile;
     out.tile_edge_off.assign(out.ntiles + 1, 0);
+    out.tile_halo_off.assign(out.ntiles + 1, 0);
     out.edges.clear();
+    out.egeo.clear();
+    out.halo.clear();
     out.eslot.assign(2 * ne, 0);
     out.max_edges = 0;
-    // interface index of each interior face (for de-duplication inside a tile)
+    out.max_halo = 0;
     std::vector<int64_t> iface(3 * ne, -1);
     for (size_t i = 0; i < T.intf.size() / 4; ++i) {
         iface[3 * (int64_t)T.intf[4 * i] + T.intf[4 * i + 2]] = (int64_t)i;
@@ -419,40 +447,70 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
     }
     std::vector<int64_t> bface(3 * ne, -1);
     for (size_t i = 0; i < T.bnd.size() / 3; ++i) bface[3 * (int64_t)T.bnd[3 * i] + T.bnd[3 * i + 1]] = (int64_t)i;
-    std::unordered_map<int64_t, int> local;
+    std::unordered_map<int64_t, int> local_edge, local_halo;
+    std::vector<int32_t> te;  // this tile's edge records
+    std::vector<double> tg;
     for (int64_t t = 0; t < out.ntiles; ++t) {
-        local.clear();
-        int64_t base = (int64_t)out.edges.size() / 4;
-        out.tile_edge_off[t] = (int32_t)base;
-        int64_t d0 = t * tile, d1 = std::min(ne, d0 + tile);
+        local_edge.clear();
+        local_halo.clear();
+        te.clear();
+        tg.clear();
+        const int64_t d0 = t * tile, d1 = std::min(ne, d0 + tile);
+        const int64_t hbase = (int64_t)out.halo.size() / 2;
+        out.tile_edge_off[t] = (int32_t)((int64_t)out.edges.size() / 4);
+        out.tile_halo_off[t] = (int32_t)hbase;
+        // trace slot of (element in reference order, face)
+        auto trace_slot = [&](int32_t r, int f) -> int32_t {
+            const int64_t d = out.dev_of_ref[r];
+            if (d >= d0 && d < d1) return (int32_t)(3 * (d - d0) + f);
+            const int64_t key = 3 * (int64_t)r + f;
+            auto it = local_halo.find(key);
+            if (it != local_halo.end()) return 3 * tile + it->second;
+            const int h = (int)local_halo.size();
+            local_halo[key] = h;
+            out.halo.push_back((int32_t)d);
+            out.halo.push_back(f);
+            return 3 * tile + h;
+        };
         for (int64_t d = d0; d < d1; ++d) {
-            int32_t r = out.ref_of_dev[d];
+            const int32_t r = out.ref_of_dev[d];
             uint32_t slots[3] = {1023, 1023, 1023};
             for (int f = 0; f < 3; ++f) {
-                int64_t ii = iface[3 * (int64_t)r + f];
-                int64_t bi = bface[3 * (int64_t)r + f];
+                const int64_t ii = iface[3 * (int64_t)r + f];
+                const int64_t bi = bface[3 * (int64_t)r + f];
                 if (ii >= 0) {
-                    auto it = local.find(ii);
-                    if (it != local.end()) {
+                    auto it = local_edge.find(ii);
+                    if (it != local_edge.end()) {
                         slots[f] = (uint32_t)it->second;
-                    } else {
-                        int idx = (int)((int64_t)out.edges.size() / 4 - base);
-                        local[ii] = idx;
-                        slots[f] = (uint32_t)idx;
-                        int32_t in = T.intf[4 * ii], ex = T.intf[4 * ii + 1];
-                        out.edges.push_back(out.dev_of_ref[in]);
-                        out.edges.push_back(out.dev_of_ref[ex]);
-                        out.edges.push_back(T.intf[4 * ii + 2] | T.intf[4 * ii + 3] << 2 | EK_INTERIOR << 4);
-                        out.edges.push_back((int32_t)ii);
+                        continue;
                     }
-                } else if (bi >= 0) {
-                    int idx = (int)((int64_t)out.edges.size() / 4 - base);
+                    const int idx = (int)(te.size() / 4);
+                    local_edge[ii] = idx;
                     slots[f] = (uint32_t)idx;
-                    int kind = T.bnd[3 * bi + 2] == DGSW_BC_LAND ? EK_LAND : EK_FUNCTION;
-                    out.edges.push_back((int32_t)d);
-                    out.edges.push_back(-1);
-                    out.edges.push_back(f | kind << 4);
-                    out.edges.push_back((int32_t)(-1 - bi));
+                    const int32_t in = T.intf[4 * ii], ex = T.intf[4 * ii + 1];
+                    const int fin = T.intf[4 * ii + 2], fex = T.intf[4 * ii + 3];
+                    te.push_back(trace_slot(in, fin));
+                    te.push_back(trace_slot(ex, fex));
+                    te.push_back(fin | fex << 2 | EK_INTERIOR << 4);
+                    te.push_back(out.dev_of_ref[in]);
+                    double nx, ny, sJ;
+                    face_geometry(X, &T.enodes[3 * (int64_t)in], fin, nx, ny, sJ);
+                    tg.push_back(nx);
+                    tg.push_back(ny);
+                    tg.push_back(sJ);
+                } else if (bi >= 0) {
+                    const int idx = (int)(te.size() / 4);
+                    slots[f] = (uint32_t)idx;
+                    const int kind = T.bnd[3 * bi + 2] == DGSW_BC_LAND ? EK_LAND : EK_FUNCTION;
+                    te.push_back((int32_t)(3 * (d - d0) + f));
+                    te.push_back(-1);
+                    te.push_back(f | kind << 4);
+                    te.push_back((int32_t)d);
+                    double nx, ny, sJ;
+                    face_geometry(X, &T.enodes[3 * (int64_t)r], f, nx, ny, sJ);
+                    tg.push_back(nx);
+                    tg.push_back(ny);
+                    tg.push_back(sJ);
                 }
             }
             int32_t roles = 0;
@@ -462,14 +520,18 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
             out.eslot[2 * d] = (int32_t)(slots[0] | slots[1] << 10 | slots[2] << 20);
             out.eslot[2 * d + 1] = roles | ord << 3;
         }
-        int n = (int)((int64_t)out.edges.size() / 4 - base);
+        const int n = (int)(te.size() / 4);
         if (n > 1022) {
             err = "tile edge list overflow";
             return DGSW_ERR_INVALID_ARGUMENT;
         }
+        out.edges.insert(out.edges.end(), te.begin(), te.end());
+        out.egeo.insert(out.egeo.end(), tg.begin(), tg.end());
         out.max_edges = std::max(out.max_edges, n);
+        out.max_halo = std::max(out.max_halo, (int)local_halo.size());
     }
     out.tile_edge_off[out.ntiles] = (int32_t)((int64_t)out.edges.size() / 4);
+    out.tile_halo_off[out.ntiles] = (int32_t)((int64_t)out.halo.size() / 2);
     return DGSW_OK;
 }
 

@@ -44,9 +44,16 @@ struct Tiling {
     std::vector<int32_t> dev_of_ref;  // [ne]
     std::vector<int32_t> ref_of_dev;  // [ne]
     std::vector<int32_t> tile_edge_off;  // [ntiles+1]
-    std::vector<int32_t> edges;          // [4 * n_edges]: A dev, B dev (-1), meta, interface/boundary index
+    // [4 * n_edges]: trace slot of the in/owner side a, trace slot of b (-1 for boundaries),
+    // meta = face_a | face_b << 2 | kind << 4, device index of a. Trace slots: 3*(element - tile start)
+    // + face for tile elements, 3*tile + h for the tile's halo face h.
+    std::vector<int32_t> edges;
+    std::vector<double> egeo;            // [3 * n_edges]: normal x, normal y, half length (of face a)
+    std::vector<int32_t> tile_halo_off;  // [ntiles+1]
+    std::vector<int32_t> halo;           // [2 * n_halo]: device element, face
     std::vector<int32_t> eslot;          // [2 * ne] per element (dev order): packed slots, roles + order
     int max_edges = 0;
+    int max_halo = 0;
 };
 
 int build_tiling(const Topology& T, const double* node_xyz, int tile, bool morton, Tiling& out, std::string& err);
@@ -70,6 +77,12 @@ int build_tables(int p, Tables& t, std::string& err);
 
 // Dubiner modes of order p at n master points: phi[dof * n + pt]
 void eval_basis(int p, const double* z1, const double* z2, int n, double* phi);
+
+// element geometry in the reference's formulas (shape_straighttriangle.cpp:95-137):
+// J^-1(0,0), J^-1(0,1), J^-1(1,0), J^-1(1,1), |det J|
+void element_geometry(const double* node_xyz, const int32_t* nodes3, double out[5]);
+// outward unit normal and surface Jacobian (half length) of face f (shape_straighttriangle.cpp:110-168)
+void face_geometry(const double* node_xyz, const int32_t* nodes3, int f, double& nx, double& ny, double& sJ);
 
 // FP64 host projections of initialize_data_serial: bathymetry modes per element (reference order)
 void project_bathymetry(const Topology& T, const double* node_xyz, const Tables& tb, std::vector<double>& bath);

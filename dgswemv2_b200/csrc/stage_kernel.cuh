@@ -1,22 +1,24 @@
 // Fused RKDG stage kernel for sm_100a.
 //
 // One CTA owns one tile of TILE consecutive elements (device order = Morton order of centroids).
-// Per stage it does, in three phases separated by __syncthreads:
-//   1. element phase (thread = element): load the element's modes into registers and shared memory,
-//      rebuild its geometry from the FP64 node coordinates, and accumulate the volume and source
-//      integrals (Problem::volume_kernel + source_kernel, rkdg_swe_proc_volume.hpp:9-35,
-//      rkdg_swe_proc_source.hpp:9-18);
-//   2. edge phase (thread = edge of the tile's list): evaluate the numerical flux at the edge Gauss
-//      points once per edge (interfaces: LLF + the wet/dry fix-ups of ISP::Internal,
+// Per RK stage it does, in three phases separated by __syncthreads:
+//   1. element phase (thread = element): load the element's modes, accumulate the volume and source
+//      integrals in registers (Problem::volume_kernel + source_kernel, rkdg_swe_proc_volume.hpp:9-35,
+//      rkdg_swe_proc_source.hpp:9-18), and write the traces of its three faces at the edge Gauss points
+//      to shared memory. Neighbours in other tiles ("halo" faces) get their face traces written by the
+//      same routine from global memory;
+//   2. edge phase (thread = edge of the tile's list): numerical flux at the edge Gauss points once per
+//      edge from the shared-memory traces (interfaces: LLF + the wet/dry fix-ups of ISP::Internal,
 //      rkdg_swe_is_internal.hpp:26-95; boundaries: BC::Land / BC::Function, rkdg_swe_bc_land.hpp:41-66,
-//      rkdg_swe_bc_function.hpp:27-60) into shared memory. An edge between two tiles is evaluated by
-//      both CTAs with the same code on the same inputs, so both see the same bits and F_ex = -F_in
-//      holds exactly as in the reference;
+//      rkdg_swe_bc_function.hpp:27-60). An edge between two tiles is evaluated by both CTAs with the
+//      same code on the same bits, so F_ex = -F_in holds exactly as in the reference;
 //   3. element phase: subtract the edge contributions in the reference's interface/boundary order,
 //      apply M^-1 and the SSP-RK stage combination (element.hpp:502-505,
-//      explicit_ssp_rk_stepper.hpp:67-80), the wetting/drying kernel (swe_post_wet_dry.hpp:6-145,
-//      its depth tests in FP64 in every precision) and the NaN scrutiny; write the next stage state.
-// Modal state layout in HBM: component-major SoA, q[(var*ND + dof) * ne_pad + element].
+//      explicit_ssp_rk_stepper.hpp:67-80), the wetting/drying kernel (swe_post_wet_dry.hpp:6-145, its
+//      depth tests in FP64 in every precision) and the NaN scrutiny; write the next stage state.
+// The master tables are compile-time constants (tables_gen.h): every table entry is an immediate,
+// zero entries are skipped and unit entries become additions.
+// HBM layout: component-major SoA, q[(var*ND + dof) * ne_pad + element].
 #ifndef DGSW_STAGE_KERNEL_CUH
 #define DGSW_STAGE_KERNEL_CUH
 
@@ -24,22 +26,22 @@
 
 #include "function_sets.h"
 #include "rk_tables.h"
+#include "tables_gen.h"
 
 namespace dgsw {
 
-template <typename Real>
-struct DevTables {  // master tables of one polynomial order, in the kernel's precision
-    Real phi[6 * 6];      // [dof][gp]
-    Real dphi[2][6 * 6];  // [z][dof][gp]
-    Real mz[2][6 * 6];    // [z][gp][dof]
-    Real phiw[6 * 6];     // [gp][dof]
-    double psi[3][6];     // [node][gp] (FP64: global coordinates of the volume points)
-    Real fphi[3][6 * 3];  // [face][dof][gp]
-    double fpsi[3][3][3]; // [face][node][gp]
-    Real gw[3];
-    double minv[6];
+// compile-time loops
+template <int N>
+struct IC {
+    static constexpr int value = N;
 };
-
+template <int B, int E, typename F>
+__device__ __forceinline__ void sfor(F&& f) {
+    if constexpr (B < E) {
+        f(IC<B>{});
+        sfor<B + 1, E>(f);
+    }
+}
 
 struct DevStatus {
     unsigned int nan_flag;
@@ -48,17 +50,13 @@ struct DevStatus {
 };
 
 struct DevClock {
-    double t;      // time at the start of the current step (ESSPRKStepper::t)
+    double t;  // time at the start of the current step (ESSPRKStepper::t)
     long long step;
 };
 
-// Kernel arguments. The master tables travel by value inside the argument block, which the
-// hardware serves from its constant bank: every table index in the kernel is a compile-time
-// constant (face tables, indexed per thread, are copied to shared memory first).
 template <typename Real>
 struct StageArgs {
-    DevTables<Real> T;
-    const Real* qk[DGSW_RK_MAX_STAGES];  // stage states q_0..q_s used by this stage's combination
+    const Real* qk[DGSW_RK_MAX_STAGES];  // stage states used by this stage's combination, q_s last
     const Real* solk[DGSW_RK_MAX_STAGES];
     double a[DGSW_RK_MAX_STAGES];
     double bdt[DGSW_RK_MAX_STAGES];
@@ -66,13 +64,17 @@ struct StageArgs {
     int store_sol;  // write sol_s (needed when a later stage uses it)
     Real* q_out;
     Real* sol_out;
-    const Real* bath;        // [ND][ne_pad]
-    const int* enodes;       // [3][ne_pad]
-    const int2* eslot;       // [ne]
-    const int4* edges;       // tile edge lists
+    const Real* bath;           // [3][ne_pad] bathymetry modes of the linear part
+    const Real* geo;            // [5][ne_pad] J^-1(0,0), J^-1(0,1), J^-1(1,0), J^-1(1,1), |J|
+    const int* enodes;          // [3][ne_pad]
+    const int2* eslot;          // [ne] edge slot per face, roles, accumulation order
+    const int4* edges;          // tile edge lists: trace slot of a, trace slot of b (-1), meta, element a
+    const Real* egeo;           // [3][n_edges]: outward unit normal of a (x, y), half length
     const int* tile_edge_off;
-    const double2* xy;       // node coordinates
-    const double* nz;        // node bathymetry depth (wet/dry vertex depths)
+    const int2* halo;           // tile halo lists: (element, face)
+    const int* tile_halo_off;
+    const double2* xy;          // node coordinates
+    const double* nz;           // node bathymetry depth (wet/dry vertex depths)
     const unsigned char* wet_in;
     unsigned char* wet_out;
     const int* ref_of_dev;
@@ -82,6 +84,7 @@ struct StageArgs {
     double drk_s;  // stage-time offset of this stage (t + dt*drk[s])
     int ne;
     int ne_pad;
+    int n_edges;  // total edge records (stride of egeo)
     double g;
     double h_o, h_o_thr;
     int fn_set;
@@ -283,32 +286,61 @@ __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double b
 }
 
 // ------------------------------------------------------------------------------------------------
-// the stage kernel
+// compile-time table access
 // ------------------------------------------------------------------------------------------------
 template <int P>
-struct Dims {
-    static constexpr int ND = (P + 1) * (P + 2) / 2;
-    static constexpr int NQ = (P == 1) ? 3 : 6;  // Dunavant degree 2p
-    static constexpr int NG = P + 1;             // Gauss-Legendre points for degree 2p+1
-};
+using MT = ct::Master<P>;
+
+// trace of an element's face F at the edge Gauss points: ze, qx, qy and bathymetry,
+// sum over the modes in ascending order (same arithmetic for tile and halo elements)
+template <int P, int F, typename Real>
+__device__ __forceinline__ void face_trace(const Real (&q)[3][MT<P>::ND], const Real (&b)[3],
+                                           Real (&t)[4][MT<P>::NG]) {
+    constexpr int ND = MT<P>::ND, NG = MT<P>::NG;
+    sfor<0, NG>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        sfor<0, 3>([&](auto V) {
+            constexpr int v = decltype(V)::value;
+            Real s = Real(0);
+            sfor<0, ND>([&](auto K) {
+                constexpr int k = decltype(K)::value;
+                constexpr double c = MT<P>::fphi((F * ND + k) * NG + g);
+                if constexpr (c != 0.0) s += q[v][k] * (Real)c;
+            });
+            t[v][g] = s;
+        });
+        Real sb = Real(0);
+        sfor<0, 3>([&](auto K) {
+            constexpr int k = decltype(K)::value;
+            constexpr double c = MT<P>::fphi((F * ND + k) * NG + g);
+            if constexpr (c != 0.0) sb += b[k] * (Real)c;
+        });
+        t[3][g] = sb;
+    });
+}
 
 // shared-memory layout of the stage kernel
 template <int P, typename Real, bool WD>
 struct Smem {
-    static constexpr int ND = Dims<P>::ND, NG = Dims<P>::NG;
+    static constexpr int ND = MT<P>::ND, NG = MT<P>::NG;
+    static constexpr int NTC = 4 * NG;                 // trace components per face slot
     static constexpr int NFC = (WD ? 2 : 1) * 3 * NG;  // flux components stored per edge
     static __host__ __device__ size_t al(size_t b) { return (b + 15) & ~size_t(15); }
-    // section offsets (16-byte aligned)
-    static __host__ __device__ size_t off_bath(int tile) { return al(sizeof(Real) * (size_t)3 * ND * tile); }
-    static __host__ __device__ size_t off_F(int tile) { return off_bath(tile) + al(sizeof(Real) * (size_t)ND * tile); }
-    static __host__ __device__ size_t off_sJ(int tile, int me) { return off_F(tile) + al(sizeof(Real) * (size_t)NFC * me); }
-    static __host__ __device__ size_t off_tab(int tile, int me) { return off_sJ(tile, me) + al(sizeof(double) * (size_t)me); }
-    static __host__ __device__ size_t off_node(int tile, int me) {
-        return off_tab(tile, me) + al(sizeof(Real) * (size_t)(3 * ND * NG + NG));
+    static __host__ __device__ int nslot(int tile, int mh) { return 3 * tile + mh; }
+    static __host__ __device__ size_t off_tr(int tile) { return al(sizeof(Real) * (size_t)3 * ND * tile); }
+    static __host__ __device__ size_t off_F(int tile, int mh) {
+        return off_tr(tile) + al(sizeof(Real) * (size_t)NTC * nslot(tile, mh));
     }
-    static __host__ __device__ size_t off_wet(int tile, int me) { return off_node(tile, me) + al(sizeof(int) * (size_t)3 * tile); }
-    static __host__ __device__ size_t off_flag(int tile, int me) { return off_wet(tile, me) + al((size_t)tile); }
-    static __host__ __device__ size_t bytes(int tile, int me) { return off_flag(tile, me) + al((size_t)me); }
+    static __host__ __device__ size_t off_sJ(int tile, int mh, int me) {
+        return off_F(tile, mh) + al(sizeof(Real) * (size_t)NFC * me);
+    }
+    static __host__ __device__ size_t off_wet(int tile, int mh, int me) {
+        return off_sJ(tile, mh, me) + al(sizeof(Real) * (size_t)me);
+    }
+    static __host__ __device__ size_t off_flag(int tile, int mh, int me) {
+        return off_wet(tile, mh, me) + al((size_t)nslot(tile, mh));
+    }
+    static __host__ __device__ size_t bytes(int tile, int mh, int me) { return off_flag(tile, mh, me) + al((size_t)me); }
 };
 
 // resident CTAs per SM the register budget is sized for
@@ -318,20 +350,18 @@ struct MinBlocks {
 };
 
 template <int P, typename Real, bool WD, bool FSRC, int TILE>
-__global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_edges) {
-    constexpr int ND = Dims<P>::ND, NQ = Dims<P>::NQ, NG = Dims<P>::NG;
-    const DevTables<Real>& T = A.T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
+    rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_halo, int max_edges) {
+    constexpr int ND = MT<P>::ND, NQ = MT<P>::NQ, NG = MT<P>::NG;
     using SM = Smem<P, Real, WD>;
-    Real* sq = reinterpret_cast<Real*>(smem_raw);                                          // [3*ND][TILE]
-    Real* sbath = reinterpret_cast<Real*>(smem_raw + SM::off_bath(TILE));                  // [ND][TILE]
-    Real* sF = reinterpret_cast<Real*>(smem_raw + SM::off_F(TILE));                        // [NFC][max_edges]
-    double* ssJ = reinterpret_cast<double*>(smem_raw + SM::off_sJ(TILE, max_edges));       // [max_edges]
-    Real* sfphi = reinterpret_cast<Real*>(smem_raw + SM::off_tab(TILE, max_edges));       // [3][ND][NG]
-    Real* sgw = sfphi + 3 * ND * NG;
-    int* snode = reinterpret_cast<int*>(smem_raw + SM::off_node(TILE, max_edges));        // [3][TILE]
-    unsigned char* swet = smem_raw + SM::off_wet(TILE, max_edges);
-    unsigned char* sflag = smem_raw + SM::off_flag(TILE, max_edges);
+    const int NS = SM::nslot(TILE, max_halo);  // trace slots: 3 per tile element, then halo faces
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* sq = reinterpret_cast<Real*>(smem_raw);                                   // [3*ND][TILE]
+    Real* str = reinterpret_cast<Real*>(smem_raw + SM::off_tr(TILE));               // [4*NG][NS]
+    Real* sF = reinterpret_cast<Real*>(smem_raw + SM::off_F(TILE, max_halo));       // [NFC][max_edges]
+    Real* ssJ = reinterpret_cast<Real*>(smem_raw + SM::off_sJ(TILE, max_halo, max_edges));
+    unsigned char* swet = smem_raw + SM::off_wet(TILE, max_halo, max_edges);        // [NS]
+    unsigned char* sflag = smem_raw + SM::off_flag(TILE, max_halo, max_edges);      // [max_edges]
 
     const int tile = blockIdx.x;
     const int e0 = tile * TILE;
@@ -339,70 +369,70 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
     const int tid = threadIdx.x;
     const int d = e0 + tid;
     const bool active = tid < nloc;
+    const int P_ = A.ne_pad;
     const double t_stage = A.clock->t + A.drk_s;  // ESSPRKStepper::GetTimeAtCurrentStage
     const Real g = (Real)A.g;
     const Real* __restrict__ qs = A.qk[A.nterms - 1];  // this stage's state
     const dgsw_fn_time FT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
-
-    // face tables are indexed by per-thread face numbers: keep them in shared memory
-    for (int i = tid; i < 3 * ND * NG; i += TILE) sfphi[i] = T.fphi[i / (ND * NG)][i % (ND * NG)];
-    if (tid < NG) sgw[tid] = T.gw[tid];
 
     Real rhs[3][ND];
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < ND; ++k) rhs[v][k] = Real(0);
-    double aJ = 1.0;
+    Real aJ = Real(1);
     bool wet = false;
 
-    // ---------------- phase 1: element volume + source ----------------
+    // ---------------- phase 1: volume + source integrals, face traces ----------------
     if (active) {
-        const int n0 = A.enodes[d], n1 = A.enodes[A.ne_pad + d], n2 = A.enodes[2 * A.ne_pad + d];
-        snode[tid] = n0;
-        snode[TILE + tid] = n1;
-        snode[2 * TILE + tid] = n2;
-        const double2 p0 = A.xy[n0], p1 = A.xy[n1], p2 = A.xy[n2];
-        // Jacobian of the straight triangle, shape_straighttriangle.cpp:95-137
-        const double J00 = (p1.x - p0.x) / 2.0, J01 = (p2.x - p0.x) / 2.0;
-        const double J10 = (p1.y - p0.y) / 2.0, J11 = (p2.y - p0.y) / 2.0;
-        const double det = J00 * J11 - J10 * J01;
-        aJ = fabs(det);
-        const double invdet = 1.0 / det;
-        const Real Ji00 = (Real)(J11 * invdet), Ji10 = (Real)(-J10 * invdet);
-        const Real Ji01 = (Real)(-J01 * invdet), Ji11 = (Real)(J00 * invdet);
-        Real q[3][ND], b[ND];
+        Real q[3][ND], b[3];
 #pragma unroll
         for (int c = 0; c < 3 * ND; ++c) {
-            const Real val = qs[c * A.ne_pad + d];
+            const Real val = qs[c * P_ + d];
             q[c / ND][c % ND] = val;
             sq[c * TILE + tid] = val;
         }
 #pragma unroll
-        for (int k = 0; k < ND; ++k) {
-            b[k] = A.bath[k * A.ne_pad + d];
-            sbath[k * TILE + tid] = b[k];
-        }
+        for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + d];
+        const Real Ji00 = A.geo[d], Ji01 = A.geo[P_ + d], Ji10 = A.geo[2 * P_ + d], Ji11 = A.geo[3 * P_ + d];
+        aJ = A.geo[4 * P_ + d];
         wet = A.wet_in[d] != 0;
-        swet[tid] = wet ? 1 : 0;
         if (wet) {
-            // unrolled: every table entry becomes an immediate constant-bank operand
-#pragma unroll
-            for (int gp = 0; gp < NQ; ++gp) {
-                Real qg[3], bg = Real(0), db0 = Real(0), db1 = Real(0);
-#pragma unroll
-                for (int v = 0; v < 3; ++v) {
+            double x0 = 0, y0 = 0, x1 = 0, y1 = 0, x2 = 0, y2 = 0;
+            if (FSRC || A.spherical) {
+                const double2 p0 = A.xy[A.enodes[d]], p1 = A.xy[A.enodes[P_ + d]], p2 = A.xy[A.enodes[2 * P_ + d]];
+                x0 = p0.x, y0 = p0.y, x1 = p1.x, y1 = p1.y, x2 = p2.x, y2 = p2.y;
+            }
+            // bathymetry gradient: the projected bathymetry is linear, its gradient constant
+            Real db0 = Real(0), db1 = Real(0);
+            sfor<0, 3>([&](auto K) {
+                constexpr int k = decltype(K)::value;
+                constexpr double c0 = MT<P>::dphi((0 * ND + k) * NQ + 0);
+                constexpr double c1 = MT<P>::dphi((1 * ND + k) * NQ + 0);
+                if constexpr (c0 != 0.0) db0 += b[k] * (Real)c0;
+                if constexpr (c1 != 0.0) db1 += b[k] * (Real)c1;
+            });
+            const Real dbx = db0 * Ji00 + db1 * Ji10;
+            const Real dby = db0 * Ji01 + db1 * Ji11;
+            sfor<0, NQ>([&](auto GP) {
+                constexpr int gp = decltype(GP)::value;
+                Real qg[3];
+                sfor<0, 3>([&](auto V) {
+                    constexpr int v = decltype(V)::value;
                     Real s = Real(0);
-#pragma unroll
-                    for (int k = 0; k < ND; ++k) s += q[v][k] * T.phi[k * NQ + gp];
+                    sfor<0, ND>([&](auto K) {
+                        constexpr int k = decltype(K)::value;
+                        constexpr double c = MT<P>::phi(k * NQ + gp);
+                        if constexpr (c != 0.0) s += q[v][k] * (Real)c;
+                    });
                     qg[v] = s;
-                }
-#pragma unroll
-                for (int k = 0; k < ND; ++k) {
-                    bg += b[k] * T.phi[k * NQ + gp];
-                    db0 += b[k] * T.dphi[0][k * NQ + gp];
-                    db1 += b[k] * T.dphi[1][k * NQ + gp];
-                }
+                });
+                Real bg = Real(0);
+                sfor<0, 3>([&](auto K) {
+                    constexpr int k = decltype(K)::value;
+                    constexpr double c = MT<P>::phi(k * NQ + gp);
+                    if constexpr (c != 0.0) bg += b[k] * (Real)c;
+                });
                 // physical flux, swe_flux.hpp:5-25
                 const Real h = qg[0] + bg;
                 const Real ih = Real(1) / h;
@@ -412,17 +442,17 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
                 Real Fy[3] = {qg[2], u * qg[2], vv * qg[2] + pe};
                 double xg = 0.0, yg = 0.0;
                 if (FSRC || A.spherical) {
-                    xg = p0.x * T.psi[0][gp] + p1.x * T.psi[1][gp] + p2.x * T.psi[2][gp];
-                    yg = p0.y * T.psi[0][gp] + p1.y * T.psi[1][gp] + p2.y * T.psi[2][gp];
+                    constexpr double s0 = MT<P>::psi(0 * NQ + gp), s1 = MT<P>::psi(1 * NQ + gp),
+                                     s2 = MT<P>::psi(2 * NQ + gp);
+                    xg = x0 * s0 + x1 * s1 + x2 * s2;
+                    yg = y0 * s0 + y1 * s1 + y2 * s2;
                 }
                 if (A.spherical) {
                     const Real sp = (Real)(A.sp_cos_lat0 / cos(yg / A.sp_R));
 #pragma unroll
                     for (int v = 0; v < 3; ++v) Fx[v] = sp * Fx[v];
                 }
-                // bathymetry-slope source, swe_source.hpp:15-21 (db/dx through J^-1)
-                const Real dbx = db0 * Ji00 + db1 * Ji10;
-                const Real dby = db0 * Ji01 + db1 * Ji11;
+                // bathymetry-slope source, swe_source.hpp:15-21
                 Real S[3] = {Real(0), g * (dbx * qg[0]), g * (dby * qg[0])};
                 if (FSRC) {
                     Real fs[3];
@@ -432,131 +462,134 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
                     S[2] += fs[2];
                 }
                 // int F . grad(phi) = sum_gp sum_z (F_x J^-1(z,x) + F_y J^-1(z,y)) dphi_z w
-#pragma unroll
-                for (int v = 0; v < 3; ++v) {
+                sfor<0, 3>([&](auto V) {
+                    constexpr int v = decltype(V)::value;
                     const Real G0 = Fx[v] * Ji00 + Fy[v] * Ji01;
                     const Real G1 = Fx[v] * Ji10 + Fy[v] * Ji11;
-#pragma unroll
-                    for (int k = 0; k < ND; ++k)
-                        rhs[v][k] += G0 * T.mz[0][gp * ND + k] + G1 * T.mz[1][gp * ND + k] + S[v] * T.phiw[gp * ND + k];
-                }
-            }
-            const Real raJ = (Real)aJ;
+                    sfor<0, ND>([&](auto K) {
+                        constexpr int k = decltype(K)::value;
+                        constexpr double m0 = MT<P>::mz((0 * NQ + gp) * ND + k);
+                        constexpr double m1 = MT<P>::mz((1 * NQ + gp) * ND + k);
+                        constexpr double pw = MT<P>::phiw(gp * ND + k);
+                        Real acc = rhs[v][k];
+                        if constexpr (m0 != 0.0) acc += G0 * (Real)m0;
+                        if constexpr (m1 != 0.0) acc += G1 * (Real)m1;
+                        if constexpr (pw != 0.0) acc += S[v] * (Real)pw;
+                        rhs[v][k] = acc;
+                    });
+                });
+            });
 #pragma unroll
             for (int v = 0; v < 3; ++v)
 #pragma unroll
-                for (int k = 0; k < ND; ++k) rhs[v][k] *= raJ;
+                for (int k = 0; k < ND; ++k) rhs[v][k] *= aJ;
+        }
+        // traces of the three faces (needed also when dry: a wet neighbour evaluates the interface)
+        sfor<0, 3>([&](auto FF) {
+            constexpr int f = decltype(FF)::value;
+            Real t[4][NG];
+            face_trace<P, f, Real>(q, b, t);
+            const int slot = 3 * tid + f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int gg = 0; gg < NG; ++gg) str[(c * NG + gg) * NS + slot] = t[c][gg];
+            swet[slot] = wet ? 1 : 0;
+        });
+    }
+    // halo faces: faces of elements in other tiles that this tile's edges need
+    {
+        const int hoff = A.tile_halo_off[tile];
+        const int nh = A.tile_halo_off[tile + 1] - hoff;
+#pragma unroll 1
+        for (int h = tid; h < nh; h += TILE) {
+            const int2 it = A.halo[hoff + h];
+            const int e = it.x;
+            Real q[3][ND], b[3], t[4][NG];
+#pragma unroll
+            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = qs[c * P_ + e];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + e];
+            if (it.y == 0)
+                face_trace<P, 0, Real>(q, b, t);
+            else if (it.y == 1)
+                face_trace<P, 1, Real>(q, b, t);
+            else
+                face_trace<P, 2, Real>(q, b, t);
+            const int slot = 3 * TILE + h;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int gg = 0; gg < NG; ++gg) str[(c * NG + gg) * NS + slot] = t[c][gg];
+            swet[slot] = A.wet_in[e] != 0 ? 1 : 0;
         }
     }
     __syncthreads();
 
     // ---------------- phase 2: edge fluxes, once per edge of the tile ----------------
-    const int eoff = A.tile_edge_off[tile];
-    const int nedge = A.tile_edge_off[tile + 1] - eoff;
+    {
+        const int eoff = A.tile_edge_off[tile];
+        const int nedge = A.tile_edge_off[tile + 1] - eoff;
 #pragma unroll 1
-    for (int le = tid; le < nedge; le += TILE) {
-        const int4 rec = A.edges[eoff + le];
-        const int ea = rec.x, eb = rec.y;
-        const int fa = rec.z & 3, fb = (rec.z >> 2) & 3, kind = (rec.z >> 4) & 3;
-        const int la = ea - e0, lb = eb - e0;
-        const bool a_loc = (la >= 0 && la < nloc), b_loc = (eb >= 0 && lb >= 0 && lb < nloc);
-        const bool wa = a_loc ? swet[la] != 0 : A.wet_in[ea] != 0;
-        const bool wb = (eb < 0) ? false : (b_loc ? swet[lb] != 0 : A.wet_in[eb] != 0);
-        const bool compute = (kind == 0) ? (wa || wb) : wa;
-        sflag[le] = compute ? 1 : 0;
-        // face geometry from element a's vertices (fa+1)%3 -> (fa+2)%3
-        const int va = (fa + 1) % 3, vb = (fa + 2) % 3;
-        const int na = a_loc ? snode[va * TILE + la] : A.enodes[va * A.ne_pad + ea];
-        const int nb = a_loc ? snode[vb * TILE + la] : A.enodes[vb * A.ne_pad + ea];
-        const double2 pa = A.xy[na], pb = A.xy[nb];
-        const double dx = pb.x - pa.x, dy = pb.y - pa.y;
-        const double len = sqrt(dx * dx + dy * dy);
-        ssJ[le] = len / 2.0;  // surface Jacobian = half edge length
-        if (!compute) continue;
-        const double ilen = 1.0 / len;
-        const Real nx = (Real)(dy * ilen), ny = (Real)(-dx * ilen);  // outward unit normal of element a
-        // traces at the edge Gauss points, accumulated over the modes in ascending order
-        Real ti[3][NG], te[3][NG], bi[NG], be[NG];
-#pragma unroll
-        for (int gp = 0; gp < NG; ++gp) {
-            ti[0][gp] = ti[1][gp] = ti[2][gp] = Real(0);
-            te[0][gp] = te[1][gp] = te[2][gp] = Real(0);
-            bi[gp] = be[gp] = Real(0);
-        }
-        const Real* fta = sfphi + fa * ND * NG;
-        const Real* ftb = sfphi + fb * ND * NG;
-#pragma unroll
-        for (int k = 0; k < ND; ++k) {
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                const Real c = a_loc ? sq[(v * ND + k) * TILE + la] : qs[(v * ND + k) * A.ne_pad + ea];
-#pragma unroll
-                for (int gp = 0; gp < NG; ++gp) ti[v][gp] += c * fta[k * NG + gp];
+        for (int le = tid; le < nedge; le += TILE) {
+            const int4 rec = A.edges[eoff + le];
+            const int sa = rec.x, sb = rec.y;
+            const int kind = (rec.z >> 4) & 3;
+            const Real nx = A.egeo[eoff + le], ny = A.egeo[A.n_edges + eoff + le];
+            ssJ[le] = A.egeo[2 * A.n_edges + eoff + le];
+            const bool wa = swet[sa] != 0;
+            const bool wb = sb >= 0 && swet[sb] != 0;
+            const bool compute = (kind == 0) ? (wa || wb) : wa;
+            sflag[le] = compute ? 1 : 0;
+            if (!compute) continue;
+            Real sp = Real(1);
+            double xa = 0, ya = 0, xb = 0, yb = 0;
+            if (kind == 2 || A.spherical) {
+                // Gauss points of face fa lie on the segment from node (fa+1)%3 to node (fa+2)%3
+                const int fa = rec.z & 3, ea = rec.w;
+                const double2 pa = A.xy[A.enodes[((fa + 1) % 3) * P_ + ea]];
+                const double2 pb = A.xy[A.enodes[((fa + 2) % 3) * P_ + ea]];
+                xa = pa.x, ya = pa.y, xb = pb.x, yb = pb.y;
             }
-            const Real c = a_loc ? sbath[k * TILE + la] : A.bath[k * A.ne_pad + ea];
-#pragma unroll
-            for (int gp = 0; gp < NG; ++gp) bi[gp] += c * fta[k * NG + gp];
-        }
-        if (kind == 0) {
-#pragma unroll
-            for (int k = 0; k < ND; ++k) {
-#pragma unroll
-                for (int v = 0; v < 3; ++v) {
-                    const Real c = b_loc ? sq[(v * ND + k) * TILE + lb] : qs[(v * ND + k) * A.ne_pad + eb];
-#pragma unroll
-                    for (int gp = 0; gp < NG; ++gp) te[v][gp] += c * ftb[k * NG + (NG - 1 - gp)];
+            sfor<0, NG>([&](auto GP) {
+                constexpr int gp = decltype(GP)::value;
+                constexpr int ge = NG - 1 - gp;  // the ex side's Gauss point paired with gp
+                // BoundaryToMasterCoordinates + LocalToGlobalCoordinates on a straight edge
+                constexpr double wa_ = MT<P>::fpsi((0 * 3 + 1) * NG + gp), wb_ = MT<P>::fpsi((0 * 3 + 2) * NG + gp);
+                if (A.spherical) sp = (Real)(A.sp_cos_lat0 / cos((ya * wa_ + yb * wb_) / A.sp_R));
+                const Real qi[3] = {str[(0 * NG + gp) * NS + sa], str[(1 * NG + gp) * NS + sa],
+                                    str[(2 * NG + gp) * NS + sa]};
+                const Real bi = str[(3 * NG + gp) * NS + sa];
+                Real qe[3], be = Real(0);
+                if (kind == 0) {
+                    qe[0] = str[(0 * NG + ge) * NS + sb];
+                    qe[1] = str[(1 * NG + ge) * NS + sb];
+                    qe[2] = str[(2 * NG + ge) * NS + sb];
+                    if (WD) be = str[(3 * NG + ge) * NS + sb];
+                } else if (kind == 1) {
+                    // BC::Land ghost state: normal momentum mirrored (rkdg_swe_bc_land.hpp:44-56)
+                    const Real tx = -ny, ty = nx;
+                    const Real qn_ex = -(qi[1] * nx + qi[2] * ny);
+                    const Real qt_ex = qi[1] * tx + qi[2] * ty;
+                    qe[0] = qi[0];
+                    qe[1] = qn_ex * nx + qt_ex * tx;
+                    qe[2] = qn_ex * ny + qt_ex * ty;
+                } else {
+                    // BC::Function ghost state: ic_q(t, x_gp) (rkdg_swe_bc_function.hpp:33-50)
+                    fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 0, (Real)(xa * wa_ + xb * wb_),
+                                      (Real)(ya * wa_ + yb * wb_), qe);
                 }
-                if (WD) {
-                    const Real c = b_loc ? sbath[k * TILE + lb] : A.bath[k * A.ne_pad + eb];
+                Real Fi[3];
+                llf_flux<Real>(g, qi, qe, bi, sp, nx, ny, Fi);
+                if (WD && kind == 0) {
+                    Real Fe[3] = {-Fi[0], -Fi[1], -Fi[2]};
+                    if (!(wa && wb)) wd_fixup<Real>(g, qi, qe, bi, be, sp, nx, ny, wa, wb, Fi, Fe);
 #pragma unroll
-                    for (int gp = 0; gp < NG; ++gp) be[gp] += c * ftb[k * NG + (NG - 1 - gp)];
+                    for (int v = 0; v < 3; ++v) sF[((3 + v) * NG + gp) * max_edges + le] = Fe[v];
                 }
-            }
-        }
-        Real sp = Real(1);
-        double xg[NG], yg[NG];
-        if (kind == 2 || A.spherical) {
-            const int m0 = a_loc ? snode[la] : A.enodes[ea];
-            const int m1 = a_loc ? snode[TILE + la] : A.enodes[A.ne_pad + ea];
-            const int m2 = a_loc ? snode[2 * TILE + la] : A.enodes[2 * A.ne_pad + ea];
-            const double2 c0 = A.xy[m0], c1 = A.xy[m1], c2 = A.xy[m2];
 #pragma unroll
-            for (int gp = 0; gp < NG; ++gp) {
-                xg[gp] = c0.x * T.fpsi[fa][0][gp] + c1.x * T.fpsi[fa][1][gp] + c2.x * T.fpsi[fa][2][gp];
-                yg[gp] = c0.y * T.fpsi[fa][0][gp] + c1.y * T.fpsi[fa][1][gp] + c2.y * T.fpsi[fa][2][gp];
-            }
-        }
-#pragma unroll
-        for (int gp = 0; gp < NG; ++gp) {
-            if (A.spherical) sp = (Real)(A.sp_cos_lat0 / cos(yg[gp] / A.sp_R));
-            const Real qi[3] = {ti[0][gp], ti[1][gp], ti[2][gp]};
-            Real qe[3];
-            if (kind == 0) {
-                qe[0] = te[0][gp];
-                qe[1] = te[1][gp];
-                qe[2] = te[2][gp];
-            } else if (kind == 1) {
-                // BC::Land ghost state: normal momentum mirrored (rkdg_swe_bc_land.hpp:44-56)
-                const Real tx = -ny, ty = nx;
-                const Real qn_ex = -(qi[1] * nx + qi[2] * ny);
-                const Real qt_ex = qi[1] * tx + qi[2] * ty;
-                qe[0] = qi[0];
-                qe[1] = qn_ex * nx + qt_ex * tx;
-                qe[2] = qn_ex * ny + qt_ex * ty;
-            } else {
-                // BC::Function ghost state: ic_q(t, x_gp) (rkdg_swe_bc_function.hpp:33-50)
-                fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 0, (Real)xg[gp], (Real)yg[gp], qe);
-            }
-            Real Fi[3];
-            llf_flux<Real>(g, qi, qe, bi[gp], sp, nx, ny, Fi);
-            if (WD && kind == 0) {
-                Real Fe[3] = {-Fi[0], -Fi[1], -Fi[2]};
-                if (!(wa && wb)) wd_fixup<Real>(g, qi, qe, bi[gp], be[gp], sp, nx, ny, wa, wb, Fi, Fe);
-#pragma unroll
-                for (int v = 0; v < 3; ++v) sF[((3 + v) * NG + gp) * max_edges + le] = Fe[v];
-            }
-#pragma unroll
-            for (int v = 0; v < 3; ++v) sF[(v * NG + gp) * max_edges + le] = Fi[v];
+                for (int v = 0; v < 3; ++v) sF[(v * NG + gp) * max_edges + le] = Fi[v];
+            });
         }
     }
     __syncthreads();
@@ -573,38 +606,53 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
         const int slot = (es.x >> (10 * f)) & 1023;
         if (!sflag[slot]) continue;
         const bool is_in = (roles >> f) & 1;
-        const Real sJ = (Real)ssJ[slot];
-        const Real* ft = sfphi + f * ND * NG;
+        const Real sJ = ssJ[slot];
+        Real F[3][NG];
 #pragma unroll
         for (int gp = 0; gp < NG; ++gp) {  // own Gauss point order
-            Real F[3];
             if (is_in) {
 #pragma unroll
-                for (int v = 0; v < 3; ++v) F[v] = sF[(v * NG + gp) * max_edges + slot];
+                for (int v = 0; v < 3; ++v) F[v][gp] = sF[(v * NG + gp) * max_edges + slot];
             } else {
                 const int ga = NG - 1 - gp;
 #pragma unroll
                 for (int v = 0; v < 3; ++v)
-                    F[v] = WD ? sF[((3 + v) * NG + ga) * max_edges + slot] : -sF[(v * NG + ga) * max_edges + slot];
-            }
-            const Real wsJ = sgw[gp] * sJ;
-#pragma unroll
-            for (int k = 0; k < ND; ++k) {
-                const Real ph = ft[k * NG + gp] * wsJ;
-#pragma unroll
-                for (int v = 0; v < 3; ++v) rhs[v][k] -= F[v] * ph;
+                    F[v][gp] = WD ? sF[((3 + v) * NG + ga) * max_edges + slot] : -sF[(v * NG + ga) * max_edges + slot];
             }
         }
+        auto contrib = [&](auto FF) {
+            constexpr int fc = decltype(FF)::value;
+            sfor<0, NG>([&](auto GP) {
+                constexpr int gp = decltype(GP)::value;
+                const Real wsJ = (Real)MT<P>::gw(gp) * sJ;
+                sfor<0, ND>([&](auto K) {
+                    constexpr int k = decltype(K)::value;
+                    constexpr double c = MT<P>::fphi((fc * ND + k) * NG + gp);
+                    if constexpr (c != 0.0) {
+                        const Real ph = (Real)c * wsJ;
+#pragma unroll
+                        for (int v = 0; v < 3; ++v) rhs[v][k] -= F[v][gp] * ph;
+                    }
+                });
+            });
+        };
+        if (f == 0)
+            contrib(IC<0>{});
+        else if (f == 1)
+            contrib(IC<1>{});
+        else
+            contrib(IC<2>{});
     }
     // M^-1 (diagonal master mass inverse over |J|) and the SSP-RK stage combination
-    const double iaJ = 1.0 / aJ;
+    const Real iaJ = Real(1) / aJ;
     Real qn[3][ND];
+    sfor<0, ND>([&](auto K) {
+        constexpr int k = decltype(K)::value;
+        const Real mk = (Real)MT<P>::minv(k) * iaJ;
 #pragma unroll
-    for (int v = 0; v < 3; ++v)
-#pragma unroll
-        for (int k = 0; k < ND; ++k) {
-            const Real sol = rhs[v][k] * (Real)(T.minv[k] * iaJ);
-            const int idx = (v * ND + k) * A.ne_pad + d;
+        for (int v = 0; v < 3; ++v) {
+            const Real sol = rhs[v][k] * mk;
+            const int idx = (v * ND + k) * P_ + d;
             if (A.store_sol) A.sol_out[idx] = sol;
             Real acc = Real(0);
             for (int j = 0; j < A.nterms - 1; ++j) {
@@ -615,9 +663,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
             acc += (Real)A.a[j] * sq[(v * ND + k) * TILE + tid] + (Real)A.bdt[j] * sol;
             qn[v][k] = acc;
         }
+    });
     bool wet_new = wet;
     if (WD) {
-        const double bv[3] = {A.nz[snode[tid]], A.nz[snode[TILE + tid]], A.nz[snode[2 * TILE + tid]]};
+        const double bv[3] = {A.nz[A.enodes[d]], A.nz[A.enodes[P_ + d]], A.nz[A.enodes[2 * P_ + d]]};
         const double bmin = fmin(bv[0], fmin(bv[1], bv[2]));
         wet_new = wetting_drying<ND, Real>(qn, bv, bmin, A.h_o, A.h_o_thr, wet);
     }
@@ -627,7 +676,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
 #pragma unroll
         for (int k = 0; k < ND; ++k) {
             has_nan |= isnan((double)qn[v][k]);
-            A.q_out[(v * ND + k) * A.ne_pad + d] = qn[v][k];
+            A.q_out[(v * ND + k) * P_ + d] = qn[v][k];
         }
     A.wet_out[d] = wet_new ? 1 : 0;
     if (A.baryctr) {
@@ -637,7 +686,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
         for (int v = 0; v < 3; ++v) {
             const double a = qn[v][0], b = qn[v][1], c = qn[v][2];
             const double l0 = a - b - c, l1 = a - b + c, l2 = a + 2.0 * b;
-            A.baryctr[v * A.ne_pad + d] = l0 * (1.0 / 3.0) + l1 * (1.0 / 3.0) + l2 * (1.0 / 3.0);
+            A.baryctr[v * P_ + d] = l0 * (1.0 / 3.0) + l1 * (1.0 / 3.0) + l2 * (1.0 / 3.0);
         }
     }
     if (has_nan) {
@@ -646,41 +695,37 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value)) rkdg_
     }
 }
 
-}  // namespace dgsw
-
-
-namespace dgsw {
 // launchers, one translation unit per (order, precision)
-cudaError_t launch_stage_p1_f64(const StageArgs<double>& A, int tile, int ntiles, int max_edges, bool wd, bool fsrc,
-                                cudaStream_t s);
-cudaError_t launch_stage_p1_f32(const StageArgs<float>& A, int tile, int ntiles, int max_edges, bool wd, bool fsrc,
-                                cudaStream_t s);
-cudaError_t launch_stage_p2_f64(const StageArgs<double>& A, int tile, int ntiles, int max_edges, bool wd, bool fsrc,
-                                cudaStream_t s);
-cudaError_t launch_stage_p2_f32(const StageArgs<float>& A, int tile, int ntiles, int max_edges, bool wd, bool fsrc,
-                                cudaStream_t s);
+cudaError_t launch_stage_p1_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
+                                bool fsrc, cudaStream_t s);
+cudaError_t launch_stage_p1_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
+                                bool fsrc, cudaStream_t s);
+cudaError_t launch_stage_p2_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
+                                bool fsrc, cudaStream_t s);
+cudaError_t launch_stage_p2_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
+                                bool fsrc, cudaStream_t s);
 
 template <int P, typename Real, bool WD, bool FSRC, int TILE>
-cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_edges, cudaStream_t s) {
+cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo, int max_edges, cudaStream_t s) {
     auto kern = rkdg_stage_kernel<P, Real, WD, FSRC, TILE>;
-    const size_t smem = Smem<P, Real, WD>::bytes(TILE, max_edges);
+    const size_t smem = Smem<P, Real, WD>::bytes(TILE, max_halo, max_edges);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(unsigned)ntiles, TILE, smem, s>>>(A, max_edges);
+    kern<<<(unsigned)ntiles, TILE, smem, s>>>(A, max_halo, max_edges);
     return cudaGetLastError();
 }
 
 template <int P, typename Real>
-cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles, int max_edges, bool wd, bool fsrc,
-                                  cudaStream_t s) {
-#define DGSW_TILE_CASES(WD_, FS_)                                                    \
-    switch (tile) {                                                                   \
-        case 128:                                                                     \
-            return launch_stage_impl<P, Real, WD_, FS_, 128>(A, ntiles, max_edges, s); \
-        case 256:                                                                     \
-            return launch_stage_impl<P, Real, WD_, FS_, 256>(A, ntiles, max_edges, s); \
-        default:                                                                      \
-            return cudaErrorInvalidValue;                                             \
+cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
+                                  bool fsrc, cudaStream_t s) {
+#define DGSW_TILE_CASES(WD_, FS_)                                                               \
+    switch (tile) {                                                                              \
+        case 128:                                                                                \
+            return launch_stage_impl<P, Real, WD_, FS_, 128>(A, ntiles, max_halo, max_edges, s); \
+        case 256:                                                                                \
+            return launch_stage_impl<P, Real, WD_, FS_, 256>(A, ntiles, max_halo, max_edges, s); \
+        default:                                                                                 \
+            return cudaErrorInvalidValue;                                                        \
     }
     if (wd) {
         if (fsrc) {
@@ -697,6 +742,7 @@ cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles
     }
 #undef DGSW_TILE_CASES
 }
+
 }  // namespace dgsw
 
 #endif
