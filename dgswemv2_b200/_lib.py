@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdgsw_rkdg.so")
 
 DGSW_FP64, DGSW_FP32 = 0, 1
+DGSW_L2_STATIC_MAX_ELEMS = 1048576
 
 STATUS = {
     0: "ok",
@@ -115,6 +116,8 @@ SIGNATURES = {
     "dgsw_rkdg_get_time": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "dgsw_rkdg_l2_error": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "dgsw_rkdg_mass": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "dgsw_l2_error_static": (C.c_int32, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                         C.POINTER(C.c_double), C.c_double, C.c_void_p, C.POINTER(C.c_double)]),
     "dgsw_rkdg_topology": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "dgsw_mesh_topology": (C.c_int32, [C.POINTER(Mesh), C.POINTER(C.c_int32), C.POINTER(C.c_uint8),

@@ -75,6 +75,11 @@ __global__ void advance_clock_kernel(DevClock* c, double dt) {
 
 }  // namespace
 
+namespace dgsw {
+// the per-thread error message for entry points defined in other translation units
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace dgsw
+
 struct dgsw_rkdg_s {
     dgsw_config cfg;
     Tables tb;

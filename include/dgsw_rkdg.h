@@ -136,6 +136,26 @@ int32_t dgsw_rkdg_l2_error(dgsw_handle h, double* out);
  * the global mass balance check of the FP32 path) */
 int32_t dgsw_rkdg_mass(dgsw_handle h, double* out);
 
+/* Allocation-free L2 error of a caller-owned FP64 state; no counterpart in the reference.
+ * For callers that may not allocate device memory during a run: drivers whose memory pool (PyTorch's
+ * caching allocator, a coupler's arena) already holds the GPU's memory, and monitoring code between
+ * asynchronously queued steps, where cudaMalloc/cudaFree can synchronise the device. It calls no
+ * cudaMalloc, cudaFree or other allocating routine and needs no handle; its scratch is a fixed static
+ * device array of 32 KiB per device, so n_elems is limited to DGSW_L2_STATIC_MAX_ELEMS (larger inputs
+ * are rejected with DGSW_ERR_INVALID_ARGUMENT; dgsw_rkdg_l2_error has no such limit).
+ * Same value as dgsw_rkdg_l2_error up to summation order. Inputs, all on the current device:
+ * d_q [n_elems][3][ndof] FP64 (the layout dgsw_rkdg_get_state_device writes for an FP64 handle),
+ * d_elem_nodes [n_elems][3] 0-based node indices, d_node_xyz [n_nodes][3] (x, y, depth);
+ * function_set / fn_params (16 values, NULL = zeros) / t select true_q. Work is queued on `stream`
+ * (NULL = default stream) and the call returns after it completes, with the result in *out (host).
+ * The first call on a device does a one-time set-up (copies the quadrature table to the device and
+ * looks up the scratch address); make that first call before any stream capture. All calls on one
+ * device share the scratch array: calls that overlap on the GPU race and may return wrong values. */
+#define DGSW_L2_STATIC_MAX_ELEMS 1048576
+int32_t dgsw_l2_error_static(int32_t p, int64_t n_elems, const double* d_q, const int32_t* d_elem_nodes,
+                             const double* d_node_xyz, int32_t function_set, const double* fn_params, double t,
+                             void* stream, double* out);
+
 /* integer topology in ascending element-ID order, for bit-exact comparison with the reference's
  * MeshMetaData (mesh_metadata.cpp:3-85) and interface/boundary creation (swe_pre_create_intface.hpp,
  * swe_pre_create_bound.hpp): neighbor element index per face (-1 none), boundary type per face
