@@ -346,7 +346,7 @@ struct Smem {
 // resident CTAs per SM the register budget is sized for
 template <int P, typename Real, int TILE>
 struct MinBlocks {
-    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? 4 : 2) : (TILE == 128 ? 3 : 1);
+    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? 4 : 2) : (TILE == 128 ? 2 : 1);
 };
 
 template <int P, typename Real, bool WD, bool FSRC, int TILE>
