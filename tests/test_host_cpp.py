@@ -1,0 +1,226 @@
+"""The C++ host side (include/dgsw_rkdg_problem.hpp): `.15` YAML + ADCIRC parsing mirrors the reference's
+InputParameters / SWE::Inputs / AdcircFormat, and the dgswemv2-b200-serial driver runs an input file
+end to end on the GPU.
+
+CPU tests compile tests/cpp/parse_check.cpp against the header and compare what it read with the values
+written and with the Python mesh arrays (bit-exact hashes, host-only topology included)."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from dgswemv2_b200 import Problem, configs, mesh_topology, meshgen
+from dgswemv2_b200.types import FUNCTION, LAND, OUTFLOW
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "dgswemv2_b200")
+CLI = os.path.join(PKG, "dgswemv2-b200-serial")
+
+
+@pytest.fixture(scope="module")
+def parse_check(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("cpp") / "parse_check")
+    subprocess.check_call(["g++", "-O1", "-std=c++17", "-Wall", "-Werror", "-o", exe,
+                           os.path.join(ROOT, "tests", "cpp", "parse_check.cpp"), "-L" + PKG, "-ldgsw_rkdg",
+                           "-Wl,-rpath," + PKG])
+    return exe
+
+
+def run_check(exe, path):
+    r = subprocess.run([exe, path], capture_output=True, text=True)
+    out = {}
+    for line in r.stdout.splitlines():
+        k, _, v = line.partition(" ")
+        out[k] = v
+    return r.returncode, out, r.stderr
+
+
+def fnv(arr):
+    h = 1469598103934665603
+    for b in np.ascontiguousarray(arr).tobytes():
+        h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return str(h)
+
+
+def write_input(d, mesh, body, mesh_name="mesh.14"):
+    meshgen.write_adcirc(mesh, os.path.join(d, mesh_name))
+    path = os.path.join(d, "input.15")
+    with open(path, "w") as f:
+        f.write(body.replace("@MESH@", mesh_name))
+    return path
+
+
+CONFIG1_15 = """###############################################################################
+#  config 1: manufactured solution, p=1, SSP-RK2, dt = 1 s, 1000 steps
+###############################################################################
+
+mesh:
+  format: Adcirc
+  file_name: @MESH@
+  coordinate_system: cartesian
+
+timestepping:
+  start_time: 01-01-2000 00:00:00      # dd-mm-yyyy hh:mm:ss
+  end_time: 01-01-2000 00:16:40
+  dt: 1.0
+  order: 2
+  nstages: 2
+
+polynomial_order: 1
+
+problem:
+  name: rkdg_swe
+  gravity: 9.81
+  density_water: 1000
+  density_air: 1.225
+  initial_conditions:
+    type: Function
+  function_source: Enable
+
+b200:
+  function_set: manufactured_sine
+  function_parameters: [40000, 0.1, 2.0, 0.0, 9.81]
+  precision: fp64
+"""
+
+
+def test_parse_config1_input_and_mesh(parse_check, tmp_path):
+    mesh, cfg = configs.config1()
+    rc, out, err = run_check(parse_check, write_input(str(tmp_path), mesh, CONFIG1_15))
+    assert rc == 0, (out, err)
+    assert out["p"] == "1" and out["mesh_format"] == "Adcirc" and out["mesh_file"] == "mesh.14"
+    assert out["bcis_file"] == "mesh.bcis" and out["coordinate_system"] == "cartesian"
+    assert float(out["run_time"]) == 1000.0 and float(out["dt"]) == 1.0
+    assert out["order"] == "2" and out["nstages"] == "2" and out["name"] == "rkdg_swe"
+    assert float(out["g"]) == 9.81 and float(out["rho_air"]) == 1.225
+    assert out["ic_type"] == "1" and out["function_source"] == "1"
+    assert out["wetting_drying"] == "0" and out["slope_limiting"] == "0"
+    assert float(out["h_o"]) == 0.1 and float(out["sl_M"]) == 1e-8 and float(out["sl_nu"]) == 1.5  # defaults
+    assert out["function_set"] == "2" and out["precision"] == "0" and out["n_params"] == "5"
+    # the mesh round trip is bit-exact (names are 0..n-1, so ascending-name order is the input order)
+    assert out["mesh_name"] == mesh.name
+    assert int(out["n_nodes"]) == mesh.n_nodes and int(out["n_elems"]) == mesh.n_elems
+    assert out["node_xyz_hash"] == fnv(mesh.node_xyz.astype(np.float64))
+    assert out["elem_nodes_hash"] == fnv(mesh.elem_nodes.astype(np.int32))
+    assert out["elem_ids_hash"] == fnv(np.arange(mesh.n_elems, dtype=np.uint32))
+    assert out["seg_type_hash"] == fnv(mesh.seg_type.astype(np.int32))
+    assert out["seg_nodes_hash"] == fnv(mesh.seg_nodes.astype(np.int32))
+    nbr, bt, intf, bnd = mesh_topology(mesh)
+    assert int(out["n_interfaces"]) == len(intf) and int(out["n_boundaries"]) == len(bnd)
+    assert out["neighbors_hash"] == fnv(nbr) and out["btype_hash"] == fnv(bt)
+    assert out["interfaces_hash"] == fnv(intf) and out["boundaries_hash"] == fnv(bnd)
+
+
+BOWL_15 = """mesh:
+  format: Adcirc
+  file_name: '@MESH@'
+  coordinate_system: cartesian
+timestepping:
+  start_time: 15-11-1987 12:00              #dd-mm-yyyy hh:mm
+  end_time: 15-11-1987 13:00                #dd-mm-yyyy hh:mm
+  dt: 0.25
+  order: 2
+  nstages: 2
+polynomial_order: 1
+problem:
+  name: rkdg_swe
+  initial_conditions:
+    type: Constant
+    initial_surface_height: 0.5
+    initial_momentum_x: -1.5e-2
+    initial_momentum_y: 0
+  wetting_drying:
+    h_o: 0.01
+  slope_limiting:
+    type: Cockburn-Shu
+    M: 1.0e-6
+    nu: 1.25
+output:
+  path: out
+  modal:
+    frequency: 10
+"""
+
+
+def test_parse_bowl_style_input(parse_check, tmp_path):
+    """Constant IC, wetting/drying and Cockburn-Shu nodes, quoted scalars, end-of-line comments, times without
+    seconds (strptime stops at the missing field, as in the reference's own bowl example), and a mesh whose
+    elements are listed with shuffled names (the reader orders them by name) and with outflow segments."""
+    mesh = meshgen.quad_mesh(6, 5, bc=(LAND, OUTFLOW, FUNCTION, LAND), jitter=0.1, seed=4,
+                             bathymetry=meshgen.bath_flat(3.0))
+    rng = np.random.default_rng(0)
+    mesh.elem_ids = rng.permutation(mesh.n_elems).astype(np.uint32) * 3 + 7
+    rc, out, err = run_check(parse_check, write_input(str(tmp_path), mesh, BOWL_15))
+    assert rc == 0, (out, err)
+    assert float(out["run_time"]) == 3600.0 and float(out["dt"]) == 0.25
+    assert float(out["g"]) == 9.81  # default
+    assert out["ic_type"] == "0" and [float(v) for v in out["ic_const"].split()] == [0.5, -1.5e-2, 0.0]
+    assert out["wetting_drying"] == "1" and float(out["h_o"]) == 0.01
+    assert out["slope_limiting"] == "1" and float(out["sl_M"]) == 1.0e-6 and float(out["sl_nu"]) == 1.25
+    assert out["writing_modal"] == "1 40" and out["function_set"] == "0"
+    order = np.argsort(mesh.elem_ids, kind="stable")
+    assert out["elem_nodes_hash"] == fnv(mesh.elem_nodes[order].astype(np.int32))
+    assert out["elem_ids_hash"] == fnv(np.sort(mesh.elem_ids).astype(np.uint32))
+    nbr, bt, intf, bnd = mesh_topology(mesh)  # the library orders by element ID itself
+    assert out["neighbors_hash"] == fnv(nbr) and out["interfaces_hash"] == fnv(intf)
+    assert out["boundaries_hash"] == fnv(bnd)
+
+
+@pytest.mark.parametrize("edit, status, text", [
+    (lambda s: s.replace("polynomial_order: 1\n", ""), "-1", "P YAML node not specified"),
+    (lambda s: s.replace("  dt: 1.0\n", ""), "-1", "Timestepping YAML node is malformatted"),
+    (lambda s: s.replace("format: Adcirc", "format: Gmsh"), "-1", "Unsupported mesh format: Gmsh"),
+    (lambda s: s.replace("cartesian", "conic"), "-1", "Unsupported coordinate system: conic"),
+    (lambda s: s.replace("  function_source: Enable\n", "  bottom_friction:\n    type: Chezy\n    coefficient: 0.1\n"),
+     "5", "bottom friction"),
+    (lambda s: s.replace("function_set: manufactured_sine", "function_set: tsunami"), "-1", "unknown b200.function_set"),
+    (lambda s: s.replace("name: rkdg_swe", "name: ehdg_swe"), "5", "is not rkdg_swe"),
+])
+def test_input_errors(parse_check, tmp_path, edit, status, text):
+    mesh, _ = configs.config1()
+    rc, out, _ = run_check(parse_check, write_input(str(tmp_path), mesh, edit(CONFIG1_15)))
+    assert rc == 3 and out["error"].split(" ", 1)[0] == status and text in out["error"], out
+
+
+def test_mesh_errors(parse_check, tmp_path):
+    mesh, _ = configs.config1()
+    path = write_input(str(tmp_path), mesh, CONFIG1_15)
+    mpath = os.path.join(str(tmp_path), "mesh.14")
+    src = open(mpath).read()
+    # an undefined IBTYPE is rejected like AdcircFormat does
+    open(mpath, "w").write(src.replace("77 = Number of nodes for land boundary 1", "5 = Number of nodes for land boundary 1"))
+    rc, out, _ = run_check(parse_check, path)
+    assert rc == 3 and "undefined boundary type in ADCIRC mesh: 5" in out["error"]
+    # internal barriers (levees) are unsupported
+    open(mpath, "w").write(src.replace("77 = Number of nodes for land boundary 1", "4 = Number of nodes for land boundary 1"))
+    rc, out, _ = run_check(parse_check, path)
+    assert rc == 3 and out["error"].startswith("5 ") and "levee" in out["error"]
+    # an island segment (IBTYPE 1) is read but never matched: its edges then have no boundary type
+    open(mpath, "w").write(src.replace("77 = Number of nodes for land boundary 1", "1 = Number of nodes for land boundary 1"))
+    rc, out, _ = run_check(parse_check, path)
+    assert rc == 3 and "boundary not found" in out["error"]
+    os.remove(mpath)
+    rc, out, _ = run_check(parse_check, path)
+    assert rc == 3 and "was not found" in out["error"]
+
+
+@pytest.mark.gpu
+def test_serial_driver_runs_config1(tmp_path, oracle):
+    """dgswemv2-b200-serial on the config-1 input: 1000 SSP-RK2 steps, L2 error equal to the FP64 oracle's
+    within 1e-12 relative."""
+    mesh, cfg = configs.config1()
+    path = write_input(str(tmp_path), mesh, CONFIG1_15)
+    r = subprocess.run([CLI, path], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    m = re.search(r"L2 error: ([0-9.eE+-]+)", r.stdout)
+    assert m and "Time Elapsed (in us)" in r.stdout, r.stdout
+    l2_cli = float(m.group(1))
+    O = oracle.problem(cfg, mesh, n_threads=8)
+    O.step(1000)
+    l2_ref = O.l2_error()
+    assert abs(l2_cli - l2_ref) <= 1e-12 * l2_ref, (l2_cli, l2_ref)
+    P = Problem(cfg, mesh)
+    P.step_serial(1000)
+    assert abs(P.compute_residual_L2() - l2_cli) <= 1e-13 * l2_ref
