@@ -164,6 +164,27 @@ class Problem:
         _lib.check(_lib.load().dgsw_rkdg_get_limited(self._h, _lib.ptr(w, C.c_uint8)))
         return w
 
+    # learned troubled-cell indicator ---------------------------------------------------------
+    def indicator_features(self, d_features, d_ok=0):
+        """Features [ne][18] (FP32) and limiter-looks flags [ne] of the current state into device buffers."""
+        _lib.check(_lib.load().dgsw_rkdg_indicator_features(self._h, C.c_void_p(d_features), C.c_void_p(d_ok or None)))
+
+    def stage_record(self, d_features, d_labels):
+        """One stage with the plain limiter, recording pre-limiter features and the limiter's decisions."""
+        _lib.check(_lib.load().dgsw_rkdg_stage_record(self._h, C.c_void_p(d_features), C.c_void_p(d_labels)))
+
+    def set_indicator(self, params, confidence=0.9, mode=1):
+        """mode 0 plain limiter, 1 MLP-gated limiter, 2 plain limiter with the gate's misses counted."""
+        prm = np.ascontiguousarray(params, np.float32)
+        assert prm.size == _lib.DGSW_MLP_NPARAM
+        _lib.check(_lib.load().dgsw_rkdg_set_indicator(self._h, _lib.ptr(prm, C.c_float), float(confidence), int(mode)))
+
+    def indicator_stats(self, reset=False):
+        """(considered, sent to the limiter, limited, missed) cell counts since the last reset."""
+        c = (C.c_int64 * 4)()
+        _lib.check(_lib.load().dgsw_rkdg_indicator_stats(self._h, c, int(reset)))
+        return tuple(int(v) for v in c)
+
     def set_state_device(self, dptr):
         _lib.check(_lib.load().dgsw_rkdg_set_state_device(self._h, C.c_void_p(dptr)))
 

@@ -13,6 +13,8 @@ LIB_PATH = os.path.join(_HERE, "libdgsw_rkdg.so")
 
 DGSW_FP64, DGSW_FP32 = 0, 1
 DGSW_L2_STATIC_MAX_ELEMS = 1048576
+DGSW_MLP_NPARAM = 5441
+DGSW_MLP_NFEATURES = 18
 
 STATUS = {
     0: "ok",
@@ -124,6 +126,16 @@ SIGNATURES = {
                                        C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int32)]),
     "dgsw_rkdg_get_limited": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "dgsw_rkdg_indicator_features": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dgsw_rkdg_stage_record": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dgsw_rkdg_set_indicator": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.c_double, C.c_int32]),
+    "dgsw_rkdg_indicator_stats": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64), C.c_int32]),
+    "dgsw_mlp_forward": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "dgsw_mlp_grad_work_floats": (C.c_int64, [C.c_int64]),
+    "dgsw_mlp_grad": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
+                                  C.c_int64, C.c_void_p, C.c_void_p]),
+    "dgsw_mlp_adam": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_float,
+                                  C.c_float, C.c_float, C.c_void_p]),
     "dgsw_rkdg_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_synchronize": (C.c_int32, [C.c_void_p]),
     "dgsw_rkdg_last_step_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

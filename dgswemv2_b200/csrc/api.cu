@@ -12,6 +12,7 @@
 
 #include "../../include/dgsw_rkdg.h"
 #include "host_setup.h"
+#include "indicator.cuh"
 #include "limiter_kernel.cuh"
 #include "quadrature.h"
 #include "reduce_kernels.cuh"
@@ -131,6 +132,17 @@ struct dgsw_rkdg_s {
     int64_t last_launches = 0;
     size_t smem_bytes = 0;
     int tile = 256;
+    int64_t graph_launches[4] = {0, 0, 0, 0};  // kernels one replay of graph[key] launches
+    // troubled-cell indicator (mode 0 off, 1 gate the limiter, 2 shadow: plain limiter, misses counted)
+    int ind_mode = 0;
+    float ind_skip_below = 0.1f;
+    DBuf<float> ind_params;
+    DBuf<int> ind_list;
+    DBuf<int> ind_count;
+    DBuf<unsigned char> ind_gate;
+    DBuf<unsigned long long> ind_counters;
+    DBuf<int> ind_error;
+    int sm_count = 148;
 };
 
 namespace {
@@ -225,11 +237,68 @@ cudaError_t launch_limiter(dgsw_rkdg_s* h, int s_out) {
     L.nu = h->cfg.sl_nu;
     L.status = h->status.p;
     L.ref_of_dev = h->ref_of_dev.p;
+    if (h->ind_mode == 1) {
+        L.list = h->ind_list.p;
+        L.list_count = h->ind_count.p;
+        L.counters = h->ind_counters.p;
+        return launch_limiter_kernel<Real>(L, h->cfg.p, h->stream, 8 * h->sm_count);
+    }
+    if (h->ind_mode == 2) {
+        L.gate = h->ind_gate.p;
+        L.counters = h->ind_counters.p;
+    }
     return launch_limiter_kernel<Real>(L, h->cfg.p, h->stream);
 }
 
-// one RK stage: stage kernel, (clock on the last stage), limiter, wet flag buffer flip
-cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches) {
+template <typename Real>
+FeatureArgs<Real> feature_args(dgsw_rkdg_s* h, int s_out) {
+    FeatureArgs<Real> F;
+    F.q = (const Real*)h->Q[s_out];
+    F.wet = h->wet[h->wet_cur].p;
+    F.nbr = h->nbr.p;
+    F.enodes = h->enodes.p;
+    F.nz = h->nz.p;
+    F.ne = (int)h->ne;
+    F.ne_pad = (int)h->ne_pad;
+    F.nd = h->nd;
+    return F;
+}
+
+// the indicator pass before the limiter: features + MLP on the tensor cores -> work list or gate flags
+template <typename Real>
+cudaError_t launch_indicator_gate(dgsw_rkdg_s* h, int s_out) {
+    TcArgs T;
+    std::memset(&T, 0, sizeof(T));
+    T.params = h->ind_params.p;
+    T.mode = h->ind_mode;
+    T.skip_below = h->ind_skip_below;
+    T.list = h->ind_list.p;
+    T.list_count = h->ind_count.p;
+    T.gate = h->ind_gate.p;
+    T.limited = h->limited.p;
+    T.counters = h->ind_counters.p;
+    T.error = h->ind_error.p;
+    if (h->ind_mode == 1) {
+        cudaError_t e = cudaMemsetAsync(h->ind_count.p, 0, sizeof(int), h->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return launch_mlp_tc<Real>(T, feature_args<Real>(h, s_out), h->stream);
+}
+
+struct StageRecord {
+    float* features;  // [ne][18], reference order (device)
+    uint8_t* labels;  // [ne], reference order (device): limiter decision, 255 where it does not look
+};
+
+__global__ void record_labels_kernel(const unsigned char* limited, const int* ref_of_dev, int ne, uint8_t* labels) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= ne) return;
+    const int r = ref_of_dev[d];
+    labels[r] = labels[r] ? limited[d] : (uint8_t)255;
+}
+
+// one RK stage: stage kernel, (clock on the last stage), indicator, limiter, wet flag buffer flip
+cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageRecord* rec = nullptr) {
     cudaError_t e = h->fp32 ? launch_stage<float>(h, s) : launch_stage<double>(h, s);
     if (e != cudaSuccess) return e;
     ++launches;
@@ -244,8 +313,36 @@ cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches) {
         h->qswap ^= 1;
         s_out = 0;
     }
+    if (rec) {
+        // features of the state the limiter is about to see; ok flags into the label buffer
+        e = h->fp32 ? launch_indicator_features<float>(feature_args<float>(h, s_out), h->ref_of_dev.p, rec->features,
+                                                        rec->labels, h->stream)
+                    : launch_indicator_features<double>(feature_args<double>(h, s_out), h->ref_of_dev.p,
+                                                         rec->features, rec->labels, h->stream);
+        if (e != cudaSuccess) return e;
+        ++launches;
+    }
     if (h->cfg.slope_limiting) {
+        const int mode = h->ind_mode;
+        if (rec) h->ind_mode = 0;  // labels come from the plain limiter
+        if (h->ind_mode) {
+            e = h->fp32 ? launch_indicator_gate<float>(h, s_out) : launch_indicator_gate<double>(h, s_out);
+            if (e != cudaSuccess) return e;
+            ++launches;
+        }
         e = h->fp32 ? launch_limiter<float>(h, s_out) : launch_limiter<double>(h, s_out);
+        h->ind_mode = mode;
+        if (e != cudaSuccess) return e;
+        ++launches;
+    }
+    if (rec) {
+        if (!h->cfg.slope_limiting) {
+            e = cudaMemsetAsync(h->limited.p, 0, h->ne_pad, h->stream);
+            if (e != cudaSuccess) return e;
+        }
+        record_labels_kernel<<<(unsigned)((h->ne + 255) / 256), 256, 0, h->stream>>>(h->limited.p, h->ref_of_dev.p,
+                                                                                     (int)h->ne, rec->labels);
+        e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         ++launches;
     }
@@ -479,6 +576,8 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return cleanup_fail("stream", e);
     h->own_stream = true;
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
+    if (h->sm_count <= 0) h->sm_count = 148;
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
     const size_t state_bytes = (size_t)3 * h->nd * h->ne_pad * h->real_size;
@@ -638,6 +737,12 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     h->limited.release();
     h->nbr.release();
     h->baryctr.release();
+    h->ind_params.release();
+    h->ind_list.release();
+    h->ind_count.release();
+    h->ind_gate.release();
+    h->ind_counters.release();
+    h->ind_error.release();
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -721,6 +826,85 @@ int32_t dgsw_rkdg_get_limited(dgsw_handle h, uint8_t* flags) {
     return DGSW_OK;
 }
 
+int32_t dgsw_rkdg_indicator_features(dgsw_handle h, float* d_features, uint8_t* d_ok) {
+    if (!h || !d_features) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (h->cfg.p != 1) return fail(DGSW_ERR_UNSUPPORTED, "the troubled-cell indicator is defined for p = 1");
+    cudaSetDevice(h->device);
+    cudaError_t e = h->fp32 ? launch_indicator_features<float>(feature_args<float>(h, h->stage), h->ref_of_dev.p,
+                                                               d_features, d_ok, h->stream)
+                            : launch_indicator_features<double>(feature_args<double>(h, h->stage), h->ref_of_dev.p,
+                                                                d_features, d_ok, h->stream);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("indicator features: ") + cudaGetErrorString(e));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_stage_record(dgsw_handle h, float* d_features, uint8_t* d_labels) {
+    if (!h || !d_features || !d_labels) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (h->cfg.p != 1) return fail(DGSW_ERR_UNSUPPORTED, "the troubled-cell indicator is defined for p = 1");
+    cudaSetDevice(h->device);
+    int64_t launches = 0;
+    StageRecord rec{d_features, d_labels};
+    cudaError_t e = enqueue_stage(h, h->stage, launches, &rec);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("stage: ") + cudaGetErrorString(e));
+    advance_host_stepper(h);
+    return check_status(h);
+}
+
+int32_t dgsw_rkdg_set_indicator(dgsw_handle h, const float* params, double confidence, int32_t mode) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (mode < 0 || mode > 2) return fail(DGSW_ERR_INVALID_ARGUMENT, "indicator mode must be 0, 1 or 2");
+    cudaSetDevice(h->device);
+    if (mode == 0) {
+        if (h->ind_mode != 0) destroy_graphs(h);
+        h->ind_mode = 0;
+        return DGSW_OK;
+    }
+    if (!params) return fail(DGSW_ERR_INVALID_ARGUMENT, "null indicator parameters");
+    if (!h->cfg.slope_limiting) return fail(DGSW_ERR_INVALID_ARGUMENT, "the indicator gates the slope limiter, "
+                                                                       "which this problem does not use");
+    if (h->cfg.p != 1) return fail(DGSW_ERR_UNSUPPORTED, "the troubled-cell indicator is defined for p = 1");
+    if (!(confidence >= 0.5 && confidence <= 1.0))
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "indicator confidence must lie in [0.5, 1]");
+    cudaError_t e;
+    if (!h->ind_params.p) {
+        if ((e = h->ind_params.alloc(MLP_NPARAM)) != cudaSuccess ||
+            (e = h->ind_list.alloc(h->ne_pad)) != cudaSuccess || (e = h->ind_count.alloc(1)) != cudaSuccess ||
+            (e = h->ind_gate.alloc(h->ne_pad)) != cudaSuccess ||
+            (e = h->ind_counters.alloc(IND_NCOUNTERS)) != cudaSuccess || (e = h->ind_error.alloc(1)) != cudaSuccess)
+            return fail(DGSW_ERR_CUDA, std::string("indicator buffers: ") + cudaGetErrorString(e));
+        h->device_bytes += (int64_t)MLP_NPARAM * 4 + h->ne_pad * 5 + 64;
+        CUDA_TRY(cudaMemsetAsync(h->ind_counters.p, 0, IND_NCOUNTERS * sizeof(unsigned long long), h->stream));
+        CUDA_TRY(cudaMemsetAsync(h->ind_error.p, 0, sizeof(int), h->stream));
+        CUDA_TRY(cudaMemsetAsync(h->ind_count.p, 0, sizeof(int), h->stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->ind_params.p, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->ind_mode != mode) destroy_graphs(h);
+    h->ind_mode = mode;
+    h->ind_skip_below = (float)(1.0 - confidence);
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_indicator_stats(dgsw_handle h, int64_t* counts, int32_t reset) {
+    if (!h || !counts) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    for (int i = 0; i < 4; ++i) counts[i] = 0;
+    if (!h->ind_counters.p) return DGSW_OK;
+    cudaSetDevice(h->device);
+    unsigned long long c[IND_NCOUNTERS];
+    int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(c, h->ind_counters.p, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(&err, h->ind_error.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < 4; ++i) counts[i] = (int64_t)c[i];
+    if (reset) {
+        CUDA_TRY(cudaMemsetAsync(h->ind_counters.p, 0, sizeof(c), h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    if (err) return fail(DGSW_ERR_CUDA, "indicator: a tensor-core wait timed out");
+    return DGSW_OK;
+}
+
 int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
     if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
@@ -791,18 +975,17 @@ int32_t dgsw_rkdg_step(dgsw_handle h, int32_t nsteps) {
                 if (ee != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("capture end: ") + cudaGetErrorString(ee));
                 CUDA_TRY(cudaGraphInstantiate(&h->graph[key], g, 0));
                 cudaGraphDestroy(g);
+                h->graph_launches[key] = l2;
             }
             CUDA_TRY(cudaGraphLaunch(h->graph[key], h->stream));
+            launches += h->graph_launches[key];
             // replay the host-side buffer rotation of one step
             for (int s = 0; s < h->ns; ++s) {
                 h->wet_cur = 1 - h->wet_cur;
                 if (s + 1 == h->ns) {
                     std::swap(h->Q[0], h->Q[h->ns]);
                     h->qswap ^= 1;
-                    ++launches;  // clock update
                 }
-                ++launches;
-                if (h->cfg.slope_limiting) ++launches;
             }
         } else {
             for (int s = 0; s < h->ns; ++s) {

@@ -30,12 +30,16 @@ struct LimiterArgs {
     double g, M, nu;
     void* status;
     const int* ref_of_dev;
+    // optional gating by the troubled-cell indicator
+    const int* list;                 // visit only list[0 .. *list_count) (NULL: every element)
+    const int* list_count;
+    const unsigned char* gate;       // write back only where gate[e] != 0 (NULL: everywhere)
+    unsigned long long* counters;    // [IND_LIMITED], [IND_MISSED] accumulators (NULL: none)
 };
 
+// the limiter decision for element e (1 if its state changes); the new state is written only if `write`
 template <int ND, typename Real>
-__global__ void __launch_bounds__(256) cs_limiter_kernel(const LimiterArgs<Real> L) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= L.ne) return;
+__device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real>& L, int e, bool write) {
     const size_t P = (size_t)L.ne_pad;
     unsigned char lim = 0;
     bool ok = L.wet[e] != 0;
@@ -52,10 +56,7 @@ __global__ void __launch_bounds__(256) cs_limiter_kernel(const LimiterArgs<Real>
             ok = ok && (bt == 0 || bt == 3);
         }
     }
-    if (!ok) {
-        L.limited[e] = 0;
-        return;
-    }
+    if (!ok) return 0;
     // own vertex values (T_basis_linear) and derived barycentre / midpoint values
     double ql[3][3], qb[3], qm[3][3];
 #pragma unroll
@@ -179,6 +180,7 @@ __global__ void __launch_bounds__(256) cs_limiter_kernel(const LimiterArgs<Real>
         }
         if (sqrt(d2) / sqrt(n2) > 1.0e-12) {
             lim = 1;
+            if (!write) continue;
             L.q[(v * ND + 0) * P + e] = (Real)(qv[0] * (1.0 / 3.0) + qv[1] * (1.0 / 3.0) + qv[2] * (1.0 / 3.0));
             L.q[(v * ND + 1) * P + e] = (Real)(qv[0] * (-1.0 / 6.0) + qv[1] * (-1.0 / 6.0) + qv[2] * (1.0 / 3.0));
             L.q[(v * ND + 2) * P + e] = (Real)(qv[0] * (-1.0 / 2.0) + qv[1] * (1.0 / 2.0));
@@ -186,12 +188,40 @@ __global__ void __launch_bounds__(256) cs_limiter_kernel(const LimiterArgs<Real>
             for (int k = 3; k < ND; ++k) L.q[(v * ND + k) * P + e] = Real(0);
         }
     }
-    L.limited[e] = lim;
+    return lim;
 }
 
+// One thread per visited element (every element, or the indicator's work list with a grid-stride loop).
+template <int ND, typename Real>
+__global__ void __launch_bounds__(256) cs_limiter_kernel(const LimiterArgs<Real> L) {
+    const int n = L.list ? *L.list_count : L.ne;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {  // block-uniform trip count
+        const int i = i0 + threadIdx.x;
+        bool applied = false, missed = false;
+        if (i < n) {
+            const int e = L.list ? L.list[i] : i;
+            const bool write = !L.gate || L.gate[e];
+            const bool lim = cs_limit_element<ND, Real>(L, e, write) != 0;
+            applied = lim && write;
+            missed = lim && !write;
+            L.limited[e] = applied ? 1 : 0;
+        }
+        if (L.counters) {
+            const unsigned ma = __ballot_sync(0xffffffffu, applied), mm = __ballot_sync(0xffffffffu, missed);
+            if ((threadIdx.x & 31) == 0) {
+                if (ma) atomicAdd(&L.counters[2], (unsigned long long)__popc(ma));
+                if (mm) atomicAdd(&L.counters[3], (unsigned long long)__popc(mm));
+            }
+        }
+    }
+}
+
+// grid: one block per 256 elements, or a persistent grid of `list_blocks` blocks over a work list
 template <typename Real>
-cudaError_t launch_limiter_kernel(const LimiterArgs<Real>& L, int p, cudaStream_t s) {
-    const int blocks = (L.ne + 255) / 256;
+cudaError_t launch_limiter_kernel(const LimiterArgs<Real>& L, int p, cudaStream_t s, int list_blocks = 0) {
+    const int blocks = L.list ? list_blocks : (L.ne + 255) / 256;
+    if (blocks <= 0) return cudaSuccess;
     if (p == 1)
         cs_limiter_kernel<3, Real><<<blocks, 256, 0, s>>>(L);
     else

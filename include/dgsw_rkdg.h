@@ -172,6 +172,46 @@ int32_t dgsw_mesh_topology(const dgsw_mesh* mesh, int32_t* neighbors, uint8_t* b
 /* per element 1 if the last slope-limiter pass changed its state (the plain limiter's decision) */
 int32_t dgsw_rkdg_get_limited(dgsw_handle h, uint8_t* flags);
 
+/* ---- learned troubled-cell indicator (no counterpart in the reference) ----------------------------
+ * An 18 -> 64 -> 64 -> 1 MLP (ReLU, sigmoid) predicts whether the Cockburn-Shu limiter
+ * (CS_slope_limiter_serial, swe_CS_sl_serial.hpp:9-23) will change a cell, from the cell's linear modal
+ * coefficients and its neighbours' means, scaled per field (18 features; p = 1 only). Parameters: FP32,
+ * DGSW_MLP_NPARAM values laid out W1[64][18], b1[64], W2[64][64], b2[64], w3[64], b3. Inference runs on the
+ * tensor cores (BF16 inputs and weights, FP32 accumulation); training runs in FP32. */
+#define DGSW_MLP_NPARAM 5441
+#define DGSW_MLP_NFEATURES 18
+
+/* features [n_elems][18] (FP32) and "the limiter looks at this cell" flags [n_elems] of the current
+ * state, in ascending element-ID order, into caller-owned device buffers (d_ok may be NULL) */
+int32_t dgsw_rkdg_indicator_features(dgsw_handle h, float* d_features, uint8_t* d_ok);
+/* one RK stage (as dgsw_rkdg_stage) with the plain limiter, recording the features of the state the
+ * limiter sees and its decisions as labels: 1 changed, 0 unchanged, 255 not looked at (device buffers,
+ * ascending element-ID order) - the training data of the indicator */
+int32_t dgsw_rkdg_stage_record(dgsw_handle h, float* d_features, uint8_t* d_labels);
+/* mode 0: plain limiter on every cell. mode 1: the MLP runs before each limiter pass and the limiter
+ * visits only cells with p >= 1 - confidence (cells the network is not confident are smooth fall back to
+ * the plain limiter). mode 2 (evaluation): the plain limiter decides every cell but writes back only
+ * the cells mode 1 would visit, counting the misses. params: host FP32 array of DGSW_MLP_NPARAM. */
+int32_t dgsw_rkdg_set_indicator(dgsw_handle h, const float* params, double confidence, int32_t mode);
+/* accumulated counts since the last reset: [0] cells the limiter would look at, [1] cells sent to it,
+ * [2] cells it changed, [3] cells it would have changed but the indicator skipped (mode 2) */
+int32_t dgsw_rkdg_indicator_stats(dgsw_handle h, int64_t* counts, int32_t reset);
+
+/* handle-free MLP kernels on caller-owned device buffers, stream-ordered on `stream` (NULL = default).
+ * forward: p[n] = MLP(x[n][18]); tensor_cores = 1 for the BF16 tcgen05 path (synchronises the stream),
+ * 0 for the FP32 CUDA-core path. grad: mean weighted binary cross-entropy
+ * -[w y log p + (1 - y) log(1 - p)] over the batch (y in {0, 1}) and its gradient into d_grad
+ * [DGSW_MLP_NPARAM]; d_loss (device, one double) may be NULL; d_work holds dgsw_mlp_grad_work_floats(n)
+ * floats. The sums run in a fixed order: repeated calls give identical results. adam: one Adam step
+ * (bias-corrected, step >= 1) on d_params with moment buffers d_m, d_v. */
+int32_t dgsw_mlp_forward(const float* d_x, int64_t n, const float* d_params, float* d_p, int32_t tensor_cores,
+                         void* stream);
+int64_t dgsw_mlp_grad_work_floats(int64_t n);
+int32_t dgsw_mlp_grad(const float* d_x, const uint8_t* d_y, int64_t n, const float* d_params, float pos_weight,
+                      float* d_grad, float* d_work, int64_t work_floats, double* d_loss, void* stream);
+int32_t dgsw_mlp_adam(float* d_params, float* d_m, float* d_v, const float* d_grad, int32_t step, float lr,
+                      float beta1, float beta2, float eps, void* stream);
+
 /* execution control */
 int32_t dgsw_rkdg_set_stream(dgsw_handle h, void* cuda_stream);
 int32_t dgsw_rkdg_synchronize(dgsw_handle h);
