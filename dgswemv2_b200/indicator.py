@@ -104,7 +104,7 @@ class Trainer:
         return self.P.cpu().numpy().copy()
 
 
-def record(nq=256, seeds=range(8), steps=400, every=4, keep=0.25, dt=0.25, precision="fp32", seed=0):
+def record(nq=256, seeds=range(8), steps=400, every=4, keep=0.035, dt=0.25, precision="fp32", seed=0):
     """Features and labels of the cells the limiter looks at, from bowl runs with random Gaussian humps:
     every `every`-th stage of `steps` SSP-RK2 steps, a random `keep` fraction of those cells."""
     torch = _torch()
@@ -170,17 +170,57 @@ def train(X, y, Xv=None, yv=None, epochs=8, batch=8192, lr=2e-3, seed=0, log=pri
     return T.params(), {"pos_weight": pos_weight, "history": hist, "train_cells": n}
 
 
+def evaluate(params, nq=1024, steps=200, dt=0.06, confidence=0.9, precision="fp32", warmup=3):
+    """Config-4 inference: Thacker bowl on nq x nq quads (2 nq^2 triangles), p = 1, SSP-RK2, wetting and
+    drying. Runs the same `steps` from t = 0 with no limiter, the plain limiter, the MLP-gated limiter and
+    the shadow mode (plain decisions, gate misses counted); reports device time per step after `warmup`
+    steps, the L2 error against the analytic solution, the miss rate and the fraction of cells sent to
+    the limiter."""
+    mesh, cfg = configs.config3(nq=nq, dt=dt, precision=precision)
+    out = {"elements": mesh.n_elems, "steps": steps, "dt": dt, "confidence": confidence, "precision": precision}
+    for name, lim, mode in (("no_limiter", False, 0), ("plain", True, 0), ("gated", True, 1), ("shadow", True, 2)):
+        cfg.slope_limiting = lim
+        P = Problem(cfg, mesh)
+        if mode:
+            P.set_indicator(params, confidence=confidence, mode=mode)
+        P.step_serial(warmup)
+        if mode:
+            P.indicator_stats(reset=True)
+        P.step_serial(steps - warmup)
+        ms, launches = P.last_step_timing()
+        r = {"ms_per_step": ms / (steps - warmup), "l2_error": P.compute_residual_L2(), "launches": launches}
+        if mode:
+            considered, sent, limited, missed = P.indicator_stats()
+            r.update({"considered": considered, "sent": sent, "limited": limited, "missed": missed,
+                      "sent_fraction": sent / max(1, considered)})
+            if mode == 2:
+                r["miss_rate"] = missed / max(1, limited + missed)
+        out[name] = r
+        P.close()
+    base = out["no_limiter"]["ms_per_step"]
+    out["limiter_ms_plain"] = out["plain"]["ms_per_step"] - base
+    out["limiter_ms_gated"] = out["gated"]["ms_per_step"] - base
+    out["l2_added_by_gate"] = out["gated"]["l2_error"] / out["plain"]["l2_error"] - 1.0
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "evaluate"])
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--nq", type=int, default=256)
     ap.add_argument("--runs", type=int, default=12)
     ap.add_argument("--steps", type=int, default=600)
     ap.add_argument("--epochs", type=int, default=8)
-    ap.add_argument("--keep", type=float, default=0.3)
+    ap.add_argument("--keep", type=float, default=0.035)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--weights", default=WEIGHTS)
+    ap.add_argument("--eval-nq", type=int, default=1024)
+    ap.add_argument("--eval-steps", type=int, default=200)
     a = ap.parse_args()
+    if a.cmd == "evaluate":
+        print(json.dumps(evaluate(load_weights(a.weights), nq=a.eval_nq, steps=a.eval_steps)), flush=True)
+        return
     t0 = time.time()
     X, y = record(nq=a.nq, seeds=range(a.runs), steps=a.steps, keep=a.keep)
     Xv, yv = record(nq=a.nq, seeds=range(1000, 1002), steps=a.steps, keep=a.keep, seed=1)
