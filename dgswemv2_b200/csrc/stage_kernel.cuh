@@ -195,13 +195,22 @@ __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double b
         qy[1] = ay - by + cy;
         qy[2] = ay + 2.0 * by;
     }
+    // FP32 state: the depths above carry the storage rounding of ze (about 2^-24 (|z| + |b|)), which the
+    // FP64 threshold 1e6 h_o eps_64 cannot absorb; a flattened dry cell at depth h_o would read as wet
+    // after one round trip through FP32. Widen the threshold to that rounding bound (FP64: unchanged).
+    const double thr_clamp = thr;
+    if (sizeof(Real) == 4) {
+        double m = 0.0;
+        for (int v = 0; v < 3; ++v) m = fmax(m, fabs(z[v]) + fabs(bv[v]));
+        thr = fmax(thr, m * (8.0 * 1.1920928955078125e-07));
+    }
     int ndry = 0;
     for (int v = 0; v < 3; ++v) {
         h[v] = z[v] + bv[v];
         if (h[v] <= h_o + thr) ++ndry;
     }
     double h_avg = (0.0 + h[0] + h[1] + h[2]) / 3;
-    if (h_avg <= thr) h_avg = thr;
+    if (h_avg <= thr_clamp) h_avg = thr_clamp;
     bool reproject = false, check = false;
     if (ndry == 0) {
         if (wet) return true;
