@@ -257,10 +257,13 @@ FeatureArgs<Real> feature_args(dgsw_rkdg_s* h, int s_out) {
     F.wet = h->wet[h->wet_cur].p;
     F.nbr = h->nbr.p;
     F.enodes = h->enodes.p;
+    F.xy = h->xy.p;
     F.nz = h->nz.p;
     F.ne = (int)h->ne;
     F.ne_pad = (int)h->ne_pad;
     F.nd = h->nd;
+    F.g = h->cfg.g;
+    F.M = h->cfg.sl_M;
     return F;
 }
 

@@ -224,7 +224,7 @@ cudaError_t launch_mlp_tc(const TcArgs& T, const FeatureArgs<Real>& F, cudaStrea
         if (e != cudaSuccess) return e;
         attr_set[which] = true;
     }
-    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * 4);
+    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * MLP_TC_CTAS_PER_SM);
     mlp_tc_kernel<Real><<<grid, MLP_TILE, TcSmem::TOTAL + 1024, s>>>(T, F);
     return cudaGetLastError();
 }

@@ -45,13 +45,16 @@ struct FeatureArgs {
     const unsigned char* wet;  // wet flags of this state
     const int* nbr;            // [3][ne_pad]: neighbour device index, or -2 - boundary type
     const int* enodes;         // [3][ne_pad]
+    const double2* xy;         // node coordinates
     const double* nz;          // node depths
     int ne, ne_pad, nd;
+    double g, M;               // gravity, TVB constant of the limiter
 };
 
-// The 18 features of element e (see oracle/mlp_oracle.py for the definition) and whether the limiter
-// looks at it (the element and its neighbours wet, boundary faces land or function). FP64 arithmetic
-// with explicit roundings (no contraction) so the values are reproducible on the host.
+// The 18 features of element e (definition in oracle/mlp_oracle.py: fields in characteristic units,
+// one common scale, TVB ratio, Froude numbers) and whether the limiter looks at the cell (it and its
+// neighbours wet, boundary faces land or function). FP64 arithmetic with explicit roundings (no
+// contraction), so the host oracle reproduces the values bit for bit.
 template <typename Real>
 __device__ __forceinline__ bool element_features(const FeatureArgs<Real>& F, int e, float* out) {
     const size_t P = (size_t)F.ne_pad;
@@ -78,26 +81,55 @@ __device__ __forceinline__ bool element_features(const FeatureArgs<Real>& F, int
             for (int v = 0; v < 3; ++v) d[f][v] = 0.0;
         }
     }
-    const int n0 = F.enodes[e], n1 = F.enodes[P + e], n2 = F.enodes[2 * P + e];
+    const int n[3] = {F.enodes[e], F.enodes[P + e], F.enodes[2 * P + e]};
     const double third = 1.0 / 3.0;
-    const double zb = __dadd_rn(__dadd_rn(__dmul_rn(F.nz[n0], third), __dmul_rn(F.nz[n1], third)),
-                                __dmul_rn(F.nz[n2], third));
+    const double zb = __dadd_rn(__dadd_rn(__dmul_rn(F.nz[n[0]], third), __dmul_rn(F.nz[n[1]], third)),
+                                __dmul_rn(F.nz[n[2]], third));
+    const double H = fmax(__dadd_rn(a[0], zb), 1.0e-3);
+    const double ic = __ddiv_rn(1.0, __dsqrt_rn(__dmul_rn(F.g, H)));
+#pragma unroll
+    for (int v = 1; v < 3; ++v) {
+        b[v] = __dmul_rn(b[v], ic);
+        c[v] = __dmul_rn(c[v], ic);
+#pragma unroll
+        for (int f = 0; f < 3; ++f) d[f][v] = __dmul_rn(d[f][v], ic);
+    }
+    double s = 0.0;
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-        double s = fmax(fmax(fabs(b[v]), fabs(c[v])), fmax(fmax(fabs(d[0][v]), fabs(d[1][v])), fabs(d[2][v])));
-        if (s == 0.0) s = 1.0;
-        double f0;
-        if (v == 0) {
-            const double H = fmax(__dadd_rn(a[0], zb), 0.0);
-            f0 = __ddiv_rn(H, __dadd_rn(H, s));
-        } else {
-            f0 = __ddiv_rn(a[v], __dadd_rn(fabs(a[v]), s));
-        }
-        out[6 * v + 0] = __double2float_rn(f0);
-        out[6 * v + 1] = __double2float_rn(__ddiv_rn(b[v], s));
-        out[6 * v + 2] = __double2float_rn(__ddiv_rn(c[v], s));
+        s = fmax(s, fmax(fabs(b[v]), fabs(c[v])));
 #pragma unroll
-        for (int f = 0; f < 3; ++f) out[6 * v + 3 + f] = __double2float_rn(__ddiv_rn(d[f][v], s));
+        for (int f = 0; f < 3; ++f) s = fmax(s, fabs(d[f][v]));
+    }
+    if (s == 0.0) s = 1.0;
+    // mean squared distance from the centroid to the edge midpoints
+    double X[3], Y[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double2 p = F.xy[n[k]];
+        X[k] = p.x;
+        Y[k] = p.y;
+    }
+    const double cx = __ddiv_rn(__dadd_rn(__dadd_rn(X[0], X[1]), X[2]), 3.0);
+    const double cy = __ddiv_rn(__dadd_rn(__dadd_rn(Y[0], Y[1]), Y[2]), 3.0);
+    double r2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double mx = __dsub_rn(__ddiv_rn(__dadd_rn(X[(k + 1) % 3], X[(k + 2) % 3]), 2.0), cx);
+        const double my = __dsub_rn(__ddiv_rn(__dadd_rn(Y[(k + 1) % 3], Y[(k + 2) % 3]), 2.0), cy);
+        r2 = __dadd_rn(r2, __dadd_rn(__dmul_rn(mx, mx), __dmul_rn(my, my)));
+    }
+    r2 = __ddiv_rn(r2, 3.0);
+    const double inv = __ddiv_rn(1.0, s);
+    out[0] = __double2float_rn(__ddiv_rn(s, __dadd_rn(s, __dmul_rn(F.M, r2))));
+    out[1] = __double2float_rn(fmin(fmax(__dmul_rn(__ddiv_rn(a[1], H), ic), -8.0), 8.0));
+    out[2] = __double2float_rn(fmin(fmax(__dmul_rn(__ddiv_rn(a[2], H), ic), -8.0), 8.0));
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        out[3 + 5 * v] = __double2float_rn(__dmul_rn(b[v], inv));
+        out[4 + 5 * v] = __double2float_rn(__dmul_rn(c[v], inv));
+#pragma unroll
+        for (int f = 0; f < 3; ++f) out[5 + 5 * v + f] = __double2float_rn(__dmul_rn(d[f][v], inv));
     }
     return ok;
 }
@@ -126,8 +158,10 @@ __device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf
 
 // shared memory of mlp_tc_kernel (bytes, 1024-aligned base)
 struct TcSmem {
+    // A1 and A2 share their space: A2 is written only after the layer-1 MMA has read A1, and the next
+    // tile's A1 only after the layer-2 MMA has read A2
     static constexpr int A1 = 0;                                  // [128][32] BF16 features
-    static constexpr int A2 = A1 + MLP_TILE * MLP_K1 * 2;         // [128][64] BF16 hidden layer 1
+    static constexpr int A2 = 0;                                  // [128][64] BF16 hidden layer 1
     static constexpr int B1 = A2 + MLP_TILE * MLP_H * 2;          // [64][32] BF16 W1 (K padded)
     static constexpr int B2 = B1 + MLP_H * MLP_K1 * 2;            // [64][64] BF16 W2
     static constexpr int VEC = B2 + MLP_H * MLP_H * 2;            // b1, b2, w3, b3 (FP32)
@@ -135,6 +169,7 @@ struct TcSmem {
     static constexpr int TOTAL = BAR + 64;
 };
 constexpr int MLP_TMEM_COLS = 64;  // one 128 x 64 FP32 accumulator, reused by both layers
+constexpr int MLP_TC_CTAS_PER_SM = 5;  // 5 x 64 TMEM columns <= 512; about 30 KB shared memory each
 
 struct TcArgs {
     const float* params;  // FP32 master parameters
@@ -166,7 +201,7 @@ __device__ __forceinline__ void store_bf16x8(__nv_bfloat16* dst, const float* v)
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(MLP_TILE, 4) mlp_tc_kernel(const TcArgs T, const FeatureArgs<Real> F) {
+__global__ void __launch_bounds__(MLP_TILE, MLP_TC_CTAS_PER_SM) mlp_tc_kernel(const TcArgs T, const FeatureArgs<Real> F) {
     extern __shared__ __align__(1024) unsigned char tsm[];
     __nv_bfloat16* A1 = reinterpret_cast<__nv_bfloat16*>(tsm + TcSmem::A1);
     __nv_bfloat16* A2 = reinterpret_cast<__nv_bfloat16*>(tsm + TcSmem::A2);

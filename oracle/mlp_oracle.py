@@ -6,13 +6,17 @@ decision (CS_slope_limiter_serial, source/problem/SWE/problem_slope_limiter/swe_
 a cell is troubled when the Cockburn-Shu pass changes its state), and its inputs are the quantities
 that limiter reads: the linear modal coefficients of ze, qx, qy and the three neighbour cell means.
 
-Features (18 per element, p = 1), for each field v in (ze, qx, qy), with a = own mean (mode 0),
-b, c = modes 1, 2, m_f = mean of the neighbour across face f (own mean at a boundary face),
-d_f = m_f - a and s = max(|b|, |c|, |d_0|, |d_1|, |d_2|) (1 where that is 0):
-  [6v+0] = H / (H + s) for ze, H = max(a + b_c, 0) the depth at the barycentre (b_c = mean of the
-           three vertex depths); a / (|a| + s) for qx, qy
-  [6v+1] = b / s, [6v+2] = c / s, [6v+3+f] = d_f / s
-Scale-free inputs: the limiter's minmod test compares slopes with neighbour differences, a ratio.
+Features (18 per element, p = 1). The limiter compares, per median direction, characteristic slopes
+w = R^-1 q of the cell with R^-1-weighted neighbour differences, where R^-1 mixes ze with q / c
+(c = sqrt(g H)) and the Froude number u / c, and leaves a slope alone when it is below M r^2 (TVB).
+So the fields are first put in common units: ze as is, qx and qy divided by the cell's c; then
+a = own mean (mode 0), b, c = modes 1, 2, d_f = (neighbour mean across face f) - a (0 at a boundary),
+and one scale s = max over the three fields of |b|, |c|, |d_f| (1 where that is 0):
+  [0]  s / (s + M r2)            r2 = mean squared centroid-to-edge-midpoint distance (TVB ratio)
+  [1]  clamp(u / c, -8, 8)       u = qx_mean / H, H = max(ze_mean + b_c, 1e-3), b_c = mean vertex depth
+  [2]  clamp(v / c, -8, 8)
+  [3 + 5 v + 0, 1]  b / s, c / s of field v
+  [3 + 5 v + 2 + f] d_f / s
 A cell takes part (ok) when it and its three neighbours are wet and each boundary face is land or
 function, the same condition under which the limiter looks at it.
 
@@ -36,29 +40,46 @@ def unpack(P):
             P[OFF_B2:OFF_W3], P[OFF_W3:OFF_B3], P[OFF_B3])
 
 
-def features(q, wet, nbr, btype, node_z, elem_nodes):
+def features(q, wet, nbr, btype, node_xyz, elem_nodes, g, M):
     """q [ne][3][nd] (ascending element ID), wet [ne], nbr [ne][3] (-1 at boundaries), btype [ne][3],
-    node_z [nn], elem_nodes [ne][3] -> (features [ne][18] float32, ok [ne] bool)."""
+    node_xyz [nn][3], elem_nodes [ne][3], gravity g, TVB constant M -> (features [ne][18] float32,
+    ok [ne] bool). Operation order matches the device code exactly (no fused multiply-adds)."""
     q = np.asarray(q, np.float64)
     ne = q.shape[0]
-    a = q[:, :, 0]
-    b = q[:, :, 1]
-    c = q[:, :, 2]
+    a = q[:, :, 0].copy()
+    b = q[:, :, 1].copy()
+    c = q[:, :, 2].copy()
     has = nbr >= 0
-    m = np.where(has[:, :, None], a[np.where(has, nbr, 0)], a[:, None, :])  # [ne][face][var]
+    m = np.where(has[:, :, None], q[np.where(has, nbr, 0), :, 0], a[:, None, :])  # [ne][face][var]
     d = m - a[:, None, :]
-    s = np.maximum(np.maximum(np.abs(b), np.abs(c)), np.max(np.abs(d), axis=1))
+    X = node_xyz[elem_nodes]  # [ne][3][3]
+    zb = X[:, 0, 2] * (1.0 / 3.0) + X[:, 1, 2] * (1.0 / 3.0) + X[:, 2, 2] * (1.0 / 3.0)
+    H = np.maximum(a[:, 0] + zb, 1e-3)
+    ic = 1.0 / np.sqrt(g * H)
+    for v in (1, 2):
+        b[:, v] = b[:, v] * ic
+        c[:, v] = c[:, v] * ic
+        d[:, :, v] = d[:, :, v] * ic[:, None]
+    s = np.maximum(np.maximum(np.abs(b), np.abs(c)).max(axis=1), np.abs(d).max(axis=(1, 2)))
     s = np.where(s == 0.0, 1.0, s)
-    z = node_z[elem_nodes]
-    zb = z[:, 0] * (1.0 / 3.0) + z[:, 1] * (1.0 / 3.0) + z[:, 2] * (1.0 / 3.0)
-    H = np.maximum(a[:, 0] + zb, 0.0)
+    cx = (X[:, 0, 0] + X[:, 1, 0] + X[:, 2, 0]) / 3.0
+    cy = (X[:, 0, 1] + X[:, 1, 1] + X[:, 2, 1]) / 3.0
+    r2 = np.zeros(ne)
+    for k in range(3):
+        mx = (X[:, (k + 1) % 3, 0] + X[:, (k + 2) % 3, 0]) / 2.0 - cx
+        my = (X[:, (k + 1) % 3, 1] + X[:, (k + 2) % 3, 1]) / 2.0 - cy
+        r2 = r2 + (mx * mx + my * my)
+    r2 = r2 / 3.0
+    inv = 1.0 / s
     F = np.empty((ne, 18), np.float64)
+    F[:, 0] = s / (s + M * r2)
+    F[:, 1] = np.clip((a[:, 1] / H) * ic, -8.0, 8.0)
+    F[:, 2] = np.clip((a[:, 2] / H) * ic, -8.0, 8.0)
     for v in range(3):
-        F[:, 6 * v] = H / (H + s[:, 0]) if v == 0 else a[:, v] / (np.abs(a[:, v]) + s[:, v])
-        F[:, 6 * v + 1] = b[:, v] / s[:, v]
-        F[:, 6 * v + 2] = c[:, v] / s[:, v]
+        F[:, 3 + 5 * v] = b[:, v] * inv
+        F[:, 4 + 5 * v] = c[:, v] * inv
         for f in range(3):
-            F[:, 6 * v + 3 + f] = d[:, f, v] / s[:, v]
+            F[:, 5 + 5 * v + f] = d[:, f, v] * inv
     w = np.asarray(wet) != 0
     nbr_wet = np.where(has, w[np.where(has, nbr, 0)], (btype == 0) | (btype == 3))
     ok = w & nbr_wet.all(axis=1)

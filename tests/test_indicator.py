@@ -50,7 +50,7 @@ def test_bf16_rounding_cases():
 
 
 def test_oracle_features_by_hand():
-    """One interior element with two neighbours and a land face: the definition evaluated by hand."""
+    """One element with two neighbours and a land face: the definition evaluated by hand."""
     q = np.zeros((3, 3, 3))         # [element][variable][mode]
     q[0, 0, :] = [1.0, 0.5, -0.2]   # ze of element 0: mean 1, slopes 0.5, -0.2
     q[0, 1, 0] = 0.25               # qx mean of element 0
@@ -58,18 +58,20 @@ def test_oracle_features_by_hand():
     nbr = np.array([[1, 2, -1], [0, -1, -1], [0, -1, -1]])
     btype = np.array([[128, 128, 0], [128, 0, 0], [128, 0, 0]])
     wet = np.array([1, 1, 1])
-    z = np.array([2.0, 2.0, 2.0, 2.0])
+    xyz = np.array([[0.0, 0.0, 2.0], [1.0, 0.0, 2.0], [0.0, 1.0, 2.0], [1.0, 1.0, 2.0]])
     en = np.array([[0, 1, 2], [1, 3, 2], [0, 2, 3]])
-    F, ok = mo.features(q, wet, nbr, btype, z, en)
+    g, M = 9.81, 0.5
+    F, ok = mo.features(q, wet, nbr, btype, xyz, en, g, M)
     assert ok.all()
-    # ze of element 0: d = (1.5 - 1, 0 - 1, 0) -> s = max(0.5, 0.2, 0.5, 1, 0) = 1, H = 1 + 2 = 3
-    assert np.allclose(F[0, :6], [3 / 4, 0.5, -0.2, 0.5, -1.0, 0.0])
-    # qx of element 0: mean 0.25, no slopes, neighbours' qx means 0 -> d = (-0.25, -0.25, 0), s = 0.25
-    assert np.allclose(F[0, 6:12], [0.25 / 0.5, 0, 0, -1, -1, 0])
-    # qy: everything zero -> s = 1, all features 0
-    assert np.all(F[0, 12:] == 0)
+    ic = 1.0 / np.sqrt(g * 3.0)  # depth H = 1 + 2
+    # common scale: ze slopes 0.5, -0.2, ze differences 0.5, -1, 0, qx differences -0.25 c^-1 -> s = 1;
+    # r2 = (1/18 + 5/36 + 5/36) / 3 = 1/9 for the unit right triangle
+    assert np.allclose(F[0, :3], [1.0 / (1.0 + M / 9.0), 0.25 / 3.0 * ic, 0.0])
+    assert np.allclose(F[0, 3:8], [0.5, -0.2, 0.5, -1.0, 0.0])
+    assert np.allclose(F[0, 8:13], [0.0, 0.0, -0.25 * ic, -0.25 * ic, 0.0])
+    assert np.all(F[0, 13:] == 0)
     wet2 = np.array([1, 0, 1])
-    assert list(mo.features(q, wet2, nbr, btype, z, en)[1]) == [False, False, True]
+    assert list(mo.features(q, wet2, nbr, btype, xyz, en, g, M)[1]) == [False, False, True]
 
 
 # ---------------------------------------------------------------------------------------------- GPU
@@ -98,7 +100,7 @@ def test_features_match_oracle_bit_exact(precision):
     ok = torch.empty(P.ne, dtype=torch.uint8, device="cuda")
     P.indicator_features(feat.data_ptr(), ok.data_ptr())
     nbr, bt, _, _ = mesh_topology(mesh)
-    F, okr = mo.features(P.get_state(), P.get_wet(), nbr, bt, mesh.node_xyz[:, 2], mesh.elem_nodes)
+    F, okr = mo.features(P.get_state(), P.get_wet(), nbr, bt, mesh.node_xyz, mesh.elem_nodes, cfg.g, cfg.sl_M)
     assert okr.sum() > P.ne // 4 and (~okr).sum() > 0  # wet and dry cells both present
     assert np.array_equal(ok.cpu().numpy() != 0, okr)
     assert np.array_equal(feat.cpu().numpy(), F)
