@@ -235,3 +235,26 @@ def test_gate_sending_nothing_counts_every_limited_cell_as_missed():
     assert N.indicator_stats()[1] == 0 and not N.get_limited().any()
     # without limiting the two unlimited runs agree with each other
     assert np.array_equal(S.get_state(), N.get_state())
+
+
+@pytest.mark.gpu
+def test_trained_indicator_on_the_thacker_bowl():
+    """The committed network (dgswemv2_b200/data/indicator_p1.f32) on the Thacker bowl at 256 x 256 quads,
+    100 SSP-RK2 steps, FP32 bulk: the gate sends fewer cells to the limiter than the plain limiter visits,
+    misses at most 2 % of the cells the plain limiter changes (shadow mode counts them), and the L2 error
+    against the analytic solution stays within 0.1 % of the plain limiter's."""
+    from dgswemv2_b200 import indicator
+
+    W = indicator.load_weights()
+    mesh, cfg = configs.config3(nq=256, dt=0.25, precision="fp32")
+    runs = {}
+    for mode in (0, 1, 2):
+        P = Problem(cfg, mesh)
+        if mode:
+            P.set_indicator(W, confidence=0.9, mode=mode)
+        P.step_serial(100)
+        runs[mode] = (P.compute_residual_L2(), P.indicator_stats() if mode else None)
+    considered, sent, limited, missed = runs[2][1]
+    assert runs[1][1][1] == sent and sent < considered
+    assert missed <= 0.02 * (limited + missed)
+    assert abs(runs[1][0] / runs[0][0] - 1) <= 1e-3
