@@ -12,7 +12,7 @@ from . import _lib
 from ._lib import DGSW_FP32, DGSW_FP64, DgswError  # noqa: F401
 from .types import MeshArrays, ProblemConfig  # noqa: F401
 
-__all__ = ["Problem", "ProblemConfig", "MeshArrays", "DgswError", "mesh_topology"]
+__all__ = ["Problem", "ProblemConfig", "MeshArrays", "DgswError", "mesh_topology", "ensemble"]
 
 
 def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True):
@@ -84,6 +84,38 @@ def mesh_topology(mesh):
     _lib.check(lib.dgsw_mesh_topology(C.byref(m), _lib.ptr(nbr, C.c_int32), _lib.ptr(bt, C.c_uint8), C.byref(ni),
                                       _lib.ptr(intf, C.c_int32), C.byref(nb), _lib.ptr(bnd, C.c_int32)))
     return nbr, bt, intf, bnd
+
+
+def ensemble(cfg, meshes, member_params=None, device=0, tile=_lib.DGSW_TILE_AUTOTUNE, renumber=True,
+             use_graphs=True, init=True):
+    """Ensemble batching (dgsw_ensemble_create): the members share `cfg` except their function-set
+    parameters (member_params: one 16-value list per member, or None for cfg.fn_params). Returns a
+    Problem whose state holds the members one after another (Problem.member_range)."""
+    lib = _lib.load()
+    P = Problem.__new__(Problem)
+    P.cfg = cfg
+    P._c = _make_config(cfg, device, tile, renumber, use_graphs)
+    arr = (_lib.Mesh * len(meshes))()
+    P._keep = []
+    for k, m in enumerate(meshes):
+        arr[k], keep = _mesh_struct(m)
+        P._keep.append(keep)
+    prm = None
+    if member_params is not None:
+        prm = np.zeros((len(meshes), 16), np.float64)
+        for k, v in enumerate(member_params):
+            prm[k, :len(v)] = v
+        P._keep.append(prm)
+    h = C.c_void_p()
+    _lib.check(lib.dgsw_ensemble_create(C.byref(P._c), len(meshes), arr, _lib.ptr(prm, C.c_double), C.byref(h)))
+    P._h = h
+    P.info = _lib.Info()
+    _lib.check(lib.dgsw_rkdg_info(h, C.byref(P.info)))
+    P.ne = P.info.n_elems
+    P.nd = P.info.ndof
+    if init:
+        P.preprocessor_serial()
+    return P
 
 
 class Problem:
@@ -214,6 +246,20 @@ class Problem:
         _lib.check(lib.dgsw_rkdg_topology(self._h, _lib.ptr(nbr, C.c_int32), _lib.ptr(bt, C.c_uint8), C.byref(ni),
                                           _lib.ptr(intf, C.c_int32), C.byref(nb), _lib.ptr(bnd, C.c_int32)))
         return nbr, bt, intf, bnd
+
+    def member_range(self, member):
+        """(first element, element count) of an ensemble member in the state order."""
+        f, n = C.c_int64(), C.c_int64()
+        _lib.check(_lib.load().dgsw_ensemble_member_range(self._h, int(member), C.byref(f), C.byref(n)))
+        return f.value, n.value
+
+    def tuning(self):
+        """The autotuner's record: [(tile, device ms per step), ...] (empty if not tuned)."""
+        t = (C.c_int32 * 4)()
+        ms = (C.c_double * 4)()
+        n = C.c_int32()
+        _lib.check(_lib.load().dgsw_rkdg_tuning(self._h, t, ms, C.byref(n)))
+        return [(t[i], ms[i]) for i in range(n.value)]
 
     def synchronize(self):
         _lib.check(_lib.load().dgsw_rkdg_synchronize(self._h))

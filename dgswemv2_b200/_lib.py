@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdgsw_rkdg.so")
 
 DGSW_FP64, DGSW_FP32 = 0, 1
+DGSW_TILE_AUTOTUNE = -1
 DGSW_L2_STATIC_MAX_ELEMS = 1048576
 DGSW_MLP_NPARAM = 5441
 DGSW_MLP_NFEATURES = 18
@@ -105,6 +106,10 @@ SIGNATURES = {
     "dgsw_config_default": (None, [C.POINTER(Config)]),
     "dgsw_rkdg_create": (C.c_int32, [C.POINTER(Config), C.POINTER(Mesh), C.POINTER(C.c_void_p)]),
     "dgsw_rkdg_destroy": (C.c_int32, [C.c_void_p]),
+    "dgsw_ensemble_create": (C.c_int32, [C.POINTER(Config), C.c_int32, C.POINTER(Mesh), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_void_p)]),
+    "dgsw_ensemble_member_range": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "dgsw_rkdg_tuning": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "dgsw_rkdg_info": (C.c_int32, [C.c_void_p, C.POINTER(Info)]),
     "dgsw_rkdg_init_state": (C.c_int32, [C.c_void_p]),
     "dgsw_rkdg_set_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),

@@ -102,3 +102,18 @@ def ensemble_member(n, seed, extent=10000.0, dt=0.5, precision="fp32"):
     cfg = ProblemConfig(p=1, rk_nstages=2, rk_order=2, dt=dt, g=9.81, wetting_drying=True, h_o=0.01, ic_type=1,
                         function_set=FN_GAUSSIAN_HUMPS, fn_params=humps_params(hump), precision=precision)
     return mesh, cfg
+
+
+def config5(n_members=256, seed=0, nmin=64, nmax=200, dt=0.5, precision="fp32"):
+    """Ensemble of independent p=1 wet/dry runs: member k has n x n quads with n uniform in [nmin, nmax]
+    (seeded), a bathymetry of 8 seeded Gaussians (depth 1-20 m) and a Gaussian hump on the surface.
+    Returns (meshes, member_cfgs): every member shares the configuration except its function-set
+    parameters (the hump)."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(nmin, nmax + 1, size=n_members)
+    meshes, cfgs = [], []
+    for k, n in enumerate(sizes):
+        mesh, cfg = ensemble_member(int(n), seed * 100003 + k, dt=dt, precision=precision)
+        meshes.append(mesh)
+        cfgs.append(cfg)
+    return meshes, cfgs

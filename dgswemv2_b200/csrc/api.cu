@@ -6,7 +6,9 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -133,6 +135,13 @@ struct dgsw_rkdg_s {
     size_t smem_bytes = 0;
     int tile = 256;
     int64_t graph_launches[4] = {0, 0, 0, 0};  // kernels one replay of graph[key] launches
+    // ensemble members: element ranges [member_first[m], member_first[m+1]) in reference order
+    int32_t n_members = 1;
+    std::vector<int64_t> member_first;
+    // autotuner record: candidate tile sizes and their measured device time per step
+    int32_t n_tuned = 0;
+    int32_t tuned_tile[4] = {0, 0, 0, 0};
+    double tuned_ms[4] = {0, 0, 0, 0};
     // troubled-cell indicator (mode 0 off, 1 gate the limiter, 2 shadow: plain limiter, misses counted)
     int ind_mode = 0;
     float ind_skip_below = 0.1f;
@@ -506,7 +515,10 @@ void dgsw_config_default(dgsw_config* c) {
     c->use_graphs = 1;
 }
 
-int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_handle* out) {
+// create for one mesh; caller_group (per caller element, may be NULL) and group_params describe the
+// members of an ensemble
+static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const int32_t* caller_group,
+                           int32_t n_groups, const double* group_params, dgsw_handle* out) {
     if (!cfg || !mesh || !out) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
     int ndev = 0;
@@ -537,6 +549,15 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
     if (rc) {
         delete h;
         return fail(rc, err);
+    }
+    if (caller_group) {
+        h->topo.group.resize(h->topo.ne);
+        for (int64_t r = 0; r < h->topo.ne; ++r) h->topo.group[r] = caller_group[h->topo.src[r]];
+        h->topo.group_params.assign(group_params, group_params + (size_t)n_groups * DGSW_FN_PARAMS);
+        h->n_members = n_groups;
+        h->member_first.assign(n_groups + 1, 0);
+        for (int64_t r = 0; r < h->topo.ne; ++r) h->member_first[h->topo.group[r] + 1]++;
+        for (int32_t m = 0; m < n_groups; ++m) h->member_first[m + 1] += h->member_first[m];
     }
     h->ne = h->topo.ne;
     h->nn = mesh->n_nodes;
@@ -706,6 +727,234 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return cleanup_fail("setup", e);
     *out = h;
+    return DGSW_OK;
+}
+
+// Autotuner: build the problem with each stage-kernel tile size, time a few steps of each on the
+// device (after two warm-up steps that also capture the step graphs) and keep the fastest. `tune_*`
+// describe the problem the timing runs on (a subset of an ensemble's members, or the problem itself);
+// the winner is then built for the full problem unless the tuning problem is the full problem.
+// Decisions are cached per (elements, order, precision, stages, options, device) for the process.
+static std::mutex g_tune_mutex;
+static std::map<std::string, int> g_tune_cache;
+
+static int32_t time_candidate(const dgsw_config* cfg, const dgsw_mesh* mesh, const int32_t* group, int32_t ng,
+                              const double* gp, int tile, double* ms, dgsw_handle* keep) {
+    dgsw_config c = *cfg;
+    c.tile = tile;
+    dgsw_handle h = nullptr;
+    int32_t rc = create_impl(&c, mesh, group, ng, gp, &h);
+    if (rc) return rc;
+    const int warm = 2, timed = 4;
+    if ((rc = dgsw_rkdg_init_state(h)) || (rc = dgsw_rkdg_step(h, warm)) || (rc = dgsw_rkdg_step(h, timed))) {
+        dgsw_rkdg_destroy(h);
+        return rc;
+    }
+    int64_t nl = 0;
+    dgsw_rkdg_last_step_timing(h, ms, &nl);
+    *ms /= timed;
+    if (keep) {
+        *keep = h;
+    } else {
+        dgsw_rkdg_destroy(h);
+    }
+    return DGSW_OK;
+}
+
+static int32_t create_tuned(const dgsw_config* cfg, const dgsw_mesh* mesh, const int32_t* group, int32_t ng,
+                            const double* gp, const dgsw_mesh* tune_mesh, const int32_t* tune_group, int32_t tune_ng,
+                            const double* tune_gp, dgsw_handle* out) {
+    const bool same = tune_mesh == mesh;
+    const int cands[2] = {128, 256};
+    cudaDeviceProp prop;
+    std::memset(&prop, 0, sizeof(prop));
+    cudaGetDeviceProperties(&prop, cfg->device);
+    char key[512];
+    std::snprintf(key, sizeof(key), "%lld/%lld/%d/%d/%d/%d/%d/%d/%d/%s", (long long)mesh->n_elems,
+                  (long long)tune_mesh->n_elems, cfg->p, cfg->precision, cfg->rk_nstages, cfg->wetting_drying,
+                  cfg->slope_limiting, cfg->function_source, ng, prop.name);
+    int chosen = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) chosen = it->second;
+    }
+    double ms[2] = {0, 0};
+    dgsw_handle best = nullptr;
+    int ntimed = 0;
+    if (!chosen) {
+        double best_ms = 1e300;
+        for (int i = 0; i < 2; ++i) {
+            dgsw_handle h = nullptr;
+            int32_t rc = time_candidate(cfg, tune_mesh, tune_group, tune_ng, tune_gp, cands[i], &ms[i],
+                                        same ? &h : nullptr);
+            if (rc) {
+                if (best) dgsw_rkdg_destroy(best);
+                return rc;
+            }
+            ++ntimed;
+            if (ms[i] < best_ms) {
+                best_ms = ms[i];
+                chosen = cands[i];
+                if (same) {
+                    if (best) dgsw_rkdg_destroy(best);
+                    best = h;
+                }
+            } else if (same) {
+                dgsw_rkdg_destroy(h);
+            }
+        }
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        g_tune_cache[key] = chosen;
+    }
+    if (!best) {
+        dgsw_config c = *cfg;
+        c.tile = chosen;
+        int32_t rc = create_impl(&c, mesh, group, ng, gp, &best);
+        if (rc) return rc;
+    } else {
+        int32_t rc = dgsw_rkdg_init_state(best);  // back to t = 0 after the timing steps
+        if (rc) {
+            dgsw_rkdg_destroy(best);
+            return rc;
+        }
+    }
+    best->n_tuned = ntimed;
+    for (int i = 0; i < ntimed; ++i) {
+        best->tuned_tile[i] = cands[i];
+        best->tuned_ms[i] = ms[i];
+    }
+    *out = best;
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_handle* out) {
+    if (!cfg || !mesh || !out) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (cfg->tile == DGSW_TILE_AUTOTUNE) return create_tuned(cfg, mesh, nullptr, 0, nullptr, mesh, nullptr, 0, nullptr, out);
+    return create_impl(cfg, mesh, nullptr, 0, nullptr, out);
+}
+
+// members -> one mesh: nodes and boundary chains appended with index offsets, element IDs renumbered
+// member-major (ascending within each member by its own IDs), caller_group = member of each element
+struct Concat {
+    std::vector<double> xyz;
+    std::vector<int32_t> en, seg_type, seg_nodes, group;
+    std::vector<uint32_t> ids;
+    std::vector<int64_t> seg_off{0};
+    dgsw_mesh m;
+};
+
+static int concat_members(int32_t n, const dgsw_mesh* members, Concat& C, std::string& err) {
+    int64_t nn = 0, ne = 0;
+    for (int32_t k = 0; k < n; ++k) {
+        const dgsw_mesh& M = members[k];
+        if (!M.node_xyz || !M.elem_nodes || M.n_nodes <= 0 || M.n_elems <= 0 || (M.n_segments && !M.seg_offsets)) {
+            err = "ensemble member " + std::to_string(k) + " has no nodes or elements";
+            return DGSW_ERR_INVALID_ARGUMENT;
+        }
+        nn += M.n_nodes;
+        ne += M.n_elems;
+    }
+    if (ne >= ((int64_t)1 << 32) || nn >= ((int64_t)1 << 31)) {
+        err = "ensemble too large for 32-bit element IDs";
+        return DGSW_ERR_UNSUPPORTED;
+    }
+    C.xyz.reserve(3 * nn);
+    C.en.reserve(3 * ne);
+    C.ids.reserve(ne);
+    C.group.reserve(ne);
+    int64_t node_base = 0, id_base = 0;
+    for (int32_t k = 0; k < n; ++k) {
+        const dgsw_mesh& M = members[k];
+        C.xyz.insert(C.xyz.end(), M.node_xyz, M.node_xyz + 3 * M.n_nodes);
+        std::vector<int64_t> order(M.n_elems);
+        std::iota(order.begin(), order.end(), 0);
+        if (M.elem_ids)
+            std::stable_sort(order.begin(), order.end(),
+                             [&](int64_t a, int64_t b) { return M.elem_ids[a] < M.elem_ids[b]; });
+        std::vector<uint32_t> rank(M.n_elems);
+        for (int64_t i = 0; i < M.n_elems; ++i) rank[order[i]] = (uint32_t)(id_base + i);
+        for (int64_t i = 0; i < M.n_elems; ++i) {
+            for (int v = 0; v < 3; ++v) {
+                const int32_t nd = M.elem_nodes[3 * i + v];
+                if (nd < 0 || nd >= M.n_nodes) {
+                    err = "ensemble member " + std::to_string(k) + ": element node index out of range";
+                    return DGSW_ERR_MESH;
+                }
+                C.en.push_back((int32_t)(nd + node_base));
+            }
+            C.ids.push_back(rank[i]);
+            C.group.push_back(k);
+        }
+        for (int32_t sgm = 0; sgm < M.n_segments; ++sgm) {
+            C.seg_type.push_back(M.seg_type[sgm]);
+            for (int64_t i = M.seg_offsets[sgm]; i < M.seg_offsets[sgm + 1]; ++i)
+                C.seg_nodes.push_back((int32_t)(M.seg_nodes[i] + node_base));
+            C.seg_off.push_back((int64_t)C.seg_nodes.size());
+        }
+        node_base += M.n_nodes;
+        id_base += M.n_elems;
+    }
+    C.m.n_nodes = nn;
+    C.m.node_xyz = C.xyz.data();
+    C.m.n_elems = ne;
+    C.m.elem_nodes = C.en.data();
+    C.m.elem_ids = C.ids.data();
+    C.m.n_segments = (int32_t)C.seg_type.size();
+    C.m.seg_type = C.seg_type.data();
+    C.m.seg_offsets = C.seg_off.data();
+    C.m.seg_nodes = C.seg_nodes.data();
+    return DGSW_OK;
+}
+
+int32_t dgsw_ensemble_create(const dgsw_config* cfg, int32_t n_members, const dgsw_mesh* members,
+                             const double* member_params, dgsw_handle* out) {
+    if (!cfg || !members || !out || n_members < 1) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument or no members");
+    *out = nullptr;
+    std::vector<double> params((size_t)n_members * DGSW_FN_PARAMS);
+    for (int32_t k = 0; k < n_members; ++k)
+        for (int i = 0; i < DGSW_FN_PARAMS; ++i)
+            params[(size_t)k * DGSW_FN_PARAMS + i] =
+                member_params ? member_params[(size_t)k * DGSW_FN_PARAMS + i] : cfg->fn_params[i];
+    Concat all;
+    std::string err;
+    int rc = concat_members(n_members, members, all, err);
+    if (rc) return fail(rc, err);
+    if (cfg->tile != DGSW_TILE_AUTOTUNE) return create_impl(cfg, &all.m, all.group.data(), n_members, params.data(), out);
+    // tune on the leading members, up to about 2^19 elements (all of them for a small ensemble)
+    int32_t nt = 0;
+    int64_t acc = 0;
+    while (nt < n_members && (nt == 0 || acc + members[nt].n_elems <= ((int64_t)1 << 19))) acc += members[nt++].n_elems;
+    if (nt == n_members)
+        return create_tuned(cfg, &all.m, all.group.data(), n_members, params.data(), &all.m, all.group.data(),
+                            n_members, params.data(), out);
+    Concat sub;
+    if ((rc = concat_members(nt, members, sub, err))) return fail(rc, err);
+    return create_tuned(cfg, &all.m, all.group.data(), n_members, params.data(), &sub.m, sub.group.data(), nt,
+                        params.data(), out);
+}
+
+int32_t dgsw_ensemble_member_range(dgsw_handle h, int32_t member, int64_t* first, int64_t* n_elems) {
+    if (!h || !first || !n_elems) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (h->member_first.empty()) {
+        if (member != 0) return fail(DGSW_ERR_INVALID_ARGUMENT, "not an ensemble: only member 0 exists");
+        *first = 0;
+        *n_elems = h->ne;
+        return DGSW_OK;
+    }
+    if (member < 0 || member >= h->n_members) return fail(DGSW_ERR_INVALID_ARGUMENT, "member index out of range");
+    *first = h->member_first[member];
+    *n_elems = h->member_first[member + 1] - h->member_first[member];
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_tuning(dgsw_handle h, int32_t* tiles, double* ms_per_step, int32_t* n) {
+    if (!h || !n) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    *n = h->n_tuned;
+    for (int i = 0; i < h->n_tuned; ++i) {
+        if (tiles) tiles[i] = h->tuned_tile[i];
+        if (ms_per_step) ms_per_step[i] = h->tuned_ms[i];
+    }
     return DGSW_OK;
 }
 

@@ -407,27 +407,37 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
     out.ref_of_dev.resize(ne);
     std::iota(out.ref_of_dev.begin(), out.ref_of_dev.end(), 0);
     if (morton) {
-        double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+        // Morton order of centroids within each ensemble member (members overlap in space), members
+        // kept in their order so that tiles rarely straddle two members
+        const bool grouped = !T.group.empty();
+        int32_t ng = 1;
+        if (grouped)
+            for (int64_t r = 0; r < ne; ++r) ng = std::max(ng, T.group[r] + 1);
+        std::vector<double> xmin(ng, 1e300), xmax(ng, -1e300), ymin(ng, 1e300), ymax(ng, -1e300);
         std::vector<double> cx(ne), cy(ne);
         for (int64_t r = 0; r < ne; ++r) {
             const int32_t* nd = &T.enodes[3 * r];
+            const int32_t gi = grouped ? T.group[r] : 0;
             cx[r] = (X[3 * nd[0]] + X[3 * nd[1]] + X[3 * nd[2]]) / 3.0;
             cy[r] = (X[3 * nd[0] + 1] + X[3 * nd[1] + 1] + X[3 * nd[2] + 1]) / 3.0;
-            xmin = std::min(xmin, cx[r]);
-            xmax = std::max(xmax, cx[r]);
-            ymin = std::min(ymin, cy[r]);
-            ymax = std::max(ymax, cy[r]);
+            xmin[gi] = std::min(xmin[gi], cx[r]);
+            xmax[gi] = std::max(xmax[gi], cx[r]);
+            ymin[gi] = std::min(ymin[gi], cy[r]);
+            ymax[gi] = std::max(ymax[gi], cy[r]);
         }
-        double span = std::max(xmax - xmin, ymax - ymin);
-        if (span <= 0) span = 1;
         std::vector<uint64_t> key(ne);
         for (int64_t r = 0; r < ne; ++r) {
-            uint64_t ix = (uint64_t)std::min(2097151.0, std::floor((cx[r] - xmin) / span * 2097151.0));
-            uint64_t iy = (uint64_t)std::min(2097151.0, std::floor((cy[r] - ymin) / span * 2097151.0));
+            const int32_t gi = grouped ? T.group[r] : 0;
+            double span = std::max(xmax[gi] - xmin[gi], ymax[gi] - ymin[gi]);
+            if (span <= 0) span = 1;
+            uint64_t ix = (uint64_t)std::min(2097151.0, std::floor((cx[r] - xmin[gi]) / span * 2097151.0));
+            uint64_t iy = (uint64_t)std::min(2097151.0, std::floor((cy[r] - ymin[gi]) / span * 2097151.0));
             key[r] = spread21(ix) | spread21(iy) << 1;
         }
-        std::stable_sort(out.ref_of_dev.begin(), out.ref_of_dev.end(),
-                         [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+        std::stable_sort(out.ref_of_dev.begin(), out.ref_of_dev.end(), [&](int32_t a, int32_t b) {
+            const int32_t ga = grouped ? T.group[a] : 0, gb = grouped ? T.group[b] : 0;
+            return ga != gb ? ga < gb : key[a] < key[b];
+        });
     }
     out.dev_of_ref.resize(ne);
     for (int64_t d = 0; d < ne; ++d) out.dev_of_ref[out.ref_of_dev[d]] = (int32_t)d;
@@ -579,6 +589,7 @@ void project_initial_condition(const Topology& T, const double* X, const Tables&
         double aJ;
         elem_geom(X, no, aJ);
         double* qe = &q[r * 3 * nd];
+        const double* params = T.group.empty() ? cfg.fn_params : &T.group_params[(size_t)T.group[r] * DGSW_FN_PARAMS];
         if (cfg.ic_type == 0) {
             for (int v = 0; v < 3; ++v) {
                 double nodal[3] = {cfg.ic_const[v], cfg.ic_const[v], cfg.ic_const[v]};
@@ -590,7 +601,7 @@ void project_initial_condition(const Topology& T, const double* X, const Tables&
                 double x = X[3 * no[0]] * tb.psi[0][gp] + X[3 * no[1]] * tb.psi[1][gp] + X[3 * no[2]] * tb.psi[2][gp];
                 double y = X[3 * no[0] + 1] * tb.psi[0][gp] + X[3 * no[1] + 1] * tb.psi[1][gp] +
                            X[3 * no[2] + 1] * tb.psi[2][gp];
-                dgsw_fn3 f = dgsw_fn_ic(cfg.function_set, cfg.fn_params, 0.0, x, y);
+                dgsw_fn3 f = dgsw_fn_ic(cfg.function_set, params, 0.0, x, y);
                 fg[0][gp] = f.ze;
                 fg[1][gp] = f.qx;
                 fg[2][gp] = f.qy;

@@ -33,6 +33,10 @@ struct Topology {
     std::vector<uint8_t> order_count;  // [ne]
     std::vector<uint8_t> order_face;   // [3*ne]
     std::vector<uint8_t> is_in;        // [3*ne] element is the "in" side of the interface on this face
+    // ensembles: member of element r (empty for a single problem) and each member's function-set
+    // parameters [n_members][DGSW_FN_PARAMS]
+    std::vector<int32_t> group;
+    std::vector<double> group_params;
 };
 
 // reference MeshMetaData + create_interfaces/create_boundaries semantics

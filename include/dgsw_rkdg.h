@@ -21,6 +21,7 @@ extern "C" {
 #endif
 
 #define DGSW_ABI_VERSION 1
+#define DGSW_TILE_AUTOTUNE (-1)
 
 typedef enum {
     DGSW_OK = 0,
@@ -62,7 +63,9 @@ typedef struct {
     /* execution options (no reference counterpart) */
     int32_t precision;         /* dgsw_precision: FP64, or FP32 bulk with FP64 wet/dry tests and reductions */
     int32_t device;            /* CUDA device ordinal */
-    int32_t tile;              /* elements per CTA tile: 0 = autotune, else 64/128/256 */
+    int32_t tile;              /* elements per stage-kernel tile: 128 or 256; 0 = by order (256 at p = 1,
+                                  128 at p = 2); DGSW_TILE_AUTOTUNE = measure both on the device at
+                                  create and keep the faster (dgsw_rkdg_tuning reports the timings) */
     int32_t renumber;          /* 0 keep input order, 1 Morton order of element centroids (default 1) */
     int32_t use_graphs;        /* capture each RK step in a CUDA graph (default 1) */
     int32_t reserved[8];
@@ -104,6 +107,24 @@ void dgsw_config_default(dgsw_config* cfg);
  * builds topology, interface/boundary order and device geometry. Does not set the state. */
 int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_handle* out);
 int32_t dgsw_rkdg_destroy(dgsw_handle h);
+
+/* Ensemble batching (no counterpart in the reference, which runs one mesh per process): n_members
+ * independent problems that share one configuration (order, RK method, dt, wetting/drying, limiter,
+ * precision) but each have their own mesh, bathymetry and initial-condition parameters
+ * (member_params: [n_members][16] values of the configuration's function set, NULL = cfg->fn_params for
+ * all; sources and function boundaries use cfg->fn_params). All members advance together: one
+ * stage-kernel launch per RK stage covers every member, and dgsw_rkdg_step replays one CUDA graph per
+ * step. The handle behaves like any other: the state and wet flags are laid out member after member
+ * (member k's elements in ascending order of its own element IDs), see dgsw_ensemble_member_range.
+ * With cfg->tile == DGSW_TILE_AUTOTUNE the tile size is tuned on the leading members (about 2^19
+ * elements). */
+int32_t dgsw_ensemble_create(const dgsw_config* cfg, int32_t n_members, const dgsw_mesh* members,
+                             const double* member_params, dgsw_handle* out);
+/* element range of one member in the handle's state order (a single problem is member 0) */
+int32_t dgsw_ensemble_member_range(dgsw_handle h, int32_t member, int64_t* first, int64_t* n_elems);
+/* the autotuner's record: candidate tile sizes and device milliseconds per step (n = 0 when the handle
+ * was not tuned, or reused a cached decision); arrays of 4 */
+int32_t dgsw_rkdg_tuning(dgsw_handle h, int32_t* tiles, double* ms_per_step, int32_t* n);
 int32_t dgsw_rkdg_info(dgsw_handle h, dgsw_info* out);
 
 /* Problem::preprocessor_serial -> initialize_data_serial (swe_pre_init_data.hpp:9-327): bathymetry and
