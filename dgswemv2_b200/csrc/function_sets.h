@@ -273,7 +273,13 @@ DGSW_HD void dgsw_sincos(double a, double* s, double* c) {
 }
 DGSW_HD void dgsw_sincos(float a, float* s, float* c) {
 #if defined(__CUDA_ARCH__)
-    sincosf(a, s, c);
+    // FP32 bulk path: reduce to [-pi, pi] with a two-term Cody-Waite split of 2 pi (6.28125 is exact in
+    // FP32 with a short mantissa, so n * 6.28125 is exact for the small n met here), then the hardware
+    // sine/cosine, whose absolute error there is a few 1e-7 - below the FP32 state's own rounding
+    const float n = rintf(a * 0.15915494309189535f);
+    float r = fmaf(-n, 6.28125f, a);
+    r = fmaf(-n, 1.9353071795864769e-3f, r);
+    __sincosf(r, s, c);
 #else
     *s = sinf(a);
     *c = cosf(a);

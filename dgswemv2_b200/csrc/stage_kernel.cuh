@@ -170,6 +170,50 @@ __device__ __noinline__ void fn_eval_dev(int id, const double* P, const dgsw_fn_
     dgsw_fn_eval<Real>(id, P, *T, source, x, y, out);
 }
 
+// The manufactured sine set's source terms inline (FP32 path), with its constants hoisted out of the
+// quadrature loops (the same formulas as dgsw_fn_eval, function_sets.h); every other set, and the FP64
+// path, goes through fn_eval_dev.
+template <typename Real>
+struct SineSrc {
+    Real k, A, B, w, st, ct, g, H;
+};
+
+template <typename Real>
+__device__ __forceinline__ SineSrc<Real> sine_src_prepare(const double* P, const dgsw_fn_time& T) {
+    SineSrc<Real> S;
+    S.k = (Real)(2.0 * M_PI / P[0]);
+    S.A = (Real)P[1];
+    S.w = (Real)T.s[2];
+    S.B = (Real)(P[1] * T.s[2] / (2.0 * (2.0 * M_PI / P[0])));
+    S.st = (Real)T.s[0];
+    S.ct = (Real)T.s[1];
+    S.g = (Real)P[4];
+    S.H = (Real)P[2];
+    return S;
+}
+
+template <typename Real>
+__device__ __forceinline__ void sine_src_eval(const SineSrc<Real>& S, Real x, Real y, Real (&out)[3]) {
+    Real sx, cx, sy, cy;
+    dgsw_sincos(S.k * x, &sx, &cx);
+    dgsw_sincos(S.k * y, &sy, &cy);
+    const Real A = S.A, B = S.B, k = S.k, w = S.w, st = S.st, ct = S.ct;
+    const Real ze = A * sx * cy * ct;
+    const Real qx = -B * cx * cy * st;
+    const Real qy = B * sx * sy * st;
+    const Real zex = A * k * cx * cy * ct, zey = -A * k * sx * sy * ct, zet = -A * w * sx * cy * st;
+    const Real qxx = B * k * sx * cy * st, qxy = B * k * cx * sy * st, qxt = -B * w * cx * cy * ct;
+    const Real qyx = B * k * cx * sy * st, qyy = B * k * sx * cy * st, qyt = B * w * sx * sy * ct;
+    const Real h = ze + S.H;
+    const Real ih = Real(1) / h;
+    const Real ih2 = ih * ih;
+    out[0] = zet + qxx + qyy;
+    out[1] = qxt + (Real(2) * qx * qxx * ih - qx * qx * zex * ih2) + ((qxy * qy + qx * qyy) * ih - qx * qy * zey * ih2) +
+             S.g * h * zex;
+    out[2] = qyt + ((qxx * qy + qx * qyx) * ih - qx * qy * zex * ih2) + (Real(2) * qy * qyy * ih - qy * qy * zey * ih2) +
+             S.g * h * zey;
+}
+
 // ------------------------------------------------------------------------------------------------
 // wetting/drying of one p>=1 element on its vertex values, swe_post_wet_dry.hpp:6-145, in FP64.
 // qv: modal state (first three modes carry the linear part); returns the new wet flag and writes
@@ -353,9 +397,12 @@ struct Smem {
 };
 
 // resident CTAs per SM the register budget is sized for
+#ifndef DGSW_F32_MB128
+#define DGSW_F32_MB128 4
+#endif
 template <int P, typename Real, int TILE>
 struct MinBlocks {
-    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? 4 : 2) : (TILE == 128 ? 2 : 1);
+    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? DGSW_F32_MB128 : 2) : (TILE == 128 ? 2 : 1);
 };
 
 template <int P, typename Real, bool WD, bool FSRC, int TILE>
@@ -383,6 +430,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     const Real g = (Real)A.g;
     const Real* __restrict__ qs = A.qk[A.nterms - 1];  // this stage's state
     const dgsw_fn_time FT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
+    // FP32 only: in FP64 the inlined double sine/cosine raise register pressure more than the call costs
+    const bool sine_set = FSRC && sizeof(Real) == 4 && A.fn_set == DGSW_FN_MANUFACTURED_SINE;
+    SineSrc<Real> SS;
+    if (sine_set) SS = sine_src_prepare<Real>(A.fn_params, FT);
 
     Real rhs[3][ND];
 #pragma unroll
@@ -465,7 +516,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                 Real S[3] = {Real(0), g * (dbx * qg[0]), g * (dby * qg[0])};
                 if (FSRC) {
                     Real fs[3];
-                    fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, (Real)xg, (Real)yg, fs);
+                    if (sine_set)
+                        sine_src_eval<Real>(SS, (Real)xg, (Real)yg, fs);
+                    else
+                        fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, (Real)xg, (Real)yg, fs);
                     S[0] += fs[0];
                     S[1] += fs[1];
                     S[2] += fs[2];
