@@ -100,7 +100,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n):
+def dist_setup(n, backend=None):
+    """One process per GPU from the torchrun environment; NCCL on GPUs (gloo when no GPU is visible, which
+    is how the rank logic is tested on a CPU host)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -110,19 +112,25 @@ def dist_setup(n):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
 def dist_max(x, world):
+    """Max over ranks (every rank takes this collective in the same order)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -130,12 +138,19 @@ def dist_max(x, world):
 def barrier(world):
     import torch
 
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+
+
+def job_value(units_per_step, steps, world, max_ms):
+    """Whole-job throughput of N replicas: all ranks' units over the slowest rank's time."""
+    return units_per_step * steps * world / (max_ms / 1e3)
 
 
 def load_peaks():
@@ -259,7 +274,7 @@ def run_ours(args):
         ms, launches, wall = time_steps(P, args.steps)
         barrier(world)
     ms = dist_max(ms, world)
-    value = units_per_step * args.steps * world / (ms / 1e3)
+    value = job_value(units_per_step, args.steps, world, ms)
 
     # the FP64 plain path on the same workload (the comparator of the FP32 path)
     fp64 = None
@@ -271,7 +286,7 @@ def run_ours(args):
         ms64, _, _ = time_steps(P64, args.steps)
         barrier(world)
         ms64 = dist_max(ms64, world)
-        fp64 = {"value": units_per_step * args.steps * world / (ms64 / 1e3), "ms_per_step": ms64 / args.steps}
+        fp64 = {"value": job_value(units_per_step, args.steps, world, ms64), "ms_per_step": ms64 / args.steps}
         l2_32, l2_64 = P.compute_residual_L2(), P64.compute_residual_L2()
         fp64["l2_error_fp64"] = l2_64
         fp64["l2_error_fp32"] = l2_32
