@@ -659,6 +659,40 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
 
     // ---------------- phase 3: edge contributions, M^-1, RK combination, wet/dry ----------------
     if (!active) return;
+    // the earlier stages' terms of the RK combination, sum_j a_j q_j + dt b_j sol_j: all loads of one
+    // term are issued together here so that their latency overlaps the edge gather below (one
+    // dependent load per value at the end of the CTA cost a global-memory latency per value, per wave)
+    Real comb[3][ND];
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+        for (int k = 0; k < ND; ++k) comb[v][k] = Real(0);
+    for (int j = 0; j < A.nterms - 1; ++j) {
+        const Real* __restrict__ qj = A.qk[j];
+        const Real aj = (Real)A.a[j];
+        Real t[3][ND];
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int k = 0; k < ND; ++k) t[v][k] = qj[(v * ND + k) * P_ + d];
+        if (A.bdt[j] != 0.0) {
+            const Real* __restrict__ sj = A.solk[j];
+            const Real bj = (Real)A.bdt[j];
+            Real u[3][ND];
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int k = 0; k < ND; ++k) u[v][k] = sj[(v * ND + k) * P_ + d];
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int k = 0; k < ND; ++k) comb[v][k] += bj * u[v][k];
+        }
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int k = 0; k < ND; ++k) comb[v][k] += aj * t[v][k];
+    }
     const int2 es = A.eslot[d];
     const int roles = es.y & 7;
     const int ord = es.y >> 3;
@@ -717,11 +751,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             const Real sol = rhs[v][k] * mk;
             const int idx = (v * ND + k) * P_ + d;
             if (A.store_sol) A.sol_out[idx] = sol;
-            Real acc = Real(0);
-            for (int j = 0; j < A.nterms - 1; ++j) {
-                acc += (Real)A.a[j] * A.qk[j][idx];
-                if (A.bdt[j] != 0.0) acc += (Real)A.bdt[j] * A.solk[j][idx];
-            }
+            Real acc = comb[v][k];
             const int j = A.nterms - 1;
             acc += (Real)A.a[j] * sq[(v * ND + k) * TILE + tid] + (Real)A.bdt[j] * sol;
             qn[v][k] = acc;
