@@ -442,6 +442,8 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
         for (int k = 0; k < ND; ++k) rhs[v][k] = Real(0);
     Real aJ = Real(1);
     bool wet = false;
+    // this element's edge slots for phase 3, loaded now so that the latency is hidden
+    const int2 es = active ? A.eslot[d] : make_int2(0, 0);
 
     // ---------------- phase 1: volume + source integrals, face traces ----------------
     if (active) {
@@ -593,13 +595,29 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     {
         const int eoff = A.tile_edge_off[tile];
         const int nedge = A.tile_edge_off[tile + 1] - eoff;
+        // the next edge's record and geometry are loaded one iteration ahead
+        int4 rec_n = make_int4(0, 0, 0, 0);
+        Real nx_n = Real(0), ny_n = Real(0), sj_n = Real(0);
+        if (tid < nedge) {
+            rec_n = A.edges[eoff + tid];
+            nx_n = A.egeo[eoff + tid];
+            ny_n = A.egeo[A.n_edges + eoff + tid];
+            sj_n = A.egeo[2 * A.n_edges + eoff + tid];
+        }
 #pragma unroll 1
         for (int le = tid; le < nedge; le += TILE) {
-            const int4 rec = A.edges[eoff + le];
+            const int4 rec = rec_n;
+            const Real nx = nx_n, ny = ny_n;
+            ssJ[le] = sj_n;
+            if (le + TILE < nedge) {
+                const int nle = eoff + le + TILE;
+                rec_n = A.edges[nle];
+                nx_n = A.egeo[nle];
+                ny_n = A.egeo[A.n_edges + nle];
+                sj_n = A.egeo[2 * A.n_edges + nle];
+            }
             const int sa = rec.x, sb = rec.y;
             const int kind = (rec.z >> 4) & 3;
-            const Real nx = A.egeo[eoff + le], ny = A.egeo[A.n_edges + eoff + le];
-            ssJ[le] = A.egeo[2 * A.n_edges + eoff + le];
             const bool wa = swet[sa] != 0;
             const bool wb = sb >= 0 && swet[sb] != 0;
             const bool compute = (kind == 0) ? (wa || wb) : wa;
@@ -693,7 +711,6 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
 #pragma unroll
             for (int k = 0; k < ND; ++k) comb[v][k] += aj * t[v][k];
     }
-    const int2 es = A.eslot[d];
     const int roles = es.y & 7;
     const int ord = es.y >> 3;
     const int cnt = ord & 3;
