@@ -502,11 +502,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                 const Real pe = g * (Real(0.5) * qg[0] * qg[0] + qg[0] * bg);
                 Real Fx[3] = {qg[1], u * qg[1] + pe, u * qg[2]};
                 Real Fy[3] = {qg[2], u * qg[2], vv * qg[2] + pe};
-                double xg = 0.0, yg = 0.0;
-                if (FSRC || A.spherical) {
+                double yg = 0.0;
+                if (A.spherical) {
                     constexpr double s0 = MT<P>::psi(0 * NQ + gp), s1 = MT<P>::psi(1 * NQ + gp),
                                      s2 = MT<P>::psi(2 * NQ + gp);
-                    xg = x0 * s0 + x1 * s1 + x2 * s2;
                     yg = y0 * s0 + y1 * s1 + y2 * s2;
                 }
                 if (A.spherical) {
@@ -514,18 +513,8 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
 #pragma unroll
                     for (int v = 0; v < 3; ++v) Fx[v] = sp * Fx[v];
                 }
-                // bathymetry-slope source, swe_source.hpp:15-21
+                // bathymetry-slope source, swe_source.hpp:15-21 (the analytic source follows in its own loop)
                 Real S[3] = {Real(0), g * (dbx * qg[0]), g * (dby * qg[0])};
-                if (FSRC) {
-                    Real fs[3];
-                    if (sine_set)
-                        sine_src_eval<Real>(SS, (Real)xg, (Real)yg, fs);
-                    else
-                        fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, (Real)xg, (Real)yg, fs);
-                    S[0] += fs[0];
-                    S[1] += fs[1];
-                    S[2] += fs[2];
-                }
                 // int F . grad(phi) = sum_gp sum_z (F_x J^-1(z,x) + F_y J^-1(z,y)) dphi_z w
                 sfor<0, 3>([&](auto V) {
                     constexpr int v = decltype(V)::value;
@@ -544,6 +533,30 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                     });
                 });
             });
+            // analytic source_q(t, x_gp) (swe_source.hpp:9-14), in a loop of its own so that its
+            // temporaries are not live together with the flux computation's
+            if (FSRC) {
+                sfor<0, NQ>([&](auto GP) {
+                    constexpr int gp = decltype(GP)::value;
+                    constexpr double s0 = MT<P>::psi(0 * NQ + gp), s1 = MT<P>::psi(1 * NQ + gp),
+                                     s2 = MT<P>::psi(2 * NQ + gp);
+                    const double xg = x0 * s0 + x1 * s1 + x2 * s2;
+                    const double yg = y0 * s0 + y1 * s1 + y2 * s2;
+                    Real fs[3];
+                    if (sine_set)
+                        sine_src_eval<Real>(SS, (Real)xg, (Real)yg, fs);
+                    else
+                        fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, (Real)xg, (Real)yg, fs);
+                    sfor<0, 3>([&](auto V) {
+                        constexpr int v = decltype(V)::value;
+                        sfor<0, ND>([&](auto K) {
+                            constexpr int k = decltype(K)::value;
+                            constexpr double pw = MT<P>::phiw(gp * ND + k);
+                            if constexpr (pw != 0.0) rhs[v][k] += fs[v] * (Real)pw;
+                        });
+                    });
+                });
+            }
 #pragma unroll
             for (int v = 0; v < 3; ++v)
 #pragma unroll
