@@ -405,9 +405,20 @@ struct MinBlocks {
     static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? DGSW_F32_MB128 : 2) : (TILE == 128 ? 2 : 1);
 };
 
-template <int P, typename Real, bool WD, bool FSRC, int TILE>
+// shared-memory capacities a tile almost always fits (measured: about 0.27 TILE halo faces and 1.65 TILE
+// edges on structured and jittered meshes); with CAPPED the trace and flux strides are these
+// compile-time constants, so every shared-memory access has an immediate offset
+template <int TILE>
+struct TileCap {
+    static constexpr int halo = TILE / 2;
+    static constexpr int edges = 2 * TILE;
+};
+
+template <int P, typename Real, bool WD, bool FSRC, int TILE, bool CAPPED>
 __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
-    rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_halo, int max_edges) {
+    rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_halo_rt, int max_edges_rt) {
+    const int max_halo = CAPPED ? TileCap<TILE>::halo : max_halo_rt;
+    const int max_edges = CAPPED ? TileCap<TILE>::edges : max_edges_rt;
     constexpr int ND = MT<P>::ND, NQ = MT<P>::NQ, NG = MT<P>::NG;
     using SM = Smem<P, Real, WD>;
     const int NS = SM::nslot(TILE, max_halo);  // trace slots: 3 per tile element, then halo faces
@@ -830,8 +841,10 @@ cudaError_t launch_stage_p2_f32(const StageArgs<float>& A, int tile, int ntiles,
 
 template <int P, typename Real, bool WD, bool FSRC, int TILE>
 cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo, int max_edges, cudaStream_t s) {
-    auto kern = rkdg_stage_kernel<P, Real, WD, FSRC, TILE>;
-    const size_t smem = Smem<P, Real, WD>::bytes(TILE, max_halo, max_edges);
+    const bool capped = max_halo <= TileCap<TILE>::halo && max_edges <= TileCap<TILE>::edges;
+    auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, TILE, true> : rkdg_stage_kernel<P, Real, WD, FSRC, TILE, false>;
+    const size_t smem = capped ? Smem<P, Real, WD>::bytes(TILE, TileCap<TILE>::halo, TileCap<TILE>::edges)
+                               : Smem<P, Real, WD>::bytes(TILE, max_halo, max_edges);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)ntiles, TILE, smem, s>>>(A, max_halo, max_edges);
