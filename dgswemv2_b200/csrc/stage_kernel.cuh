@@ -175,18 +175,23 @@ __device__ __noinline__ void fn_eval_dev(int id, const double* P, const dgsw_fn_
 // path, goes through fn_eval_dev.
 template <typename Real>
 struct SineSrc {
-    Real k, A, B, w, st, ct, g, H;
+    // ze = c1 P, qx = -c2 Q, qy = c2 R, zex = c3 Q, zey = -c3 R, zet = -c4 P, qxx = qyy = c5 P,
+    // qxy = qyx = c5 S, qxt = -c6 Q, qyt = c6 R with P = sx cy, Q = cx cy, R = sx sy, S = cx sy
+    Real k, c1, c2, c3, c5, c6, c0, g, H;  // c0 = 2 c5 - c4 (the continuity source)
 };
 
 template <typename Real>
 __device__ __forceinline__ SineSrc<Real> sine_src_prepare(const double* P, const dgsw_fn_time& T) {
+    const double k = 2.0 * M_PI / P[0], A = P[1], w = T.s[2], B = P[1] * T.s[2] / (2.0 * k);
+    const double st = T.s[0], ct = T.s[1];
     SineSrc<Real> S;
-    S.k = (Real)(2.0 * M_PI / P[0]);
-    S.A = (Real)P[1];
-    S.w = (Real)T.s[2];
-    S.B = (Real)(P[1] * T.s[2] / (2.0 * (2.0 * M_PI / P[0])));
-    S.st = (Real)T.s[0];
-    S.ct = (Real)T.s[1];
+    S.k = (Real)k;
+    S.c1 = (Real)(A * ct);
+    S.c2 = (Real)(B * st);
+    S.c3 = (Real)(A * k * ct);
+    S.c5 = (Real)(B * k * st);
+    S.c6 = (Real)(B * w * ct);
+    S.c0 = (Real)(2.0 * B * k * st - A * w * st);
     S.g = (Real)P[4];
     S.H = (Real)P[2];
     return S;
@@ -197,20 +202,17 @@ __device__ __forceinline__ void sine_src_eval(const SineSrc<Real>& S, Real x, Re
     Real sx, cx, sy, cy;
     dgsw_sincos(S.k * x, &sx, &cx);
     dgsw_sincos(S.k * y, &sy, &cy);
-    const Real A = S.A, B = S.B, k = S.k, w = S.w, st = S.st, ct = S.ct;
-    const Real ze = A * sx * cy * ct;
-    const Real qx = -B * cx * cy * st;
-    const Real qy = B * sx * sy * st;
-    const Real zex = A * k * cx * cy * ct, zey = -A * k * sx * sy * ct, zet = -A * w * sx * cy * st;
-    const Real qxx = B * k * sx * cy * st, qxy = B * k * cx * sy * st, qxt = -B * w * cx * cy * ct;
-    const Real qyx = B * k * cx * sy * st, qyy = B * k * sx * cy * st, qyt = B * w * sx * sy * ct;
-    const Real h = ze + S.H;
+    const Real Pp = sx * cy, Q = cx * cy, R = sx * sy, Sq = cx * sy;
+    const Real qx = -S.c2 * Q, qy = S.c2 * R;
+    const Real zex = S.c3 * Q, zey = -S.c3 * R;
+    const Real qxx = S.c5 * Pp, qxy = S.c5 * Sq;  // qyy = qxx, qyx = qxy
+    const Real h = S.c1 * Pp + S.H;
     const Real ih = Real(1) / h;
     const Real ih2 = ih * ih;
-    out[0] = zet + qxx + qyy;
-    out[1] = qxt + (Real(2) * qx * qxx * ih - qx * qx * zex * ih2) + ((qxy * qy + qx * qyy) * ih - qx * qy * zey * ih2) +
-             S.g * h * zex;
-    out[2] = qyt + ((qxx * qy + qx * qyx) * ih - qx * qy * zex * ih2) + (Real(2) * qy * qyy * ih - qy * qy * zey * ih2) +
+    out[0] = S.c0 * Pp;
+    out[1] = -S.c6 * Q + (Real(2) * qx * qxx * ih - qx * qx * zex * ih2) +
+             ((qxy * qy + qx * qxx) * ih - qx * qy * zey * ih2) + S.g * h * zex;
+    out[2] = S.c6 * R + ((qxx * qy + qx * qxy) * ih - qx * qy * zex * ih2) + (Real(2) * qy * qxx * ih - qy * qy * zey * ih2) +
              S.g * h * zey;
 }
 
@@ -393,8 +395,26 @@ struct Smem {
     static __host__ __device__ size_t off_flag(int tile, int mh, int me) {
         return off_wet(tile, mh, me) + al((size_t)nslot(tile, mh));
     }
-    static __host__ __device__ size_t bytes(int tile, int mh, int me) { return off_flag(tile, mh, me) + al((size_t)me); }
+    // halo staging: the state and bathymetry modes of each halo face's element, copied asynchronously
+    static __host__ __device__ size_t off_halo(int tile, int mh, int me) { return off_flag(tile, mh, me) + al((size_t)me); }
+    static __host__ __device__ size_t bytes(int tile, int mh, int me) {
+        return off_halo(tile, mh, me) + al(sizeof(Real) * (size_t)(3 * ND + 3) * mh);
+    }
 };
+
+// asynchronous global -> shared copies of one 4- or 8-byte value (the thread does not wait for it)
+template <typename Real>
+__device__ __forceinline__ void cp_async_value(Real* dst, const Real* src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(Real) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_and_wait() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
 
 // resident CTAs per SM the register budget is sized for
 #ifndef DGSW_F32_MB128
@@ -429,6 +449,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     Real* ssJ = reinterpret_cast<Real*>(smem_raw + SM::off_sJ(TILE, max_halo, max_edges));
     unsigned char* swet = smem_raw + SM::off_wet(TILE, max_halo, max_edges);        // [NS]
     unsigned char* sflag = smem_raw + SM::off_flag(TILE, max_halo, max_edges);      // [max_edges]
+    Real* shq = reinterpret_cast<Real*>(smem_raw + SM::off_halo(TILE, max_halo, max_edges));  // [3*ND+3][max_halo]
 
     const int tile = blockIdx.x;
     const int e0 = tile * TILE;
@@ -455,6 +476,20 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     bool wet = false;
     // this element's edge slots for phase 3, loaded now so that the latency is hidden
     const int2 es = active ? A.eslot[d] : make_int2(0, 0);
+    // with capped tiles (at most TILE / 2 halo faces) thread h < nh owns halo face h: its record is
+    // loaded now and its element's data copied asynchronously into shared memory during phase 1
+    const int hoff = A.tile_halo_off[tile];
+    const int nh = A.tile_halo_off[tile + 1] - hoff;
+    int2 hrec = make_int2(0, -1);
+    if (CAPPED && tid < nh) hrec = A.halo[hoff + tid];
+    bool hwet = false;
+    auto issue_halo_copies = [&]() {
+#pragma unroll
+        for (int c = 0; c < 3 * ND; ++c) cp_async_value<Real>(&shq[c * max_halo + tid], &qs[c * P_ + hrec.x]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) cp_async_value<Real>(&shq[(3 * ND + k) * max_halo + tid], &A.bath[k * P_ + hrec.x]);
+        hwet = A.wet_in[hrec.x] != 0;
+    };
 
     // ---------------- phase 1: volume + source integrals, face traces ----------------
     if (active) {
@@ -465,6 +500,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             q[c / ND][c % ND] = val;
             sq[c * TILE + tid] = val;
         }
+        if (CAPPED && hrec.y >= 0) issue_halo_copies();
 #pragma unroll
         for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + d];
         const Real Ji00 = A.geo[d], Ji01 = A.geo[P_ + d], Ji10 = A.geo[2 * P_ + d], Ji11 = A.geo[3 * P_ + d];
@@ -547,17 +583,20 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             // analytic source_q(t, x_gp) (swe_source.hpp:9-14), in a loop of its own so that its
             // temporaries are not live together with the flux computation's
             if (FSRC) {
+                const Real xr0 = (Real)x0, xr1 = (Real)x1, xr2 = (Real)x2;
+                const Real yr0 = (Real)y0, yr1 = (Real)y1, yr2 = (Real)y2;
                 sfor<0, NQ>([&](auto GP) {
                     constexpr int gp = decltype(GP)::value;
                     constexpr double s0 = MT<P>::psi(0 * NQ + gp), s1 = MT<P>::psi(1 * NQ + gp),
                                      s2 = MT<P>::psi(2 * NQ + gp);
-                    const double xg = x0 * s0 + x1 * s1 + x2 * s2;
-                    const double yg = y0 * s0 + y1 * s1 + y2 * s2;
+                    // FP32 path: Gauss-point coordinates in FP32 (the analytic source is evaluated in FP32)
+                    const Real xg = xr0 * (Real)s0 + xr1 * (Real)s1 + xr2 * (Real)s2;
+                    const Real yg = yr0 * (Real)s0 + yr1 * (Real)s1 + yr2 * (Real)s2;
                     Real fs[3];
                     if (sine_set)
-                        sine_src_eval<Real>(SS, (Real)xg, (Real)yg, fs);
+                        sine_src_eval<Real>(SS, xg, yg, fs);
                     else
-                        fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, (Real)xg, (Real)yg, fs);
+                        fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, xg, yg, fs);
                     sfor<0, 3>([&](auto V) {
                         constexpr int v = decltype(V)::value;
                         sfor<0, ND>([&](auto K) {
@@ -587,9 +626,30 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
         });
     }
     // halo faces: faces of elements in other tiles that this tile's edges need
-    {
-        const int hoff = A.tile_halo_off[tile];
-        const int nh = A.tile_halo_off[tile + 1] - hoff;
+    if (CAPPED) {
+        if (hrec.y >= 0) {
+            if (!active) issue_halo_copies();  // threads past the last element of the last tile
+            const int h = tid;
+            cp_async_commit_and_wait();  // this thread's own copies
+            Real q[3][ND], b[3], t[4][NG];
+#pragma unroll
+            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = shq[c * max_halo + h];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) b[k] = shq[(3 * ND + k) * max_halo + h];
+            if (hrec.y == 0)
+                face_trace<P, 0, Real>(q, b, t);
+            else if (hrec.y == 1)
+                face_trace<P, 1, Real>(q, b, t);
+            else
+                face_trace<P, 2, Real>(q, b, t);
+            const int slot = 3 * TILE + h;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int gg = 0; gg < NG; ++gg) str[(c * NG + gg) * NS + slot] = t[c][gg];
+            swet[slot] = hwet ? 1 : 0;
+        }
+    } else {
 #pragma unroll 1
         for (int h = tid; h < nh; h += TILE) {
             const int2 it = A.halo[hoff + h];
