@@ -35,7 +35,7 @@ ALG_BYTES_PER_UNIT = {("fp32", 2): 45.0, ("fp64", 2): 87.0, ("fp32", 1): 52.0, (
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])

@@ -1,0 +1,61 @@
+"""Device throughput of the RK step on the named configurations, in FP32 bulk and FP64:
+
+    python -m dgswemv2_b200.throughput [config2 config3 ...] [--steps N]
+
+config1: manufactured sine, 800 triangles, p = 1, SSP-RK2 (fits in L2: a latency figure, not a roofline one)
+config2: manufactured sine, 524,288 jittered triangles, p = 2, SSP-RK3
+config3: Thacker bowl, 131,072 triangles, p = 1, SSP-RK2, wetting/drying + Cockburn-Shu limiter
+config3_nolim: the same without the limiter
+config4: Thacker bowl, 2,097,152 triangles, p = 1, SSP-RK2, wetting/drying + limiter
+Prints one JSON line per (configuration, precision): device ms per step after warm-up (CUDA events on
+the handle's stream around graph-replayed steps), element-DOF updates per second per RK stage, and the
+L2 error against the analytic solution at the end.
+"""
+import argparse
+import json
+
+from . import Problem, configs
+
+
+def build(name, precision):
+    if name == "config1":
+        return configs.config1(precision=precision)
+    if name == "config2":
+        return configs.config2(precision=precision)
+    if name == "config3":
+        return configs.config3(precision=precision)
+    if name == "config3_nolim":
+        return configs.config3(precision=precision, limiter=False)
+    if name == "config4":
+        return configs.config3(nq=1024, dt=0.06, precision=precision)
+    raise ValueError(name)
+
+
+def measure(name, precision, steps, warmup=5):
+    mesh, cfg = build(name, precision)
+    P = Problem(cfg, mesh)
+    P.step_serial(warmup)
+    P.step_serial(steps)
+    ms, launches = P.last_step_timing()
+    per_step = ms / steps
+    return {
+        "config": name, "precision": precision, "elements": P.ne, "p": cfg.p, "stages": cfg.rk_nstages,
+        "tile": P.info.tile, "steps": steps, "ms_per_step": per_step,
+        "element_dof_per_s_per_stage": P.ne * P.nd * cfg.rk_nstages / (per_step * 1e-3),
+        "kernel_launches_per_step": launches / steps, "l2_error": P.compute_residual_L2(),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("configs", nargs="*", default=["config1", "config2", "config3", "config3_nolim", "config4"])
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--precisions", default="fp32,fp64")
+    a = ap.parse_args()
+    for name in a.configs:
+        for prec in a.precisions.split(","):
+            print(json.dumps(measure(name, prec, a.steps)), flush=True)
+
+
+if __name__ == "__main__":
+    main()
