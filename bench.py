@@ -29,7 +29,10 @@ METRIC = "element-DOF updates/s per RK stage, FP32+MLP vs FP64 plain on B200 at 
 UNIT = "element-DOF/s"
 # compulsory HBM bytes per element-DOF and RK stage for p=2 SSP-RK3 (state in, q0 on 2 of 3 stages,
 # state out, per-element geometry and per-edge data, each array touched once): FP32 45 B, FP64 87 B
-ALG_BYTES_PER_UNIT = {("fp32", 2): 45.0, ("fp64", 2): 87.0, ("fp32", 1): 52.0, ("fp64", 1): 99.0}
+# compulsory HBM bytes per element-DOF per RK stage (each array touched once): stage states read
+# (1 + the fraction of stages that also read q_0) and written, FP64 in both precisions; element
+# geometry and bathymetry (FP32 in the FP32 path) and the edge records. p = 2 SSP-RK3, p = 1 SSP-RK2.
+ALG_BYTES_PER_UNIT = {("fp32", 2): 77.0, ("fp64", 2): 87.0, ("fp32", 1): 82.0, ("fp64", 1): 99.0}
 
 
 def parse():

@@ -162,22 +162,22 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     int n = 0;
     for (int k = 0; k < s; ++k) {
         if (h->rk.ark[s][k] != 0.0 || h->rk.brk[s][k] != 0.0) {
-            A.qk[n] = (const Real*)h->Q[k];
-            A.solk[n] = (const Real*)h->SOL[k];
+            A.qk[n] = (const double*)h->Q[k];
+            A.solk[n] = (const double*)h->SOL[k];
             A.a[n] = h->rk.ark[s][k];
             A.bdt[n] = h->cfg.dt * h->rk.brk[s][k];
             ++n;
         }
     }
-    A.qk[n] = (const Real*)h->Q[s];
+    A.qk[n] = (const double*)h->Q[s];
     A.solk[n] = nullptr;
     A.a[n] = h->rk.ark[s][s];
     A.bdt[n] = h->cfg.dt * h->rk.brk[s][s];
     ++n;
     A.nterms = n;
     A.store_sol = h->need_sol[s] ? 1 : 0;
-    A.sol_out = (Real*)h->SOL[s];
-    A.q_out = (Real*)h->Q[s + 1];
+    A.sol_out = (double*)h->SOL[s];
+    A.q_out = (double*)h->Q[s + 1];
     A.bath = (const Real*)h->bath;
     A.geo = (const Real*)h->geo;
     A.enodes = h->enodes.p;
@@ -327,10 +327,8 @@ cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageR
     }
     if (rec) {
         // features of the state the limiter is about to see; ok flags into the label buffer
-        e = h->fp32 ? launch_indicator_features<float>(feature_args<float>(h, s_out), h->ref_of_dev.p, rec->features,
-                                                        rec->labels, h->stream)
-                    : launch_indicator_features<double>(feature_args<double>(h, s_out), h->ref_of_dev.p,
-                                                         rec->features, rec->labels, h->stream);
+        e = launch_indicator_features<double>(feature_args<double>(h, s_out), h->ref_of_dev.p, rec->features,
+                                              rec->labels, h->stream);
         if (e != cudaSuccess) return e;
         ++launches;
     }
@@ -338,11 +336,11 @@ cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageR
         const int mode = h->ind_mode;
         if (rec) h->ind_mode = 0;  // labels come from the plain limiter
         if (h->ind_mode) {
-            e = h->fp32 ? launch_indicator_gate<float>(h, s_out) : launch_indicator_gate<double>(h, s_out);
+            e = launch_indicator_gate<double>(h, s_out);
             if (e != cudaSuccess) return e;
             ++launches;
         }
-        e = h->fp32 ? launch_limiter<float>(h, s_out) : launch_limiter<double>(h, s_out);
+        e = launch_limiter<double>(h, s_out);
         h->ind_mode = mode;
         if (e != cudaSuccess) return e;
         ++launches;
@@ -406,10 +404,8 @@ int upload_state(dgsw_rkdg_s* h, const double* q) {
     if (rc) return rc;
     const size_t bytes = (size_t)h->ne * 3 * h->nd * sizeof(double);
     CUDA_TRY(cudaMemcpyAsync(h->staging.p, q, bytes, cudaMemcpyHostToDevice, h->stream));
-    cudaError_t e = h->fp32 ? launch_permute_in<double, float>(h->staging.p, (float*)h->Q[h->stage], h->ref_of_dev.p,
-                                                               (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream)
-                            : launch_permute_in<double, double>(h->staging.p, (double*)h->Q[h->stage], h->ref_of_dev.p,
-                                                                (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    cudaError_t e = launch_permute_in<double, double>(h->staging.p, (double*)h->Q[h->stage], h->ref_of_dev.p,
+                                                      (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("set_state: ") + cudaGetErrorString(e));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return DGSW_OK;
@@ -418,12 +414,8 @@ int upload_state(dgsw_rkdg_s* h, const double* q) {
 int download_state(dgsw_rkdg_s* h, double* q) {
     int rc = ensure_staging(h);
     if (rc) return rc;
-    cudaError_t e = h->fp32 ? launch_permute_out<float, double>((const float*)h->Q[h->stage], h->staging.p,
-                                                                h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
-                                                                h->stream)
-                            : launch_permute_out<double, double>((const double*)h->Q[h->stage], h->staging.p,
-                                                                 h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
-                                                                 h->stream);
+    cudaError_t e = launch_permute_out<double, double>((const double*)h->Q[h->stage], h->staging.p, h->ref_of_dev.p,
+                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("get_state: ") + cudaGetErrorString(e));
     const size_t bytes = (size_t)h->ne * 3 * h->nd * sizeof(double);
     CUDA_TRY(cudaMemcpyAsync(q, h->staging.p, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -444,7 +436,7 @@ int run_reduction(dgsw_rkdg_s* h, int what, double* out) {
     ReduceArgs<Real> R;
     std::memset(&R, 0, sizeof(R));
     // the L2 error reads state[0] (swe_post_comp_res_l2.hpp:12), the mass the current stage state
-    R.q = (const Real*)h->Q[what == 0 ? 0 : h->stage];
+    R.q = (const double*)h->Q[what == 0 ? 0 : h->stage];
     R.bath = (const Real*)h->bath;
     R.enodes = h->enodes.p;
     R.xy = h->xy.p;
@@ -604,7 +596,7 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
     if (h->sm_count <= 0) h->sm_count = 148;
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
-    const size_t state_bytes = (size_t)3 * h->nd * h->ne_pad * h->real_size;
+    const size_t state_bytes = (size_t)3 * h->nd * h->ne_pad * sizeof(double);  // FP64 states in both precisions
     h->Q.assign(h->ns + 1, nullptr);
     h->SOL.assign(h->ns, nullptr);
     for (int s = 0; s <= h->ns; ++s) {
@@ -1019,7 +1011,7 @@ int32_t dgsw_rkdg_info(dgsw_handle h, dgsw_info* o) {
     o->precision = h->cfg.precision;
     o->tile = h->tile;
     o->device_bytes = h->device_bytes;
-    o->state_bytes = (int64_t)3 * h->nd * h->ne_pad * h->real_size;
+    o->state_bytes = (int64_t)3 * h->nd * h->ne_pad * (int64_t)sizeof(double);
     return DGSW_OK;
 }
 
@@ -1082,10 +1074,8 @@ int32_t dgsw_rkdg_indicator_features(dgsw_handle h, float* d_features, uint8_t* 
     if (!h || !d_features) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     if (h->cfg.p != 1) return fail(DGSW_ERR_UNSUPPORTED, "the troubled-cell indicator is defined for p = 1");
     cudaSetDevice(h->device);
-    cudaError_t e = h->fp32 ? launch_indicator_features<float>(feature_args<float>(h, h->stage), h->ref_of_dev.p,
-                                                               d_features, d_ok, h->stream)
-                            : launch_indicator_features<double>(feature_args<double>(h, h->stage), h->ref_of_dev.p,
-                                                                d_features, d_ok, h->stream);
+    cudaError_t e = launch_indicator_features<double>(feature_args<double>(h, h->stage), h->ref_of_dev.p, d_features,
+                                                      d_ok, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("indicator features: ") + cudaGetErrorString(e));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return DGSW_OK;
@@ -1160,12 +1150,8 @@ int32_t dgsw_rkdg_indicator_stats(dgsw_handle h, int64_t* counts, int32_t reset)
 int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
     if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
-    cudaError_t e = h->fp32 ? launch_permute_in<float, float>((const float*)d_q, (float*)h->Q[h->stage],
-                                                              h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
-                                                              h->stream)
-                            : launch_permute_in<double, double>((const double*)d_q, (double*)h->Q[h->stage],
-                                                                h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
-                                                                h->stream);
+    cudaError_t e = launch_permute_in<double, double>((const double*)d_q, (double*)h->Q[h->stage], h->ref_of_dev.p,
+                                                      (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("set_state_device: ") + cudaGetErrorString(e));
     return DGSW_OK;
 }
@@ -1173,12 +1159,8 @@ int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
 int32_t dgsw_rkdg_get_state_device(dgsw_handle h, void* d_q) {
     if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
-    cudaError_t e = h->fp32 ? launch_permute_out<float, float>((const float*)h->Q[h->stage], (float*)d_q,
-                                                               h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad, 3 * h->nd,
-                                                               h->stream)
-                            : launch_permute_out<double, double>((const double*)h->Q[h->stage], (double*)d_q,
-                                                                 h->ref_of_dev.p, (int)h->ne, (int)h->ne_pad,
-                                                                 3 * h->nd, h->stream);
+    cudaError_t e = launch_permute_out<double, double>((const double*)h->Q[h->stage], (double*)d_q, h->ref_of_dev.p,
+                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("get_state_device: ") + cudaGetErrorString(e));
     return DGSW_OK;
 }

@@ -272,7 +272,9 @@ DGSW_HD void dgsw_sincos(double a, double* s, double* c) {
 #endif
 }
 DGSW_HD void dgsw_sincos(float a, float* s, float* c) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && defined(DGSW_ACCURATE_SINCOS)
+    sincosf(a, s, c);
+#elif defined(__CUDA_ARCH__)
     // FP32 bulk path: reduce to [-pi, pi] with a two-term Cody-Waite split of 2 pi (6.28125 is exact in
     // FP32 with a short mantissa, so n * 6.28125 is exact for the small n met here), then the hardware
     // sine/cosine, whose absolute error there is a few 1e-7 - below the FP32 state's own rounding

@@ -28,7 +28,7 @@ struct L2Rule {
 
 template <typename Real>
 struct ReduceArgs {
-    const Real* q;
+    const double* q;   // FP64 state (both precisions)
     const Real* bath;
     const int* enodes;
     const double2* xy;

@@ -54,16 +54,18 @@ struct DevClock {
     long long step;
 };
 
+// Real is the arithmetic type of the stage (FP32 bulk or FP64); the stage states and stored stage
+// solutions are FP64 in both, so that the RK update does not accumulate FP32 rounding from stage to stage
 template <typename Real>
 struct StageArgs {
-    const Real* qk[DGSW_RK_MAX_STAGES];  // stage states used by this stage's combination, q_s last
-    const Real* solk[DGSW_RK_MAX_STAGES];
+    const double* qk[DGSW_RK_MAX_STAGES];  // stage states used by this stage's combination, q_s last
+    const double* solk[DGSW_RK_MAX_STAGES];
     double a[DGSW_RK_MAX_STAGES];
     double bdt[DGSW_RK_MAX_STAGES];
     int nterms;
     int store_sol;  // write sol_s (needed when a later stage uses it)
-    Real* q_out;
-    Real* sol_out;
+    double* q_out;
+    double* sol_out;
     const Real* bath;           // [3][ne_pad] bathymetry modes of the linear part
     const Real* geo;            // [5][ne_pad] J^-1(0,0), J^-1(0,1), J^-1(1,0), J^-1(1,1), |J|
     const int* enodes;          // [3][ne_pad]
@@ -241,22 +243,13 @@ __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double b
         qy[1] = ay - by + cy;
         qy[2] = ay + 2.0 * by;
     }
-    // FP32 state: the depths above carry the storage rounding of ze (about 2^-24 (|z| + |b|)), which the
-    // FP64 threshold 1e6 h_o eps_64 cannot absorb; a flattened dry cell at depth h_o would read as wet
-    // after one round trip through FP32. Widen the threshold to that rounding bound (FP64: unchanged).
-    const double thr_clamp = thr;
-    if (sizeof(Real) == 4) {
-        double m = 0.0;
-        for (int v = 0; v < 3; ++v) m = fmax(m, fabs(z[v]) + fabs(bv[v]));
-        thr = fmax(thr, m * (8.0 * 1.1920928955078125e-07));
-    }
     int ndry = 0;
     for (int v = 0; v < 3; ++v) {
         h[v] = z[v] + bv[v];
         if (h[v] <= h_o + thr) ++ndry;
     }
     double h_avg = (0.0 + h[0] + h[1] + h[2]) / 3;
-    if (h_avg <= thr_clamp) h_avg = thr_clamp;
+    if (h_avg <= thr) h_avg = thr;
     bool reproject = false, check = false;
     if (ndry == 0) {
         if (wet) return true;
@@ -382,7 +375,7 @@ struct Smem {
     static constexpr int NFC = (WD ? 2 : 1) * 3 * NG;  // flux components stored per edge
     static __host__ __device__ size_t al(size_t b) { return (b + 15) & ~size_t(15); }
     static __host__ __device__ int nslot(int tile, int mh) { return 3 * tile + mh; }
-    static __host__ __device__ size_t off_tr(int tile) { return al(sizeof(Real) * (size_t)3 * ND * tile); }
+    static __host__ __device__ size_t off_tr(int) { return 0; }
     static __host__ __device__ size_t off_F(int tile, int mh) {
         return off_tr(tile) + al(sizeof(Real) * (size_t)NTC * nslot(tile, mh));
     }
@@ -397,8 +390,11 @@ struct Smem {
     }
     // halo staging: the state and bathymetry modes of each halo face's element, copied asynchronously
     static __host__ __device__ size_t off_halo(int tile, int mh, int me) { return off_flag(tile, mh, me) + al((size_t)me); }
+    static __host__ __device__ size_t off_hbath(int tile, int mh, int me) {
+        return off_halo(tile, mh, me) + al(sizeof(double) * (size_t)3 * ND * mh);
+    }
     static __host__ __device__ size_t bytes(int tile, int mh, int me) {
-        return off_halo(tile, mh, me) + al(sizeof(Real) * (size_t)(3 * ND + 3) * mh);
+        return off_hbath(tile, mh, me) + al(sizeof(Real) * (size_t)3 * mh);
     }
 };
 
@@ -443,13 +439,13 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     using SM = Smem<P, Real, WD>;
     const int NS = SM::nslot(TILE, max_halo);  // trace slots: 3 per tile element, then halo faces
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real* sq = reinterpret_cast<Real*>(smem_raw);                                   // [3*ND][TILE]
     Real* str = reinterpret_cast<Real*>(smem_raw + SM::off_tr(TILE));               // [4*NG][NS]
     Real* sF = reinterpret_cast<Real*>(smem_raw + SM::off_F(TILE, max_halo));       // [NFC][max_edges]
     Real* ssJ = reinterpret_cast<Real*>(smem_raw + SM::off_sJ(TILE, max_halo, max_edges));
     unsigned char* swet = smem_raw + SM::off_wet(TILE, max_halo, max_edges);        // [NS]
     unsigned char* sflag = smem_raw + SM::off_flag(TILE, max_halo, max_edges);      // [max_edges]
-    Real* shq = reinterpret_cast<Real*>(smem_raw + SM::off_halo(TILE, max_halo, max_edges));  // [3*ND+3][max_halo]
+    double* shq = reinterpret_cast<double*>(smem_raw + SM::off_halo(TILE, max_halo, max_edges));  // [3*ND][max_halo]
+    Real* shb = reinterpret_cast<Real*>(smem_raw + SM::off_hbath(TILE, max_halo, max_edges));      // [3][max_halo]
 
     const int tile = blockIdx.x;
     const int e0 = tile * TILE;
@@ -460,7 +456,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     const int P_ = A.ne_pad;
     const double t_stage = A.clock->t + A.drk_s;  // ESSPRKStepper::GetTimeAtCurrentStage
     const Real g = (Real)A.g;
-    const Real* __restrict__ qs = A.qk[A.nterms - 1];  // this stage's state
+    const double* __restrict__ qs = A.qk[A.nterms - 1];  // this stage's state
     const dgsw_fn_time FT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
     // FP32 only: in FP64 the inlined double sine/cosine raise register pressure more than the call costs
     const bool sine_set = FSRC && sizeof(Real) == 4 && A.fn_set == DGSW_FN_MANUFACTURED_SINE;
@@ -485,9 +481,9 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     bool hwet = false;
     auto issue_halo_copies = [&]() {
 #pragma unroll
-        for (int c = 0; c < 3 * ND; ++c) cp_async_value<Real>(&shq[c * max_halo + tid], &qs[c * P_ + hrec.x]);
+        for (int c = 0; c < 3 * ND; ++c) cp_async_value<double>(&shq[c * max_halo + tid], &qs[c * P_ + hrec.x]);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) cp_async_value<Real>(&shq[(3 * ND + k) * max_halo + tid], &A.bath[k * P_ + hrec.x]);
+        for (int k = 0; k < 3; ++k) cp_async_value<Real>(&shb[k * max_halo + tid], &A.bath[k * P_ + hrec.x]);
         hwet = A.wet_in[hrec.x] != 0;
     };
 
@@ -495,11 +491,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     if (active) {
         Real q[3][ND], b[3];
 #pragma unroll
-        for (int c = 0; c < 3 * ND; ++c) {
-            const Real val = qs[c * P_ + d];
-            q[c / ND][c % ND] = val;
-            sq[c * TILE + tid] = val;
-        }
+        for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)qs[c * P_ + d];
         if (CAPPED && hrec.y >= 0) issue_halo_copies();
 #pragma unroll
         for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + d];
@@ -633,9 +625,9 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             cp_async_commit_and_wait();  // this thread's own copies
             Real q[3][ND], b[3], t[4][NG];
 #pragma unroll
-            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = shq[c * max_halo + h];
+            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)shq[c * max_halo + h];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) b[k] = shq[(3 * ND + k) * max_halo + h];
+            for (int k = 0; k < 3; ++k) b[k] = shb[k * max_halo + h];
             if (hrec.y == 0)
                 face_trace<P, 0, Real>(q, b, t);
             else if (hrec.y == 1)
@@ -656,7 +648,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             const int e = it.x;
             Real q[3][ND], b[3], t[4][NG];
 #pragma unroll
-            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = qs[c * P_ + e];
+            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)qs[c * P_ + e];
 #pragma unroll
             for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + e];
             if (it.y == 0)
@@ -761,26 +753,27 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
 
     // ---------------- phase 3: edge contributions, M^-1, RK combination, wet/dry ----------------
     if (!active) return;
-    // the earlier stages' terms of the RK combination, sum_j a_j q_j + dt b_j sol_j: all loads of one
-    // term are issued together here so that their latency overlaps the edge gather below (one
-    // dependent load per value at the end of the CTA cost a global-memory latency per value, per wave)
-    Real comb[3][ND];
+    // the RK combination's state terms, sum_j a_j q_j + dt b_j sol_j over the earlier stages plus
+    // a_s q_s, in FP64: all loads of one term are issued together here so that their latency overlaps
+    // the edge gather below (one dependent load per value at the end of the CTA cost a global-memory
+    // latency per value, per wave)
+    double comb[3][ND];
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
-        for (int k = 0; k < ND; ++k) comb[v][k] = Real(0);
-    for (int j = 0; j < A.nterms - 1; ++j) {
-        const Real* __restrict__ qj = A.qk[j];
-        const Real aj = (Real)A.a[j];
-        Real t[3][ND];
+        for (int k = 0; k < ND; ++k) comb[v][k] = 0.0;
+    for (int j = 0; j < A.nterms; ++j) {
+        const double* __restrict__ qj = A.qk[j];
+        const double aj = A.a[j];
+        double t[3][ND];
 #pragma unroll
         for (int v = 0; v < 3; ++v)
 #pragma unroll
             for (int k = 0; k < ND; ++k) t[v][k] = qj[(v * ND + k) * P_ + d];
-        if (A.bdt[j] != 0.0) {
-            const Real* __restrict__ sj = A.solk[j];
-            const Real bj = (Real)A.bdt[j];
-            Real u[3][ND];
+        if (j < A.nterms - 1 && A.bdt[j] != 0.0) {
+            const double* __restrict__ sj = A.solk[j];
+            const double bj = A.bdt[j];
+            double u[3][ND];
 #pragma unroll
             for (int v = 0; v < 3; ++v)
 #pragma unroll
@@ -843,26 +836,24 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     }
     // M^-1 (diagonal master mass inverse over |J|) and the SSP-RK stage combination
     const Real iaJ = Real(1) / aJ;
-    Real qn[3][ND];
+    const double bdt_s = A.bdt[A.nterms - 1];
+    double qn[3][ND];
     sfor<0, ND>([&](auto K) {
         constexpr int k = decltype(K)::value;
         const Real mk = (Real)MT<P>::minv(k) * iaJ;
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
-            const Real sol = rhs[v][k] * mk;
+            const double sol = (double)(rhs[v][k] * mk);
             const int idx = (v * ND + k) * P_ + d;
             if (A.store_sol) A.sol_out[idx] = sol;
-            Real acc = comb[v][k];
-            const int j = A.nterms - 1;
-            acc += (Real)A.a[j] * sq[(v * ND + k) * TILE + tid] + (Real)A.bdt[j] * sol;
-            qn[v][k] = acc;
+            qn[v][k] = comb[v][k] + bdt_s * sol;
         }
     });
     bool wet_new = wet;
     if (WD) {
         const double bv[3] = {A.nz[A.enodes[d]], A.nz[A.enodes[P_ + d]], A.nz[A.enodes[2 * P_ + d]]};
         const double bmin = fmin(bv[0], fmin(bv[1], bv[2]));
-        wet_new = wetting_drying<ND, Real>(qn, bv, bmin, A.h_o, A.h_o_thr, wet);
+        wet_new = wetting_drying<ND, double>(qn, bv, bmin, A.h_o, A.h_o_thr, wet);
     }
     bool has_nan = false;
 #pragma unroll

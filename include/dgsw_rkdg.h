@@ -61,7 +61,8 @@ typedef struct {
     int32_t spherical;         /* problem.spherical_projection present */
     double sp_lat0_deg, sp_R;  /* spherical_projection.{latitude_o, R} */
     /* execution options (no reference counterpart) */
-    int32_t precision;         /* dgsw_precision: FP64, or FP32 bulk with FP64 wet/dry tests and reductions */
+    int32_t precision;         /* dgsw_precision: FP64, or FP32 bulk arithmetic (volume, edge and source
+                                  integrals) with FP64 stage states, wet/dry tests, limiter and reductions */
     int32_t device;            /* CUDA device ordinal */
     int32_t tile;              /* elements per stage-kernel tile: 128 or 256; 0 = by order (256 at p = 1,
                                   128 at p = 2); DGSW_TILE_AUTOTUNE = measure both on the device at
@@ -138,8 +139,8 @@ int32_t dgsw_rkdg_set_state(dgsw_handle h, const double* q);
 int32_t dgsw_rkdg_get_state(dgsw_handle h, double* q);
 int32_t dgsw_rkdg_set_wet(dgsw_handle h, const uint8_t* wet);
 int32_t dgsw_rkdg_get_wet(dgsw_handle h, uint8_t* wet);
-/* the same on device buffers of the library's device (layout [elem][var][dof], precision of the handle:
- * double for FP64, float for FP32); ordered on the handle's stream */
+/* the same on device buffers of the library's device (layout [elem][var][dof], FP64 in both precisions:
+ * the FP32 path computes in FP32 but keeps its stage states in FP64); ordered on the handle's stream */
 int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q);
 int32_t dgsw_rkdg_get_state_device(dgsw_handle h, void* d_q);
 
@@ -165,7 +166,7 @@ int32_t dgsw_rkdg_mass(dgsw_handle h, double* out);
  * device array of 32 KiB per device, so n_elems is limited to DGSW_L2_STATIC_MAX_ELEMS (larger inputs
  * are rejected with DGSW_ERR_INVALID_ARGUMENT; dgsw_rkdg_l2_error has no such limit).
  * Same value as dgsw_rkdg_l2_error up to summation order. Inputs, all on the current device:
- * d_q [n_elems][3][ndof] FP64 (the layout dgsw_rkdg_get_state_device writes for an FP64 handle),
+ * d_q [n_elems][3][ndof] FP64 (the layout dgsw_rkdg_get_state_device writes),
  * d_elem_nodes [n_elems][3] 0-based node indices, d_node_xyz [n_nodes][3] (x, y, depth);
  * function_set / fn_params (16 values, NULL = zeros) / t select true_q. Work is queued on `stream`
  * (NULL = default stream) and the call returns after it completes, with the result in *out (host).
