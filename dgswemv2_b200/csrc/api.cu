@@ -118,6 +118,7 @@ struct dgsw_rkdg_s {
     DBuf<unsigned char> limited;
     DBuf<int> nbr;     // neighbours per face, device order (limiter)
     DBuf<double> baryctr;  // barycentre values of the newest state (limiter)
+    DBuf<double> lgeo;     // limiter geometry per element, [16][ne_pad]
     int64_t device_bytes = 0;
     // stepper mirror on the host (ESSPRKStepper state)
     double t = 0.0;
@@ -246,6 +247,7 @@ cudaError_t launch_limiter(dgsw_rkdg_s* h, int s_out) {
     L.nu = h->cfg.sl_nu;
     L.status = h->status.p;
     L.ref_of_dev = h->ref_of_dev.p;
+    L.lgeo = h->lgeo.p;
     if (h->ind_mode == 1) {
         L.list = h->ind_list.p;
         L.list_count = h->ind_count.p;
@@ -717,6 +719,21 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         }
         h->device_bytes += en.size() * 4 + nb.size() * 4 + h->nn * 24 + nedges * 16 + h->ne * 12 + 3 * h->ne_pad;
     }
+    if (cfg->slope_limiting) {
+        // the limiter's geometry, once (the same device code the limiter would run per stage)
+        if ((e = h->lgeo.alloc((size_t)LIM_GEO * h->ne_pad)) != cudaSuccess) return cleanup_fail("alloc", e);
+        h->device_bytes += (int64_t)LIM_GEO * h->ne_pad * 8;
+        LimiterArgs<double> L;
+        std::memset(&L, 0, sizeof(L));
+        L.nbr = h->nbr.p;
+        L.enodes = h->enodes.p;
+        L.xy = h->xy.p;
+        L.nz = h->nz.p;
+        L.ne = (int)h->ne;
+        L.ne_pad = (int)h->ne_pad;
+        limiter_geometry_kernel<double><<<(unsigned)((h->ne + 255) / 256), 256, 0, h->stream>>>(L, h->lgeo.p);
+        if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cleanup_fail("limiter geometry", e);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return cleanup_fail("setup", e);
     *out = h;
     return DGSW_OK;
@@ -981,6 +998,7 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     h->limited.release();
     h->nbr.release();
     h->baryctr.release();
+    h->lgeo.release();
     h->ind_params.release();
     h->ind_list.release();
     h->ind_count.release();

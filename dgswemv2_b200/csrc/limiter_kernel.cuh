@@ -35,7 +35,72 @@ struct LimiterArgs {
     const int* list_count;
     const unsigned char* gate;       // write back only where gate[e] != 0 (NULL: everywhere)
     unsigned long long* counters;    // [IND_LIMITED], [IND_MISSED] accumulators (NULL: none)
+    const double* lgeo;              // precomputed limiter geometry [16][ne_pad] (NULL: computed here)
 };
+
+// Limiter geometry of element e (swe_pre_init_data.hpp:252-326): per median b (from the centroid to the
+// midpoint of edge b) the coefficients alpha of the median in the basis of the centroid-to-neighbour-
+// centroid vectors of faces b and b+1 (a boundary face mirrors the centroid across the edge), the unit
+// median direction and its squared length; then the bathymetry at the barycentre.
+// G = {al0, al1, nx, ny, r^2} x 3 medians, zb
+constexpr int LIM_GEO = 16;
+
+template <typename Real>
+__device__ __forceinline__ void limiter_geometry(const LimiterArgs<Real>& L, int e, const int (&nb)[3],
+                                                 double (&G)[LIM_GEO]) {
+    const size_t P = (size_t)L.ne_pad;
+    const int n0 = L.enodes[e], n1 = L.enodes[P + e], n2 = L.enodes[2 * P + e];
+    const double2 X0 = L.xy[n0], X1 = L.xy[n1], X2 = L.xy[n2];
+    const double X[3][2] = {{X0.x, X0.y}, {X1.x, X1.y}, {X2.x, X2.y}};
+    const double cx = (X[0][0] + X[1][0] + X[2][0]) / 3.0, cy = (X[0][1] + X[1][1] + X[2][1]) / 3.0;
+    double mid[3][2], nbc[3][2];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        mid[b][0] = (X[(b + 1) % 3][0] + X[(b + 2) % 3][0]) / 2.0;
+        mid[b][1] = (X[(b + 1) % 3][1] + X[(b + 2) % 3][1]) / 2.0;
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        if (nb[f] >= 0) {
+            const int m = nb[f];
+            const double2 Y0 = L.xy[L.enodes[m]], Y1 = L.xy[L.enodes[P + m]], Y2 = L.xy[L.enodes[2 * P + m]];
+            nbc[f][0] = (Y0.x + Y1.x + Y2.x) / 3.0;
+            nbc[f][1] = (Y0.y + Y1.y + Y2.y) / 3.0;
+        } else {
+            nbc[f][0] = 2.0 * mid[f][0] - cx;
+            nbc[f][1] = 2.0 * mid[f][1] - cy;
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const int e1 = b, e2 = (b + 1) % 3;
+        const double bx = mid[b][0] - cx, by = mid[b][1] - cy;
+        const double nrm = sqrt(bx * bx + by * by);
+        const double A00 = nbc[e1][0] - cx, A10 = nbc[e1][1] - cy, A01 = nbc[e2][0] - cx, A11 = nbc[e2][1] - cy;
+        const double idet = 1.0 / (A00 * A11 - A10 * A01);
+        G[5 * b] = (A11 * idet) * bx + (-A01 * idet) * by;
+        G[5 * b + 1] = (-A10 * idet) * bx + (A00 * idet) * by;
+        G[5 * b + 2] = bx / nrm;
+        G[5 * b + 3] = by / nrm;
+        G[5 * b + 4] = bx * bx + by * by;
+    }
+    G[15] = L.nz[n0] * (1.0 / 3.0) + L.nz[n1] * (1.0 / 3.0) + L.nz[n2] * (1.0 / 3.0);
+}
+
+// once per handle: the geometry of every element into lgeo [LIM_GEO][ne_pad]
+template <typename Real>
+__global__ void __launch_bounds__(256) limiter_geometry_kernel(const LimiterArgs<Real> L, double* __restrict__ lgeo) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= L.ne) return;
+    const size_t P = (size_t)L.ne_pad;
+    int nb[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) nb[f] = L.nbr[f * P + e];
+    double G[LIM_GEO];
+    limiter_geometry(L, e, nb, G);
+#pragma unroll
+    for (int i = 0; i < LIM_GEO; ++i) lgeo[i * P + e] = G[i];
+}
 
 // the limiter decision for element e (1 if its state changes); the new state is written only if `write`
 template <int ND, typename Real>
@@ -72,35 +137,20 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
         qm[v][1] = ql[v][0] * 0.5 + ql[v][2] * 0.5;
         qm[v][2] = ql[v][0] * 0.5 + ql[v][1] * 0.5;
     }
-    // geometry
-    const int n0 = L.enodes[e], n1 = L.enodes[P + e], n2 = L.enodes[2 * P + e];
-    const double2 X0 = L.xy[n0], X1 = L.xy[n1], X2 = L.xy[n2];
-    const double X[3][2] = {{X0.x, X0.y}, {X1.x, X1.y}, {X2.x, X2.y}};
-    const double cx = (X[0][0] + X[1][0] + X[2][0]) / 3.0, cy = (X[0][1] + X[1][1] + X[2][1]) / 3.0;
-    double mid[3][2], nbc[3][2], qnb[3][3];
+    // limiter geometry (precomputed once per handle by limiter_geometry_kernel, or built here)
+    double G[LIM_GEO];
+    if (L.lgeo) {
 #pragma unroll
-    for (int b = 0; b < 3; ++b) {
-        mid[b][0] = (X[(b + 1) % 3][0] + X[(b + 2) % 3][0]) / 2.0;
-        mid[b][1] = (X[(b + 1) % 3][1] + X[(b + 2) % 3][1]) / 2.0;
+        for (int i = 0; i < LIM_GEO; ++i) G[i] = L.lgeo[i * P + e];
+    } else {
+        limiter_geometry(L, e, nb, G);
     }
+    double qnb[3][3];
 #pragma unroll
-    for (int f = 0; f < 3; ++f) {
-        if (nb[f] >= 0) {
-            const int m = nb[f];
-            const double2 Y0 = L.xy[L.enodes[m]], Y1 = L.xy[L.enodes[P + m]], Y2 = L.xy[L.enodes[2 * P + m]];
-            nbc[f][0] = (Y0.x + Y1.x + Y2.x) / 3.0;
-            nbc[f][1] = (Y0.y + Y1.y + Y2.y) / 3.0;
+    for (int f = 0; f < 3; ++f)
 #pragma unroll
-            for (int v = 0; v < 3; ++v) qnb[f][v] = L.baryctr[v * P + m];
-        } else {
-            // mirrored centroid across the boundary edge, own barycentre state
-            nbc[f][0] = 2.0 * mid[f][0] - cx;
-            nbc[f][1] = 2.0 * mid[f][1] - cy;
-#pragma unroll
-            for (int v = 0; v < 3; ++v) qnb[f][v] = qb[v];
-        }
-    }
-    const double zb = L.nz[n0] * (1.0 / 3.0) + L.nz[n1] * (1.0 / 3.0) + L.nz[n2] * (1.0 / 3.0);
+        for (int v = 0; v < 3; ++v) qnb[f][v] = nb[f] >= 0 ? L.baryctr[v * P + nb[f]] : qb[v];
+    const double zb = G[15];
     const double h = qb[0] + zb;
     const double u = qb[1] / h, vv = qb[2] / h;
     const double c = sqrt(L.g * h);
@@ -108,14 +158,7 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
         const int e1 = b, e2 = (b + 1) % 3;
-        const double bx = mid[b][0] - cx, by = mid[b][1] - cy;
-        const double nrm = sqrt(bx * bx + by * by);
-        const double nx = bx / nrm, ny = by / nrm;  // normalised median
-        const double A00 = nbc[e1][0] - cx, A10 = nbc[e1][1] - cy, A01 = nbc[e2][0] - cx, A11 = nbc[e2][1] - cy;
-        const double idet = 1.0 / (A00 * A11 - A10 * A01);
-        const double al0 = (A11 * idet) * bx + (-A01 * idet) * by;
-        const double al1 = (-A10 * idet) * bx + (A00 * idet) * by;
-        const double rsq = bx * bx + by * by;
+        const double al0 = G[5 * b], al1 = G[5 * b + 1], nx = G[5 * b + 2], ny = G[5 * b + 3], rsq = G[5 * b + 4];
         const double un = u * nx + vv * ny;
         const double iR[3][3] = {{(c + un) / (2 * c), -nx / (2 * c), -ny / (2 * c)},
                                  {u * ny - vv * nx, -ny, nx},
