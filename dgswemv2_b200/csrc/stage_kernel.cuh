@@ -416,9 +416,12 @@ __device__ __forceinline__ void cp_async_commit_and_wait() {
 #ifndef DGSW_F32_MB128
 #define DGSW_F32_MB128 4
 #endif
+#ifndef DGSW_F64_MB128
+#define DGSW_F64_MB128 3
+#endif
 template <int P, typename Real, int TILE>
 struct MinBlocks {
-    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? DGSW_F32_MB128 : 2) : (TILE == 128 ? 2 : 1);
+    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? DGSW_F32_MB128 : 2) : (TILE == 128 ? DGSW_F64_MB128 : 1);
 };
 
 // shared-memory capacities a tile almost always fits (measured: about 0.27 TILE halo faces and 1.65 TILE
@@ -427,7 +430,7 @@ struct MinBlocks {
 template <int TILE>
 struct TileCap {
     static constexpr int halo = TILE / 2;
-    static constexpr int edges = 2 * TILE;
+    static constexpr int edges = TILE + TILE / 2 + TILE / 4 + 16;  // 240 for 128, 464 for 256
 };
 
 template <int P, typename Real, bool WD, bool FSRC, int TILE, bool CAPPED>
@@ -599,10 +602,8 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                     });
                 });
             }
-#pragma unroll
-            for (int v = 0; v < 3; ++v)
-#pragma unroll
-                for (int k = 0; k < ND; ++k) rhs[v][k] *= aJ;
+            // the volume integrals stay in master-element units: sol = (|J| V + E) M^-1 / |J| is
+            // computed as V M^-1 + (E / |J|) M^-1, with 1 / |J| folded into the edge weights below
         }
         // traces of the three faces (needed also when dry: a wet neighbour evaluates the interface)
         sfor<0, 3>([&](auto FF) {
@@ -788,6 +789,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
 #pragma unroll
             for (int k = 0; k < ND; ++k) comb[v][k] += aj * t[v][k];
     }
+    const Real iaJ = Real(1) / aJ;
     const int roles = es.y & 7;
     const int ord = es.y >> 3;
     const int cnt = ord & 3;
@@ -797,7 +799,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
         const int slot = (es.x >> (10 * f)) & 1023;
         if (!sflag[slot]) continue;
         const bool is_in = (roles >> f) & 1;
-        const Real sJ = ssJ[slot];
+        const Real sJe = ssJ[slot] * iaJ;  // edge half length over |J|
         Real F[3][NG];
 #pragma unroll
         for (int gp = 0; gp < NG; ++gp) {  // own Gauss point order
@@ -815,14 +817,16 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             constexpr int fc = decltype(FF)::value;
             sfor<0, NG>([&](auto GP) {
                 constexpr int gp = decltype(GP)::value;
-                const Real wsJ = (Real)MT<P>::gw(gp) * sJ;
+                const Real wsJ = (Real)MT<P>::gw(gp) * sJe;
+                Real T[3];
+#pragma unroll
+                for (int v = 0; v < 3; ++v) T[v] = F[v][gp] * wsJ;
                 sfor<0, ND>([&](auto K) {
                     constexpr int k = decltype(K)::value;
                     constexpr double c = MT<P>::fphi((fc * ND + k) * NG + gp);
                     if constexpr (c != 0.0) {
-                        const Real ph = (Real)c * wsJ;
 #pragma unroll
-                        for (int v = 0; v < 3; ++v) rhs[v][k] -= F[v][gp] * ph;
+                        for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * (Real)c;
                     }
                 });
             });
@@ -834,13 +838,12 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
         else
             contrib(IC<2>{});
     }
-    // M^-1 (diagonal master mass inverse over |J|) and the SSP-RK stage combination
-    const Real iaJ = Real(1) / aJ;
+    // M^-1 (the diagonal master mass inverse; 1 / |J| is already in) and the SSP-RK stage combination
     const double bdt_s = A.bdt[A.nterms - 1];
     double qn[3][ND];
     sfor<0, ND>([&](auto K) {
         constexpr int k = decltype(K)::value;
-        const Real mk = (Real)MT<P>::minv(k) * iaJ;
+        const Real mk = (Real)MT<P>::minv(k);
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
             const double sol = (double)(rhs[v][k] * mk);
