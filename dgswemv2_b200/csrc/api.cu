@@ -565,7 +565,7 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
     if (cfg->wetting_drying) h->h_o_thr = 1.0e6 * cfg->h_o * std::numeric_limits<double>::epsilon();
     h->node_xyz.assign(mesh->node_xyz, mesh->node_xyz + 3 * mesh->n_nodes);
     int tile = cfg->tile;
-    if (tile == 0) tile = (cfg->p == 1) ? 256 : 128;
+    if (tile == 0) tile = 128;  // measured faster than 256 at p = 1 and p = 2 in both precisions
     if (tile != 128 && tile != 256) {
         delete h;
         return fail(DGSW_ERR_INVALID_ARGUMENT, "tile must be 0 (automatic), 128 or 256");

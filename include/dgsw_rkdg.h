@@ -64,9 +64,9 @@ typedef struct {
     int32_t precision;         /* dgsw_precision: FP64, or FP32 bulk arithmetic (volume, edge and source
                                   integrals) with FP64 stage states, wet/dry tests, limiter and reductions */
     int32_t device;            /* CUDA device ordinal */
-    int32_t tile;              /* elements per stage-kernel tile: 128 or 256; 0 = by order (256 at p = 1,
-                                  128 at p = 2); DGSW_TILE_AUTOTUNE = measure both on the device at
-                                  create and keep the faster (dgsw_rkdg_tuning reports the timings) */
+    int32_t tile;              /* elements per stage-kernel tile: 128 or 256; 0 = 128; DGSW_TILE_AUTOTUNE =
+                                  measure both on the device at create and keep the faster
+                                  (dgsw_rkdg_tuning reports the timings) */
     int32_t renumber;          /* 0 keep input order, 1 Morton order of element centroids (default 1) */
     int32_t use_graphs;        /* capture each RK step in a CUDA graph (default 1) */
     int32_t reserved[8];
