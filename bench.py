@@ -256,6 +256,35 @@ def time_steps(P, K):
     return ms, launches, wall
 
 
+def limiter_workload(dev, steps=400, warmup=5):
+    """The metric's "FP32 + MLP vs FP64 plain" on the limited workload it concerns: config 3 (Thacker bowl,
+    131,072 triangles, p = 1, wetting/drying + Cockburn-Shu limiter). FP32 bulk with the learned
+    indicator gating the limiter (confidence 0.9, committed weights) against the FP64 path with the
+    plain limiter, plus FP32 with the plain limiter; device time of graph-replayed steps, L2 error
+    against the analytic solution after the same number of steps."""
+    from dgswemv2_b200 import Problem, configs, indicator
+
+    W = indicator.load_weights()
+    out = {"workload": "config 3: Thacker bowl, 131072 triangles, p=1, SSP-RK2, wetting/drying + limiter",
+           "steps": steps + warmup}
+    for name, prec, mode in (("fp32_mlp", "fp32", 1), ("fp32_plain", "fp32", 0), ("fp64_plain", "fp64", 0)):
+        mesh, cfg = configs.config3(precision=prec)
+        P = Problem(cfg, mesh, device=dev)
+        if mode:
+            P.set_indicator(W, confidence=0.9, mode=mode)
+        P.step_serial(warmup)
+        ms, _, _ = time_steps(P, steps)
+        units = P.ne * P.nd * cfg.rk_nstages * steps
+        out[name] = {"value": units / (ms / 1e3), "ms_per_step": ms / steps, "l2_error": P.compute_residual_L2()}
+        if mode:
+            c = P.indicator_stats()
+            out[name]["sent_fraction"] = c[1] / max(1, c[0])
+        del P
+    out["speedup_fp32_mlp_over_fp64_plain"] = out["fp32_mlp"]["value"] / out["fp64_plain"]["value"]
+    out["l2_ratio_fp32_mlp_over_fp64_plain"] = out["fp32_mlp"]["l2_error"] / out["fp64_plain"]["l2_error"]
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -341,6 +370,9 @@ def run_ours(args):
     if fp64:
         out["fp64_plain"] = fp64
         out["speedup_fp32_over_fp64"] = value / fp64["value"]
+    if args.precision == "fp32":
+        out["limiter_workload"] = limiter_workload(dev)
+        barrier(world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(args.nq, args.cpu_seconds, args.precision)
