@@ -217,6 +217,17 @@ class Problem:
         _lib.check(_lib.load().dgsw_rkdg_indicator_stats(self._h, c, int(reset)))
         return tuple(int(v) for v in c)
 
+    def set_trouble(self, enable=True):
+        """Evaluate the reference's (unused) KXRCF trouble indicator in every limiter pass."""
+        _lib.check(_lib.load().dgsw_rkdg_set_trouble(self._h, int(enable)))
+
+    def get_trouble(self):
+        """(I [ne], troubled flags [ne]) of the last limiter pass, ascending element ID."""
+        I = np.empty(self.ne, np.float64)
+        t = np.empty(self.ne, np.uint8)
+        _lib.check(_lib.load().dgsw_rkdg_get_trouble(self._h, _lib.ptr(I, C.c_double), _lib.ptr(t, C.c_uint8)))
+        return I, t
+
     def set_state_device(self, dptr):
         _lib.check(_lib.load().dgsw_rkdg_set_state_device(self._h, C.c_void_p(dptr)))
 

@@ -131,6 +131,8 @@ SIGNATURES = {
                                        C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int32)]),
     "dgsw_rkdg_get_limited": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "dgsw_rkdg_set_trouble": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "dgsw_rkdg_get_trouble": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint8)]),
     "dgsw_rkdg_indicator_features": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_stage_record": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_set_indicator": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.c_double, C.c_int32]),

@@ -19,6 +19,7 @@
 #include "quadrature.h"
 #include "reduce_kernels.cuh"
 #include "stage_kernel.cuh"
+#include "trouble.cuh"
 
 using namespace dgsw;
 
@@ -119,6 +120,11 @@ struct dgsw_rkdg_s {
     DBuf<int> nbr;     // neighbours per face, device order (limiter)
     DBuf<double> baryctr;  // barycentre values of the newest state (limiter)
     DBuf<double> lgeo;     // limiter geometry per element, [16][ne_pad]
+    // trouble indicator (computed in each limiter pass only when asked for)
+    int trouble_on = 0;
+    DBuf<signed char> nbr_face;  // [3][ne_pad] the neighbour's face across each face
+    DBuf<double> tI;
+    DBuf<unsigned char> tflag, tscratch, tout;
     int64_t device_bytes = 0;
     // stepper mirror on the host (ESSPRKStepper state)
     double t = 0.0;
@@ -333,6 +339,34 @@ cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageR
                                               rec->labels, h->stream);
         if (e != cudaSuccess) return e;
         ++launches;
+    }
+    if (h->cfg.slope_limiting && h->trouble_on) {
+        TroubleArgs<double> T;
+        TroubleArgs<float> Tf;
+        auto fill = [&](auto& X, auto bath) {
+            std::memset(&X, 0, sizeof(X));
+            X.q = (const double*)h->Q[s_out];
+            X.bath = bath;
+            X.wet = h->wet[h->wet_cur].p;
+            X.nbr = h->nbr.p;
+            X.nbr_face = h->nbr_face.p;
+            X.enodes = h->enodes.p;
+            X.xy = h->xy.p;
+            X.ref_of_dev = h->ref_of_dev.p;
+            X.I = h->tI.p;
+            X.flag = h->tflag.p;
+            X.ne = (int)h->ne;
+            X.ne_pad = (int)h->ne_pad;
+        };
+        if (h->fp32) {
+            fill(Tf, (const float*)h->bath);
+            e = launch_trouble<float>(Tf, h->cfg.p, h->tscratch.p, h->tout.p, h->stream);
+        } else {
+            fill(T, (const double*)h->bath);
+            e = launch_trouble<double>(T, h->cfg.p, h->tscratch.p, h->tout.p, h->stream);
+        }
+        if (e != cudaSuccess) return e;
+        launches += 6;
     }
     if (h->cfg.slope_limiting) {
         const int mode = h->ind_mode;
@@ -999,6 +1033,11 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     h->nbr.release();
     h->baryctr.release();
     h->lgeo.release();
+    h->nbr_face.release();
+    h->tI.release();
+    h->tflag.release();
+    h->tscratch.release();
+    h->tout.release();
     h->ind_params.release();
     h->ind_list.release();
     h->ind_count.release();
@@ -1162,6 +1201,50 @@ int32_t dgsw_rkdg_indicator_stats(dgsw_handle h, int64_t* counts, int32_t reset)
         CUDA_TRY(cudaStreamSynchronize(h->stream));
     }
     if (err) return fail(DGSW_ERR_CUDA, "indicator: a tensor-core wait timed out");
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_set_trouble(dgsw_handle h, int32_t enable) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (enable && !h->cfg.slope_limiting)
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "the trouble indicator belongs to the slope limiter, which this "
+                                               "problem does not use");
+    cudaSetDevice(h->device);
+    if (enable && !h->tI.p) {
+        cudaError_t e;
+        std::vector<signed char> nf((size_t)3 * h->ne_pad, -1);
+        for (int64_t d = 0; d < h->ne; ++d) {
+            const int64_t r = h->tiling.ref_of_dev[d];
+            for (int f = 0; f < 3; ++f) nf[(size_t)f * h->ne_pad + d] = h->topo.nbr_face[3 * r + f];
+        }
+        if ((e = h->nbr_face.alloc(nf.size())) != cudaSuccess || (e = h->tI.alloc(h->ne_pad)) != cudaSuccess ||
+            (e = h->tflag.alloc(h->ne_pad)) != cudaSuccess || (e = h->tscratch.alloc(h->ne_pad)) != cudaSuccess ||
+            (e = h->tout.alloc(h->ne_pad)) != cudaSuccess)
+            return fail(DGSW_ERR_CUDA, std::string("trouble buffers: ") + cudaGetErrorString(e));
+        CUDA_TRY(cudaMemcpy(h->nbr_face.p, nf.data(), nf.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemset(h->tI.p, 0, h->ne_pad * sizeof(double)));
+        CUDA_TRY(cudaMemset(h->tout.p, 0, h->ne_pad));
+        h->device_bytes += (int64_t)h->ne_pad * 14;
+    }
+    if ((enable != 0) != (h->trouble_on != 0)) destroy_graphs(h);
+    h->trouble_on = enable != 0;
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_get_trouble(dgsw_handle h, double* I, uint8_t* troubled) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (!h->tI.p) return fail(DGSW_ERR_INVALID_ARGUMENT, "the trouble indicator is not enabled");
+    cudaSetDevice(h->device);
+    std::vector<double> v(h->ne);
+    std::vector<unsigned char> t(h->ne);
+    CUDA_TRY(cudaMemcpyAsync(v.data(), h->tI.p, h->ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(t.data(), h->tout.p, h->ne, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int64_t d = 0; d < h->ne; ++d) {
+        const int64_t r = h->tiling.ref_of_dev[d];
+        if (I) I[r] = v[d];
+        if (troubled) troubled[r] = t[d];
+    }
     return DGSW_OK;
 }
 

@@ -191,6 +191,13 @@ int32_t dgsw_rkdg_topology(dgsw_handle h, int32_t* neighbors, uint8_t* btype, in
 int32_t dgsw_mesh_topology(const dgsw_mesh* mesh, int32_t* neighbors, uint8_t* btype, int64_t* n_interfaces,
                            int32_t* interfaces, int64_t* n_boundaries, int32_t* boundaries);
 
+/* check_trouble (swe_trouble_check.hpp:6-116): the KXRCF-type indicator the reference evaluates in every
+ * limiter pass but does not use. Off by default; once enabled, each limiter pass also computes it on the
+ * state the limiter sees, and dgsw_rkdg_get_trouble returns the last pass's indicator I and troubled
+ * flags (after the five-layer neighbour growth), in ascending element-ID order (either may be NULL). */
+int32_t dgsw_rkdg_set_trouble(dgsw_handle h, int32_t enable);
+int32_t dgsw_rkdg_get_trouble(dgsw_handle h, double* I, uint8_t* troubled);
+
 /* per element 1 if the last slope-limiter pass changed its state (the plain limiter's decision) */
 int32_t dgsw_rkdg_get_limited(dgsw_handle h, uint8_t* flags);
 

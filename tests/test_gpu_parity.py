@@ -148,3 +148,24 @@ def test_fp32_bowl_keeps_the_fp64_wet_set():
     assert np.isfinite(P["fp32"].get_state()).all()
     assert abs(P["fp32"].mass() / m0["fp32"] - 1) <= 1e-7
     assert abs(P["fp64"].mass() / m0["fp64"] - 1) <= 1e-12
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_trouble_indicator_matches_oracle(oracle, p):
+    """check_trouble (swe_trouble_check.hpp:6-116), which the reference computes in every limiter pass
+    without using it: indicator values within 1e-9 relative (1e-12 absolute) and troubled flags equal to
+    the oracle's after the same steps (flags may differ only where I is within 1e-9 of the threshold 1)."""
+    mesh, cfg = configs.bowl_humps(nq=24, seed=5, precision="fp64")
+    cfg.p = p
+    P = Problem(cfg, mesh)
+    P.set_trouble(True)
+    O = oracle.problem(cfg, mesh, n_threads=8)
+    for _ in range(3):
+        P.step_serial(10)
+        O.step(10)
+        Ig, tg = P.get_trouble()
+        Io, to = O.trouble()
+        assert np.allclose(Ig, Io, rtol=1e-9, atol=1e-12), np.max(np.abs(Ig - Io))
+        near = np.abs(Io - 1.0) < 1e-9
+        assert np.array_equal(tg[~near] != 0, to[~near] != 0)
+    assert to.sum() > 0 and (Io > 0).sum() > 0
