@@ -155,17 +155,26 @@ def test_trouble_indicator_matches_oracle(oracle, p):
     """check_trouble (swe_trouble_check.hpp:6-116), which the reference computes in every limiter pass
     without using it: indicator values within 1e-9 relative (1e-12 absolute) and troubled flags equal to
     the oracle's after the same steps (flags may differ only where I is within 1e-9 of the threshold 1)."""
-    mesh, cfg = configs.bowl_humps(nq=24, seed=5, precision="fp64")
-    cfg.p = p
+    # the indicator divides by r^((p+1)/2) in mesh units, so it trips on a unit-size basin (metre-size
+    # meshes never reach I > 1): a Gaussian hump on 1 m of still water in a 1 m x 1 m box
+    from dgswemv2_b200.types import ProblemConfig
+
+    mesh = meshgen.quad_mesh(12, 12, bc=(LAND,) * 4, jitter=0.15, seed=2, bathymetry=meshgen.bath_flat(1.0))
+    cfg = ProblemConfig(p=p, rk_nstages=2, rk_order=2, dt=5e-4, g=9.81, wetting_drying=True, h_o=0.01,
+                        slope_limiting=True, sl_M=1.0e-8, sl_nu=1.5, ic_type=1,
+                        function_set=configs.FN_GAUSSIAN_HUMPS,
+                        fn_params=configs.humps_params([(0.9, 0.5, 0.5, 0.05)]), precision="fp64")
     P = Problem(cfg, mesh)
     P.set_trouble(True)
     O = oracle.problem(cfg, mesh, n_threads=8)
+    seen = 0
     for _ in range(3):
-        P.step_serial(10)
-        O.step(10)
+        P.step_serial(5)
+        O.step(5)
         Ig, tg = P.get_trouble()
         Io, to = O.trouble()
         assert np.allclose(Ig, Io, rtol=1e-9, atol=1e-12), np.max(np.abs(Ig - Io))
         near = np.abs(Io - 1.0) < 1e-9
         assert np.array_equal(tg[~near] != 0, to[~near] != 0)
-    assert to.sum() > 0 and (Io > 0).sum() > 0
+        seen += int(to.sum())
+    assert seen > 0
