@@ -39,6 +39,9 @@ def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True):
     c.spherical = int(cfg.spherical)
     c.sp_lat0_deg = cfg.sp_lat0_deg
     c.sp_R = cfg.sp_R
+    c.bottom_friction = int(getattr(cfg, "bottom_friction", 0))
+    c.friction_cf = float(getattr(cfg, "friction_cf", 0.0))
+    c.ramp_duration = float(getattr(cfg, "ramp_duration", 0.0))
     c.precision = DGSW_FP32 if cfg.precision == "fp32" else DGSW_FP64
     c.device = device
     c.tile = tile
@@ -66,6 +69,17 @@ def _mesh_struct(mesh):
     m.seg_type = _lib.ptr(keep[3], C.c_int32)
     m.seg_offsets = _lib.ptr(keep[4], C.c_int64)
     m.seg_nodes = _lib.ptr(keep[5], C.c_int32)
+    mann = getattr(mesh, "node_manning_n", None)
+    if mann is not None:
+        mann = np.ascontiguousarray(mann, np.float64)
+        if mann.shape != (mesh.n_nodes,):
+            raise ValueError("node_manning_n must hold one value per node")
+        keep.append(mann)
+        m.node_manning_n = _lib.ptr(mann, C.c_double)
+    arr, nf, fkeep = _lib.forcing_blocks(mesh)
+    keep.append(fkeep)
+    m.n_forcing = nf
+    m.forcing = arr
     return m, keep
 
 

@@ -55,12 +55,29 @@ class Config(C.Structure):
         ("spherical", C.c_int32),
         ("sp_lat0_deg", C.c_double),
         ("sp_R", C.c_double),
+        ("bottom_friction", C.c_int32),
+        ("friction_cf", C.c_double),
+        ("ramp_duration", C.c_double),
         ("precision", C.c_int32),
         ("device", C.c_int32),
         ("tile", C.c_int32),
         ("renumber", C.c_int32),
         ("use_graphs", C.c_int32),
         ("reserved", C.c_int32 * 8),
+    ]
+
+
+class ForcingBlock(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("n_nodes", C.c_int32),
+        ("n_constituents", C.c_int32),
+        ("nodes", C.POINTER(C.c_int32)),
+        ("frequency", C.POINTER(C.c_double)),
+        ("forcing_fact", C.POINTER(C.c_double)),
+        ("equilib_arg", C.POINTER(C.c_double)),
+        ("amplitude", C.POINTER(C.c_double)),
+        ("phase", C.POINTER(C.c_double)),
     ]
 
 
@@ -75,7 +92,38 @@ class Mesh(C.Structure):
         ("seg_type", C.POINTER(C.c_int32)),
         ("seg_offsets", C.POINTER(C.c_int64)),
         ("seg_nodes", C.POINTER(C.c_int32)),
+        ("node_manning_n", C.POINTER(C.c_double)),
+        ("n_forcing", C.c_int32),
+        ("forcing", C.POINTER(ForcingBlock)),
     ]
+
+
+def forcing_blocks(mesh, block_type=None):
+    """ctypes array of the mesh's forcing blocks (block_type: ForcingBlock struct class to fill) plus the
+    numpy arrays it points into (keep them alive as long as the array is used)."""
+    block_type = block_type or ForcingBlock
+    blocks = list(getattr(mesh, "forcing", None) or [])
+    keep = []
+    arr = (block_type * max(len(blocks), 1))()
+    for k, b in enumerate(blocks):
+        nodes = np.ascontiguousarray(b.nodes, np.int32)
+        fr = np.ascontiguousarray(b.frequency, np.float64)
+        ff = np.ascontiguousarray(b.forcing_fact, np.float64)
+        eq = np.ascontiguousarray(b.equilib_arg, np.float64)
+        am = np.ascontiguousarray(b.amplitude, np.float64).reshape(len(fr), len(nodes))
+        ph = np.ascontiguousarray(b.phase, np.float64).reshape(len(fr), len(nodes))
+        keep += [nodes, fr, ff, eq, am, ph]
+        arr[k].type = int(b.type)
+        arr[k].n_nodes = len(nodes)
+        arr[k].n_constituents = len(fr)
+        arr[k].nodes = ptr(nodes, C.c_int32)
+        arr[k].frequency = ptr(fr, C.c_double)
+        arr[k].forcing_fact = ptr(ff, C.c_double)
+        arr[k].equilib_arg = ptr(eq, C.c_double)
+        arr[k].amplitude = ptr(am, C.c_double)
+        arr[k].phase = ptr(ph, C.c_double)
+    keep.append(arr)
+    return (arr if blocks else None), len(blocks), keep
 
 
 class Info(C.Structure):

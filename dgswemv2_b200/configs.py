@@ -8,13 +8,16 @@
    h0 = 10 m, a = 3000 m, amplitude 2 m, p=1, SSP-RK2, h_o = 0.01 m, two periods
 4. learned troubled-cell indicator on bowl meshes with random Gaussian humps
 5. ensemble of p=1 members with random smooth bathymetry and wet/dry
+6. tidal channel: two-constituent tide on the open (x = 0) end, a steady + periodic river flow on the
+   other, land sides, sloping bathymetry, Chezy or Manning bottom friction, forcing ramp
 """
 import math
 
 import numpy as np
 
 from . import meshgen
-from .types import (FN_GAUSSIAN_HUMPS, FN_MANUFACTURED_SINE, FN_THACKER_BOWL, FUNCTION, LAND, ProblemConfig)
+from .types import (FLOW, FN_GAUSSIAN_HUMPS, FN_MANUFACTURED_SINE, FN_THACKER_BOWL, FRICTION_CHEZY, FRICTION_MANNING,
+                    FRICTION_NONE, FUNCTION, LAND, TIDE, ForcingBlock, ProblemConfig)
 
 L_MMS = 40000.0
 
@@ -117,3 +120,41 @@ def config5(n_members=256, seed=0, nmin=64, nmax=200, dt=0.5, precision="fp32"):
         meshes.append(mesh)
         cfgs.append(cfg)
     return meshes, cfgs
+
+
+# tidal constituents used by the channel workload (frequencies in rad/s)
+M2_FREQ = 1.405189e-4
+K1_FREQ = 7.292117e-5
+
+
+def tidal_channel(nx=24, ny=6, p=1, rk=(2, 2), dt=2.0, friction="chezy", cf=0.0025, ramp_days=0.01, flow=True,
+                  precision="fp64", jitter=0.15, seed=3, length=10000.0, width=2000.0, depth=10.0):
+    """Channel [0, length] x [0, width]: tide (M2 + K1, amplitude and phase varying along the open end) on
+    x = 0, a river inflow (steady part plus a one-hour oscillation) on x = length (land there when
+    flow=False), land along both sides; depth falls linearly from `depth` to 0.6 `depth`. friction:
+    None, "chezy" (coefficient cf) or "manning" (n from 0.02 to 0.03 along the channel, lower bound cf).
+    Starts at rest; the forcing ramps up over ramp_days."""
+    def bath(x, y):
+        return depth - 0.4 * depth * x / length
+
+    mesh = meshgen.quad_mesh(nx, ny, corners=((0, 0), (length, 0), (length, width), (0, width)),
+                             bc=(LAND, FLOW if flow else LAND, LAND, TIDE), jitter=jitter, seed=seed, bathymetry=bath,
+                             name="tidal_channel_%dx%d" % (nx, ny))
+    x, y = mesh.node_xyz[:, 0], mesh.node_xyz[:, 1]
+    left = np.arange(ny + 1) * (nx + 1)
+    right = nx + np.arange(ny + 1) * (nx + 1)
+    yl = y[left] / width
+    forcing = [ForcingBlock(TIDE, left, np.array([M2_FREQ, K1_FREQ]), np.array([1.0, 0.9]), np.array([30.0, 120.0]),
+                            np.stack([0.4 + 0.1 * yl, 0.15 + 0.0 * yl]), np.stack([10.0 + 20.0 * yl, 50.0 + 0.0 * yl]))]
+    if flow:
+        yr = y[right] / width
+        forcing.append(ForcingBlock(FLOW, right, np.array([0.0, 2 * math.pi / 3600.0]), np.array([1.0, 1.0]),
+                                    np.array([0.0, 0.0]), np.stack([-0.3 + 0.0 * yr, 0.1 + 0.05 * yr]),
+                                    np.stack([0.0 * yr, 90.0 + 0.0 * yr])))
+    mesh.forcing = forcing
+    kind = {None: FRICTION_NONE, "chezy": FRICTION_CHEZY, "manning": FRICTION_MANNING}[friction]
+    if kind == FRICTION_MANNING:
+        mesh.node_manning_n = 0.02 + 0.01 * x / length
+    cfg = ProblemConfig(p=p, rk_nstages=rk[0], rk_order=rk[1], dt=dt, g=9.81, ic_type=0, ic_const=(0.0, 0.0, 0.0),
+                        bottom_friction=kind, friction_cf=cf, ramp_duration=ramp_days, precision=precision)
+    return mesh, cfg

@@ -104,6 +104,10 @@ struct dgsw_rkdg_s {
     void* bath = nullptr;  // [3][ne_pad] bathymetry modes of the linear part
     void* geo = nullptr;   // [5][ne_pad] J^-1 and |J|
     void* egeo = nullptr;  // [3][n_edges] edge normal and half length
+    void* manning = nullptr;  // [ne_pad] g n^2 per element (Manning friction only)
+    Forcing forcing;
+    DBuf<int2> fface;      // tide / flow forcing records
+    DBuf<double> fcon;
     DBuf<int2> halo;
     DBuf<int> tile_halo_off;
     DBuf<int> enodes, tile_edge_off, ref_of_dev;
@@ -212,17 +216,25 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.spherical = h->cfg.spherical;
     A.sp_cos_lat0 = std::cos(h->cfg.sp_lat0_deg * M_PI / 180.0);
     A.sp_R = h->cfg.sp_R;
+    A.friction = h->cfg.bottom_friction;
+    A.friction_cf = h->cfg.friction_cf;
+    A.manning = (const Real*)h->manning;
+    A.fface = h->fface.p;
+    A.fcon = h->fcon.p;
+    // ESSPRKStepper keeps ramp = 1 when Utilities::almost_equal(ramp_duration, 0)
+    A.ramp_on = std::fabs(h->cfg.ramp_duration) < std::numeric_limits<double>::epsilon() * 100 ? 0 : 1;
+    A.ramp_duration = h->cfg.ramp_duration;
 }
 
-cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, bool wd, bool fs) {
+cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, int mode) {
     const int nt = (int)h->tiling.ntiles, mh = h->tiling.max_halo, me = h->tiling.max_edges;
-    return h->cfg.p == 1 ? launch_stage_p1_f64(A, h->tile, nt, mh, me, wd, fs, h->stream)
-                         : launch_stage_p2_f64(A, h->tile, nt, mh, me, wd, fs, h->stream);
+    return h->cfg.p == 1 ? launch_stage_p1_f64(A, h->tile, nt, mh, me, mode, h->stream)
+                         : launch_stage_p2_f64(A, h->tile, nt, mh, me, mode, h->stream);
 }
-cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<float>& A, bool wd, bool fs) {
+cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<float>& A, int mode) {
     const int nt = (int)h->tiling.ntiles, mh = h->tiling.max_halo, me = h->tiling.max_edges;
-    return h->cfg.p == 1 ? launch_stage_p1_f32(A, h->tile, nt, mh, me, wd, fs, h->stream)
-                         : launch_stage_p2_f32(A, h->tile, nt, mh, me, wd, fs, h->stream);
+    return h->cfg.p == 1 ? launch_stage_p1_f32(A, h->tile, nt, mh, me, mode, h->stream)
+                         : launch_stage_p2_f32(A, h->tile, nt, mh, me, mode, h->stream);
 }
 
 template <typename Real>
@@ -231,7 +243,9 @@ cudaError_t launch_stage(dgsw_rkdg_s* h, int s) {
     fill_stage_args<Real>(h, s, A);
     A.wet_in = h->wet[h->wet_cur].p;
     A.wet_out = h->wet[1 - h->wet_cur].p;
-    return launch_stage_any(h, A, h->cfg.wetting_drying != 0, h->cfg.function_source != 0);
+    const int mode = (h->cfg.wetting_drying ? 1 : 0) | (h->cfg.function_source ? 2 : 0) |
+                     (h->cfg.bottom_friction != DGSW_FRICTION_NONE ? 4 : 0);
+    return launch_stage_any(h, A, mode);
 }
 
 template <typename Real>
@@ -558,6 +572,12 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         return fail(DGSW_ERR_INVALID_ARGUMENT, "precision must be DGSW_FP64 or DGSW_FP32");
     if (cfg->function_set < 0 || cfg->function_set >= DGSW_FN_COUNT)
         return fail(DGSW_ERR_INVALID_ARGUMENT, "unknown function set");
+    if (cfg->bottom_friction < DGSW_FRICTION_NONE || cfg->bottom_friction > DGSW_FRICTION_MANNING)
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "unknown bottom friction type");
+    if (cfg->bottom_friction != DGSW_FRICTION_NONE && cfg->friction_cf < 0.)
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "Fatal Error: Chezy friction coefficient must be postive!");
+    if (cfg->bottom_friction == DGSW_FRICTION_MANNING && !mesh->node_manning_n)
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "Manning friction needs the mesh's node_manning_n");
     auto* h = new dgsw_rkdg_s();
     h->cfg = *cfg;
     h->device = cfg->device;
@@ -574,6 +594,7 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
     h->ns = cfg->rk_nstages;
     h->nd = h->tb.nd;
     rc = build_topology(mesh, h->topo, err);
+    if (!rc) rc = build_forcing(mesh, h->topo, cfg->p, h->forcing, err);
     if (rc) {
         delete h;
         return fail(rc, err);
@@ -696,6 +717,24 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         upload_real(h->bath, bdev);
         upload_real(h->geo, gdev);
         upload_real(h->egeo, edev);
+        if (cfg->bottom_friction == DGSW_FRICTION_MANNING) {
+            std::vector<double> mf, mdev((size_t)h->ne_pad, 0.0);
+            manning_factor(h->topo, mesh->node_manning_n, cfg->g, mf);
+            for (int64_t d = 0; d < h->ne; ++d) mdev[d] = mf[h->tiling.ref_of_dev[d]];
+            if ((e = cudaMalloc(&h->manning, (size_t)h->ne_pad * h->real_size)) != cudaSuccess)
+                return cleanup_fail("alloc", e);
+            upload_real(h->manning, mdev);
+            h->device_bytes += (int64_t)h->ne_pad * h->real_size;
+        }
+        static_assert(FORCE_STRIDE == FORCE_STRIDE_DEV, "forcing record layout");
+        const size_t nff = h->forcing.face.size() / 2, nfc = h->forcing.con.size();
+        if (nff) {
+            if ((e = h->fface.alloc(nff)) != cudaSuccess) return cleanup_fail("alloc", e);
+            cudaMemcpy(h->fface.p, h->forcing.face.data(), nff * sizeof(int2), cudaMemcpyHostToDevice);
+            if ((e = h->fcon.alloc(std::max<size_t>(nfc, 1))) != cudaSuccess) return cleanup_fail("alloc", e);
+            if (nfc) cudaMemcpy(h->fcon.p, h->forcing.con.data(), nfc * sizeof(double), cudaMemcpyHostToDevice);
+            h->device_bytes += (int64_t)(nff * 8 + nfc * 8);
+        }
         const size_t nhalo = h->tiling.halo.size() / 2;
         if ((e = h->halo.alloc(std::max<size_t>(nhalo, 1))) != cudaSuccess) return cleanup_fail("alloc", e);
         if (nhalo) cudaMemcpy(h->halo.p, h->tiling.halo.data(), nhalo * sizeof(int2), cudaMemcpyHostToDevice);
@@ -880,11 +919,13 @@ int32_t dgsw_rkdg_create(const dgsw_config* cfg, const dgsw_mesh* mesh, dgsw_han
 // members -> one mesh: nodes and boundary chains appended with index offsets, element IDs renumbered
 // member-major (ascending within each member by its own IDs), caller_group = member of each element
 struct Concat {
-    std::vector<double> xyz;
+    std::vector<double> xyz, manning;
     std::vector<int32_t> en, seg_type, seg_nodes, group;
     std::vector<uint32_t> ids;
     std::vector<int64_t> seg_off{0};
-    dgsw_mesh m;
+    std::vector<std::vector<int32_t>> fnodes;  // forcing block nodes, offset to the joint numbering
+    std::vector<dgsw_forcing_block> forcing;
+    dgsw_mesh m{};
 };
 
 static int concat_members(int32_t n, const dgsw_mesh* members, Concat& C, std::string& err) {
@@ -935,6 +976,32 @@ static int concat_members(int32_t n, const dgsw_mesh* members, Concat& C, std::s
                 C.seg_nodes.push_back((int32_t)(M.seg_nodes[i] + node_base));
             C.seg_off.push_back((int64_t)C.seg_nodes.size());
         }
+        if (M.node_manning_n) {
+            C.manning.resize(node_base, 0.0);
+            C.manning.insert(C.manning.end(), M.node_manning_n, M.node_manning_n + M.n_nodes);
+        }
+        if (M.n_forcing > 0 && !M.forcing) {
+            err = "ensemble member " + std::to_string(k) + ": null forcing block list";
+            return DGSW_ERR_INVALID_ARGUMENT;
+        }
+        // a member's blocks hold only its own nodes, so its faces find only its own blocks
+        for (int32_t b = 0; b < M.n_forcing; ++b) {
+            const dgsw_forcing_block& B = M.forcing[b];
+            if (B.n_nodes > 0 && !B.nodes) {
+                err = "ensemble member " + std::to_string(k) + ": forcing block without nodes";
+                return DGSW_ERR_INVALID_ARGUMENT;
+            }
+            std::vector<int32_t> nodes((size_t)std::max(B.n_nodes, 0));
+            for (int32_t j = 0; j < B.n_nodes; ++j) {
+                if (B.nodes[j] < 0 || B.nodes[j] >= M.n_nodes) {
+                    err = "ensemble member " + std::to_string(k) + ": forcing node index out of range";
+                    return DGSW_ERR_MESH;
+                }
+                nodes[j] = (int32_t)(B.nodes[j] + node_base);
+            }
+            C.fnodes.push_back(std::move(nodes));
+            C.forcing.push_back(B);
+        }
         node_base += M.n_nodes;
         id_base += M.n_elems;
     }
@@ -947,6 +1014,13 @@ static int concat_members(int32_t n, const dgsw_mesh* members, Concat& C, std::s
     C.m.seg_type = C.seg_type.data();
     C.m.seg_offsets = C.seg_off.data();
     C.m.seg_nodes = C.seg_nodes.data();
+    if (!C.manning.empty()) {
+        C.manning.resize(nn, 0.0);
+        C.m.node_manning_n = C.manning.data();
+    }
+    for (size_t b = 0; b < C.forcing.size(); ++b) C.forcing[b].nodes = C.fnodes[b].data();
+    C.m.n_forcing = (int32_t)C.forcing.size();
+    C.m.forcing = C.forcing.empty() ? nullptr : C.forcing.data();
     return DGSW_OK;
 }
 
@@ -1013,6 +1087,9 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     if (h->bath) cudaFree(h->bath);
     if (h->geo) cudaFree(h->geo);
     if (h->egeo) cudaFree(h->egeo);
+    if (h->manning) cudaFree(h->manning);
+    h->fface.release();
+    h->fcon.release();
     h->halo.release();
     h->tile_halo_off.release();
     h->enodes.release();

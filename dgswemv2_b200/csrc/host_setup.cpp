@@ -278,11 +278,8 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
                       std::to_string(n0) + ", " + std::to_string(n1) + ")!";
                 return DGSW_ERR_MESH;
             }
-            if (bt == DGSW_BC_TIDE || bt == DGSW_BC_FLOW) {
-                err = "tide and flow boundaries need .bcis forcing data, which this build does not support";
-                return DGSW_ERR_UNSUPPORTED;
-            }
-            if (bt != DGSW_BC_LAND && bt != DGSW_BC_FUNCTION && bt != DGSW_BC_OUTFLOW) {
+            if (bt != DGSW_BC_LAND && bt != DGSW_BC_TIDE && bt != DGSW_BC_FLOW && bt != DGSW_BC_FUNCTION &&
+                bt != DGSW_BC_OUTFLOW) {
                 err = "unsupported boundary type " + std::to_string(bt);
                 return DGSW_ERR_UNSUPPORTED;
             }
@@ -324,7 +321,7 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
     // boundaries grouped by type (Land, Tide, Flow, Function tuple order), each by (element, face)
     T.bnd.clear();
     std::vector<int64_t> bnd_of_face(3 * ne, -1);
-    for (int bt : {DGSW_BC_LAND, DGSW_BC_FUNCTION}) {
+    for (int bt : {DGSW_BC_LAND, DGSW_BC_TIDE, DGSW_BC_FLOW, DGSW_BC_FUNCTION}) {
         for (int64_t r = 0; r < ne; ++r)
             for (int f = 0; f < 3; ++f)
                 if (T.btype[3 * r + f] == bt) {
@@ -360,7 +357,7 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
 // Device order and tiles: Morton order of element centroids, cut into tiles of `tile` elements.
 // Each tile lists the edges its elements need: interior edges once per tile (an edge between two
 // tiles appears in both lists and is evaluated by both CTAs with the same code), boundary edges
-// with a boundary object (land, function). Outflow faces have no object and contribute nothing.
+// with a boundary object (land, tide, flow, function). Outflow faces have no object and contribute nothing.
 // ------------------------------------------------------------------------------------------------
 static uint64_t spread21(uint64_t v) {
     v &= 0x1fffff;
@@ -511,9 +508,15 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
                 } else if (bi >= 0) {
                     const int idx = (int)(te.size() / 4);
                     slots[f] = (uint32_t)idx;
-                    const int kind = T.bnd[3 * bi + 2] == DGSW_BC_LAND ? EK_LAND : EK_FUNCTION;
+                    const int bt = T.bnd[3 * bi + 2];
+                    const int kind = bt == DGSW_BC_LAND   ? EK_LAND
+                                     : bt == DGSW_BC_TIDE ? EK_TIDE
+                                     : bt == DGSW_BC_FLOW ? EK_FLOW
+                                                          : EK_FUNCTION;
+                    // tide / flow faces carry their forcing record as -2 - index in the b slot
+                    const int32_t fidx = (kind == EK_TIDE || kind == EK_FLOW) ? T.bnd_force[bi] : -1;
                     te.push_back((int32_t)(3 * (d - d0) + f));
-                    te.push_back(-1);
+                    te.push_back(fidx >= 0 ? -2 - fidx : -1);
                     te.push_back(f | kind << 4);
                     te.push_back((int32_t)d);
                     double nx, ny, sJ;
@@ -543,6 +546,100 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
     out.tile_edge_off[out.ntiles] = (int32_t)((int64_t)out.edges.size() / 4);
     out.tile_halo_off[out.ntiles] = (int32_t)((int64_t)out.halo.size() / 2);
     return DGSW_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Tide / flow forcing and Manning friction data
+// ------------------------------------------------------------------------------------------------
+int build_forcing(const dgsw_mesh* m, Topology& T, int p, Forcing& out, std::string& err) {
+    const size_t nb = T.bnd.size() / 3;
+    T.bnd_force.assign(nb, -1);
+    out.face.clear();
+    out.con.clear();
+    bool forced = false;
+    for (size_t i = 0; i < nb; ++i) forced = forced || T.bnd[3 * i + 2] == DGSW_BC_TIDE || T.bnd[3 * i + 2] == DGSW_BC_FLOW;
+    if (!forced) return DGSW_OK;
+    if (m->n_forcing < 0 || (m->n_forcing > 0 && !m->forcing)) {
+        err = "invalid forcing block list";
+        return DGSW_ERR_INVALID_ARGUMENT;
+    }
+    // node -> position in each block; the reference keeps one map per block keyed by node ID
+    std::vector<std::unordered_map<int32_t, int32_t>> pos(m->n_forcing);
+    for (int32_t b = 0; b < m->n_forcing; ++b) {
+        const dgsw_forcing_block& B = m->forcing[b];
+        if ((B.type != DGSW_BC_TIDE && B.type != DGSW_BC_FLOW) || B.n_nodes < 0 || B.n_constituents < 0 ||
+            (B.n_nodes > 0 && !B.nodes) ||
+            (B.n_constituents > 0 && (!B.frequency || !B.forcing_fact || !B.equilib_arg)) ||
+            ((int64_t)B.n_nodes * B.n_constituents > 0 && (!B.amplitude || !B.phase))) {
+            err = "forcing block " + std::to_string(b) + " is malformed";
+            return DGSW_ERR_INVALID_ARGUMENT;
+        }
+        for (int32_t j = 0; j < B.n_nodes; ++j) {
+            const int32_t n = B.nodes[j];
+            if (n < 0 || n >= m->n_nodes) {
+                err = "forcing block " + std::to_string(b) + ": node index out of range";
+                return DGSW_ERR_MESH;
+            }
+            // the reference appends a repeated node's values to the same per-node lists, which shifts
+            // its constituents; such input is rejected here instead
+            if (!pos[b].emplace(n, j).second) {
+                err = "forcing block " + std::to_string(b) + " lists node " + std::to_string(n) + " twice";
+                return DGSW_ERR_MESH;
+            }
+        }
+    }
+    const Rule1D gl = gauss_legendre_degree(2 * p + 1);
+    const int ng = (int)gl.z.size();
+    for (size_t i = 0; i < nb; ++i) {
+        const int bt = T.bnd[3 * i + 2];
+        if (bt != DGSW_BC_TIDE && bt != DGSW_BC_FLOW) continue;
+        const int64_t r = T.bnd[3 * i];
+        const int f = T.bnd[3 * i + 1];
+        // Shape::GetBoundaryNodeID: the face's nodes (f+1)%3, (f+2)%3
+        const int32_t n0 = T.enodes[3 * r + (f + 1) % 3], n1 = T.enodes[3 * r + (f + 2) % 3];
+        int32_t blk = -1, p0 = 0, p1 = 0;
+        for (int32_t b = 0; b < m->n_forcing && blk < 0; ++b) {
+            if (m->forcing[b].type != bt) continue;
+            auto a = pos[b].find(n0), c = pos[b].find(n1);
+            if (a != pos[b].end() && c != pos[b].end()) {
+                blk = b;
+                p0 = a->second;
+                p1 = c->second;
+            }
+        }
+        if (blk < 0) {
+            err = bt == DGSW_BC_TIDE ? "Fatal Error: unable to find tide data!" : "Fatal Error: unable to find flow data!";
+            return DGSW_ERR_MESH;
+        }
+        const dgsw_forcing_block& B = m->forcing[blk];
+        T.bnd_force[i] = (int32_t)(out.face.size() / 2);
+        out.face.push_back((int32_t)(out.con.size() / FORCE_STRIDE));
+        out.face.push_back(B.n_constituents);
+        for (int32_t c = 0; c < B.n_constituents; ++c) {
+            double rec[FORCE_STRIDE] = {0};
+            rec[0] = B.frequency[c];
+            rec[1] = B.forcing_fact[c];
+            rec[2] = B.equilib_arg[c];
+            const size_t row = (size_t)c * B.n_nodes;
+            // ComputeBoundaryNodalUgp: nodal values times the boundary shape functions (1 - z)/2, (1 + z)/2
+            for (int g = 0; g < ng; ++g) {
+                const double N1 = (1.0 - gl.z[g]) / 2.0, N2 = (1.0 + gl.z[g]) / 2.0;
+                rec[3 + g] = B.amplitude[row + p0] * N1 + B.amplitude[row + p1] * N2;
+                rec[3 + MAX_NG + g] = B.phase[row + p0] * N1 + B.phase[row + p1] * N2;
+            }
+            out.con.insert(out.con.end(), rec, rec + FORCE_STRIDE);
+        }
+    }
+    return DGSW_OK;
+}
+
+void manning_factor(const Topology& T, const double* node_n, double g, std::vector<double>& out) {
+    out.assign(T.ne, 0.0);
+    for (int64_t r = 0; r < T.ne; ++r) {
+        double s = 0.0;
+        for (int v = 0; v < 3; ++v) s += node_n[T.enodes[3 * r + v]];
+        out[r] = g * std::pow(s / 3.0, 2);
+    }
 }
 
 // ------------------------------------------------------------------------------------------------

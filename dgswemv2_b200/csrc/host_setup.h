@@ -17,7 +17,7 @@ constexpr int MAX_NQ = 6;
 constexpr int MAX_NG = 3;
 
 // Edge kinds in the per-tile edge lists
-enum EdgeKind { EK_INTERIOR = 0, EK_LAND = 1, EK_FUNCTION = 2 };
+enum EdgeKind { EK_INTERIOR = 0, EK_LAND = 1, EK_FUNCTION = 2, EK_TIDE = 3, EK_FLOW = 4 };
 
 struct Topology {
     int64_t ne = 0, nn = 0;
@@ -37,7 +37,27 @@ struct Topology {
     // parameters [n_members][DGSW_FN_PARAMS]
     std::vector<int32_t> group;
     std::vector<double> group_params;
+    // tide / flow boundaries: forcing record of boundary i (T.bnd order), -1 for the other types
+    std::vector<int32_t> bnd_force;
 };
+
+// Tide and flow forcing of the boundary faces (BC::Tide / BC::Flow constructors and Initialize,
+// discretization_RKDG/boundary_conditions/rkdg_swe_bc_tide.hpp:33-71): one record per forced face, in
+// T.bnd order, holding its first constituent entry and their count; per entry the frequency, forcing
+// factor and equilibrium argument, then amplitude and phase at the edge Gauss points.
+constexpr int FORCE_STRIDE = 3 + 2 * MAX_NG;
+struct Forcing {
+    std::vector<int32_t> face;  // [2 * n_forced] first entry, n_constituents
+    std::vector<double> con;    // [FORCE_STRIDE * n_entries]: freq, forcing_fact, equilib_arg, amp[NG], phase[NG]
+};
+
+// matches tide/flow faces to their .bcis blocks (create_boundaries, swe_pre_create_bound.hpp:33-96) and
+// interpolates amplitude and phase to the face's Gauss points; fills T.bnd_force
+int build_forcing(const dgsw_mesh* m, Topology& T, int p, Forcing& out, std::string& err);
+
+// Manning friction: per element g * (mean of its three nodes' n)^2 (swe_pre_init_data.hpp:165-196),
+// in reference element order
+void manning_factor(const Topology& T, const double* node_n, double g, std::vector<double>& out);
 
 // reference MeshMetaData + create_interfaces/create_boundaries semantics
 int build_topology(const dgsw_mesh* m, Topology& T, std::string& err);

@@ -24,6 +24,7 @@
 
 #include <cstdint>
 
+#include "../../include/dgsw_rkdg.h"
 #include "function_sets.h"
 #include "rk_tables.h"
 #include "tables_gen.h"
@@ -93,7 +94,19 @@ struct StageArgs {
     double fn_params[16];
     int spherical;
     double sp_cos_lat0, sp_R;
+    // bottom friction (swe_source.hpp:29-51): DGSW_FRICTION_NONE / CHEZY / MANNING
+    int friction;
+    double friction_cf;
+    const Real* manning;  // [ne_pad] g n^2 per element (Manning)
+    // tide / flow boundary forcing: per forced face its first constituent entry and count; per entry
+    // frequency, forcing factor, equilibrium argument, amplitude[3] and phase[3] at the Gauss points
+    const int2* fface;
+    const double* fcon;
+    int ramp_on;           // ramp_duration not almost zero
+    double ramp_duration;  // days
 };
+
+constexpr int FORCE_STRIDE_DEV = 9;
 
 // ------------------------------------------------------------------------------------------------
 // LLF flux, rkdg_swe_LLF_flux.hpp:7-60 (sp applied to the in-side normal flux only, as there)
@@ -170,6 +183,51 @@ template <typename Real>
 __device__ __noinline__ void fn_eval_dev(int id, const double* P, const dgsw_fn_time* T, int source, Real x, Real y,
                                          Real* out) {
     dgsw_fn_eval<Real>(id, P, *T, source, x, y, out);
+}
+
+// Ghost states of the boundaries with data, out of line (one call site per Gauss point):
+// BC::Function (kind 2): ic_q(t, x_gp) (rkdg_swe_bc_function.hpp:33-50);
+// BC::Tide (kind 3) and BC::Flow (kind 4) (rkdg_swe_bc_tide.hpp:73-100, rkdg_swe_bc_flow.hpp:72-102), in
+// FP64 in both precisions: the forced value is
+// sum_con ramp * forcing_fact * amplitude_gp * cos(frequency * t + (equilib_arg - phase_gp) * PI / 180)
+// with the reference's PI = 3.14159265359 and ramp = tanh(2 (t / 86400) / ramp_duration)
+// (ESSPRKStepper::operator++, explicit_ssp_rk_stepper.hpp:49-65; 1 without a ramp). A tide sets the
+// ghost surface elevation to it and keeps the interior momentum; a flow keeps the interior elevation
+// and sets the ghost momentum to it times the outward normal. fi is the face's forcing record.
+template <typename Real>
+__device__ __noinline__ void boundary_ghost(const StageArgs<Real>* Ap, const dgsw_fn_time* T, int kind, int fi,
+                                            int gp, double t, Real x, Real y, Real qi0, Real qi1, Real qi2, Real nx,
+                                            Real ny, Real* qe) {
+    const StageArgs<Real>& A = *Ap;
+    if (kind == 2) {
+        dgsw_fn_eval<Real>(A.fn_set, A.fn_params, *T, 0, x, y, qe);
+        return;
+    }
+    constexpr double REF_PI = 3.14159265359;
+    const double ramp = A.ramp_on ? tanh(2.0 * (t / 86400.0) / A.ramp_duration) : 1.0;
+    const int2 fc = A.fface[fi];
+    double acc = 0.0;
+    for (int c = 0; c < fc.y; ++c) {
+        const double* r = A.fcon + (size_t)(fc.x + c) * FORCE_STRIDE_DEV;
+        acc += ramp * r[1] * r[3 + gp] * cos(r[0] * t + (r[2] - r[6 + gp]) * REF_PI / 180.0);
+    }
+    if (kind == 4) {
+        qe[0] = qi0;
+        qe[1] = (Real)acc * nx;
+        qe[2] = (Real)acc * ny;
+    } else {
+        qe[0] = (Real)acc;
+        qe[1] = qi1;
+        qe[2] = qi2;
+    }
+}
+
+// the Manning friction factor g n^2 / h^(1/3), bounded below by the Chezy coefficient (swe_source.hpp:37-42)
+template <typename Real>
+__device__ __noinline__ Real manning_cf(Real gn2, Real h, Real cf0) {
+    Real cf = gn2 / pow(h, Real(1.0 / 3.0));
+    if (cf < cf0) cf = cf0;
+    return cf;
 }
 
 // The manufactured sine set's source terms inline (FP32 path), with its constants hoisted out of the
@@ -433,7 +491,7 @@ struct TileCap {
     static constexpr int edges = TILE + TILE / 2 + TILE / 4 + 16;  // 240 for 128, 464 for 256
 };
 
-template <int P, typename Real, bool WD, bool FSRC, int TILE, bool CAPPED>
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, bool CAPPED>
 __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_halo_rt, int max_edges_rt) {
     const int max_halo = CAPPED ? TileCap<TILE>::halo : max_halo_rt;
@@ -557,6 +615,15 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                 }
                 // bathymetry-slope source, swe_source.hpp:15-21 (the analytic source follows in its own loop)
                 Real S[3] = {Real(0), g * (dbx * qg[0]), g * (dby * qg[0])};
+                // bottom friction, swe_source.hpp:29-51: S(qx, qy) -= Cf |u| / h (qx, qy), Cf the Chezy
+                // coefficient or, for Manning, max(g n^2 / h^(1/3), Cf)
+                if (FRIC) {
+                    const Real cf = A.friction == DGSW_FRICTION_MANNING ? manning_cf<Real>(A.manning[d], h, (Real)A.friction_cf)
+                                                                        : (Real)A.friction_cf;
+                    const Real tau = cf * hypot(u, vv) / h;
+                    S[1] -= tau * qg[1];
+                    S[2] -= tau * qg[2];
+                }
                 // int F . grad(phi) = sum_gp sum_z (F_x J^-1(z,x) + F_y J^-1(z,y)) dphi_z w
                 sfor<0, 3>([&](auto V) {
                     constexpr int v = decltype(V)::value;
@@ -694,7 +761,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                 sj_n = A.egeo[2 * A.n_edges + nle];
             }
             const int sa = rec.x, sb = rec.y;
-            const int kind = (rec.z >> 4) & 3;
+            const int kind = (rec.z >> 4) & 7;
             const bool wa = swet[sa] != 0;
             const bool wb = sb >= 0 && swet[sb] != 0;
             const bool compute = (kind == 0) ? (wa || wb) : wa;
@@ -733,9 +800,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                     qe[1] = qn_ex * nx + qt_ex * tx;
                     qe[2] = qn_ex * ny + qt_ex * ty;
                 } else {
-                    // BC::Function ghost state: ic_q(t, x_gp) (rkdg_swe_bc_function.hpp:33-50)
-                    fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 0, (Real)(xa * wa_ + xb * wb_),
-                                      (Real)(ya * wa_ + yb * wb_), qe);
+                    // function, tide and flow boundaries (a tide / flow face's b slot holds -2 - its
+                    // forcing record)
+                    boundary_ghost<Real>(&A, &FT, kind, -2 - sb, gp, t_stage, (Real)(xa * wa_ + xb * wb_),
+                                         (Real)(ya * wa_ + yb * wb_), qi[0], qi[1], qi[2], nx, ny, qe);
                 }
                 Real Fi[3];
                 llf_flux<Real>(g, qi, qe, bi, sp, nx, ny, Fi);
@@ -884,19 +952,20 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
 }
 
 // launchers, one translation unit per (order, precision)
-cudaError_t launch_stage_p1_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
-                                bool fsrc, cudaStream_t s);
-cudaError_t launch_stage_p1_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
-                                bool fsrc, cudaStream_t s);
-cudaError_t launch_stage_p2_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
-                                bool fsrc, cudaStream_t s);
-cudaError_t launch_stage_p2_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
-                                bool fsrc, cudaStream_t s);
+cudaError_t launch_stage_p1_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                int mode, cudaStream_t s);
+cudaError_t launch_stage_p1_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                int mode, cudaStream_t s);
+cudaError_t launch_stage_p2_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                int mode, cudaStream_t s);
+cudaError_t launch_stage_p2_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                int mode, cudaStream_t s);
 
-template <int P, typename Real, bool WD, bool FSRC, int TILE>
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE>
 cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo, int max_edges, cudaStream_t s) {
     const bool capped = max_halo <= TileCap<TILE>::halo && max_edges <= TileCap<TILE>::edges;
-    auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, TILE, true> : rkdg_stage_kernel<P, Real, WD, FSRC, TILE, false>;
+    auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, true>
+                       : rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, false>;
     const size_t smem = capped ? Smem<P, Real, WD>::bytes(TILE, TileCap<TILE>::halo, TileCap<TILE>::edges)
                                : Smem<P, Real, WD>::bytes(TILE, max_halo, max_edges);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -905,32 +974,33 @@ cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo
     return cudaGetLastError();
 }
 
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC>
+cudaError_t launch_stage_tile(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges,
+                              cudaStream_t s) {
+    switch (tile) {
+        case 128:
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 128>(A, ntiles, max_halo, max_edges, s);
+        case 256:
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 256>(A, ntiles, max_halo, max_edges, s);
+        default:
+            return cudaErrorInvalidValue;
+    }
+}
+
+// wetting/drying, function source and bottom friction select the instantiation (bit 0, 1, 2 of `mode`)
 template <int P, typename Real>
-cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
-                                  bool fsrc, cudaStream_t s) {
-#define DGSW_TILE_CASES(WD_, FS_)                                                               \
-    switch (tile) {                                                                              \
-        case 128:                                                                                \
-            return launch_stage_impl<P, Real, WD_, FS_, 128>(A, ntiles, max_halo, max_edges, s); \
-        case 256:                                                                                \
-            return launch_stage_impl<P, Real, WD_, FS_, 256>(A, ntiles, max_halo, max_edges, s); \
-        default:                                                                                 \
-            return cudaErrorInvalidValue;                                                        \
+cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                  int mode, cudaStream_t s) {
+    switch (mode & 7) {
+        case 0: return launch_stage_tile<P, Real, false, false, false>(A, tile, ntiles, max_halo, max_edges, s);
+        case 1: return launch_stage_tile<P, Real, true, false, false>(A, tile, ntiles, max_halo, max_edges, s);
+        case 2: return launch_stage_tile<P, Real, false, true, false>(A, tile, ntiles, max_halo, max_edges, s);
+        case 3: return launch_stage_tile<P, Real, true, true, false>(A, tile, ntiles, max_halo, max_edges, s);
+        case 4: return launch_stage_tile<P, Real, false, false, true>(A, tile, ntiles, max_halo, max_edges, s);
+        case 5: return launch_stage_tile<P, Real, true, false, true>(A, tile, ntiles, max_halo, max_edges, s);
+        case 6: return launch_stage_tile<P, Real, false, true, true>(A, tile, ntiles, max_halo, max_edges, s);
+        default: return launch_stage_tile<P, Real, true, true, true>(A, tile, ntiles, max_halo, max_edges, s);
     }
-    if (wd) {
-        if (fsrc) {
-            DGSW_TILE_CASES(true, true)
-        } else {
-            DGSW_TILE_CASES(true, false)
-        }
-    } else {
-        if (fsrc) {
-            DGSW_TILE_CASES(false, true)
-        } else {
-            DGSW_TILE_CASES(false, false)
-        }
-    }
-#undef DGSW_TILE_CASES
 }
 
 }  // namespace dgsw

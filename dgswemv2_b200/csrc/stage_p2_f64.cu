@@ -2,8 +2,8 @@
 #include "stage_kernel.cuh"
 
 namespace dgsw {
-cudaError_t launch_stage_p2_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges, bool wd,
-                                bool fsrc, cudaStream_t s) {
-    return launch_stage_dispatch<2, double>(A, tile, ntiles, max_halo, max_edges, wd, fsrc, s);
+cudaError_t launch_stage_p2_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                int mode, cudaStream_t s) {
+    return launch_stage_dispatch<2, double>(A, tile, ntiles, max_halo, max_edges, mode, s);
 }
 }  // namespace dgsw

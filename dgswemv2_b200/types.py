@@ -10,6 +10,9 @@ import numpy as np
 LAND, TIDE, FLOW, FUNCTION, OUTFLOW = 0, 1, 2, 3, 4
 INTERNAL = 128
 
+# bottom friction types (source/problem/SWE/swe_definitions.hpp:92)
+FRICTION_NONE, FRICTION_CHEZY, FRICTION_MANNING = 0, 1, 2
+
 # function sets (dgswemv2_b200/csrc/function_sets.h)
 FN_NONE, FN_REFERENCE_MANUFACTURED, FN_MANUFACTURED_SINE, FN_THACKER_BOWL, FN_GAUSSIAN_HUMPS = range(5)
 
@@ -35,6 +38,21 @@ class ProblemConfig:
     sp_lat0_deg: float = 0.0
     sp_R: float = 6378200.0
     precision: str = "fp64"  # "fp64" or "fp32" (FP32 bulk, FP64 wet/dry tests and mass reduction)
+    bottom_friction: int = FRICTION_NONE  # problem.bottom_friction.type
+    friction_cf: float = 0.0  # bottom_friction.coefficient
+    ramp_duration: float = 0.0  # timestepping.ramp_duration (days) of the tide/flow forcing
+
+
+@dataclass
+class ForcingBlock:
+    """One tide or flow block of a `.bcis` file (SWE::Inputs::read_bcis, swe_inputs.cpp:211-290)."""
+    type: int  # TIDE or FLOW
+    nodes: np.ndarray  # (n_nodes,) 0-based node indices
+    frequency: np.ndarray  # (n_constituents,) rad/s
+    forcing_fact: np.ndarray  # (n_constituents,)
+    equilib_arg: np.ndarray  # (n_constituents,) degrees
+    amplitude: np.ndarray  # (n_constituents, n_nodes)
+    phase: np.ndarray  # (n_constituents, n_nodes) degrees
 
 
 @dataclass
@@ -46,6 +64,8 @@ class MeshArrays:
     seg_nodes: np.ndarray  # concatenated node chains
     elem_ids: Optional[np.ndarray] = None  # reference element IDs (default 0..n-1)
     name: str = "mesh"
+    node_manning_n: Optional[np.ndarray] = None  # (n_nodes,) Manning's n (FRICTION_MANNING)
+    forcing: List[ForcingBlock] = field(default_factory=list)  # tide / flow data
 
     @property
     def n_elems(self):

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define DGSW_ABI_VERSION 1
+#define DGSW_ABI_VERSION 2
 #define DGSW_TILE_AUTOTUNE (-1)
 
 typedef enum {
@@ -35,6 +35,9 @@ typedef enum {
 } dgsw_status;
 
 typedef enum { DGSW_FP64 = 0, DGSW_FP32 = 1 } dgsw_precision;
+
+/* Bottom friction types, source/problem/SWE/swe_definitions.hpp:92 */
+enum { DGSW_FRICTION_NONE = 0, DGSW_FRICTION_CHEZY = 1, DGSW_FRICTION_MANNING = 2 };
 
 /* Boundary condition / edge types, source/problem/SWE/swe_definitions.hpp:61-69 */
 enum { DGSW_BC_LAND = 0, DGSW_BC_TIDE = 1, DGSW_BC_FLOW = 2, DGSW_BC_FUNCTION = 3, DGSW_BC_OUTFLOW = 4,
@@ -60,6 +63,10 @@ typedef struct {
     double fn_params[16];      /* parameters of that set */
     int32_t spherical;         /* problem.spherical_projection present */
     double sp_lat0_deg, sp_R;  /* spherical_projection.{latitude_o, R} */
+    int32_t bottom_friction;   /* problem.bottom_friction.type: DGSW_FRICTION_{NONE,CHEZY,MANNING} */
+    double friction_cf;        /* bottom_friction.coefficient: Chezy Cf, or the lower bound of the Manning
+                                  factor g n^2 / h^(1/3) */
+    double ramp_duration;      /* timestepping.ramp_duration in days (tide/flow forcing ramp; 0 = none) */
     /* execution options (no reference counterpart) */
     int32_t precision;         /* dgsw_precision: FP64, or FP32 bulk arithmetic (volume, edge and source
                                   integrals) with FP64 stage states, wet/dry tests, limiter and reductions */
@@ -72,10 +79,27 @@ typedef struct {
     int32_t reserved[8];
 } dgsw_config;
 
+/* One tide or flow block of the `.bcis` file (SWE::Inputs::read_bcis, problem_input/swe_inputs.cpp:211-
+ * 290): its nodes and, per constituent, frequency (rad/s), forcing factor and equilibrium argument
+ * (degrees), and the amplitude and phase (degrees) at each node. A tide/flow boundary face takes its data
+ * from the first block of its type that holds both of its nodes (create_boundaries,
+ * problem_preprocessor/swe_pre_create_bound.hpp:33-96). */
+typedef struct {
+    int32_t type;              /* DGSW_BC_TIDE or DGSW_BC_FLOW */
+    int32_t n_nodes;
+    int32_t n_constituents;
+    const int32_t* nodes;      /* [n_nodes] 0-based node indices, each at most once */
+    const double* frequency;   /* [n_constituents] */
+    const double* forcing_fact;
+    const double* equilib_arg;
+    const double* amplitude;   /* [n_constituents][n_nodes] */
+    const double* phase;       /* [n_constituents][n_nodes] */
+} dgsw_forcing_block;
+
 /* Mesh: node coordinates (x, y, bathymetry depth), element node triples (0-based node indices), the
  * reference element IDs (the order the reference iterates elements in; NULL = 0..n-1), and ADCIRC-style
  * boundary node chains with their types, searched in the given order like AdcircFormat::get_ibtype
- * (source/preprocessor/ADCIRC_reader/adcirc_format.cpp). */
+ * (source/preprocessor/ADCIRC_reader/adcirc_format.cpp), then the optional Manning and tide/flow data. */
 typedef struct {
     int64_t n_nodes;
     const double* node_xyz;     /* [3*n_nodes] */
@@ -86,6 +110,9 @@ typedef struct {
     const int32_t* seg_type;    /* [n_segments], DGSW_BC_* */
     const int64_t* seg_offsets; /* [n_segments+1] */
     const int32_t* seg_nodes;   /* [seg_offsets[n_segments]] */
+    const double* node_manning_n;        /* [n_nodes] Manning's n per node (DGSW_FRICTION_MANNING), or NULL */
+    int32_t n_forcing;                   /* tide / flow forcing blocks */
+    const dgsw_forcing_block* forcing;   /* [n_forcing] */
 } dgsw_mesh;
 
 typedef struct {

@@ -304,7 +304,7 @@ struct AdcircMesh {
     int64_t n_elems() const { return (int64_t)elem_names.size(); }
 
     dgsw_mesh view() const {
-        dgsw_mesh m;
+        dgsw_mesh m{};
         m.n_nodes = n_nodes();
         m.node_xyz = node_xyz.data();
         m.n_elems = n_elems();

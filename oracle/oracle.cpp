@@ -35,6 +35,7 @@ constexpr uint32_t DEFAULT_ID = 4294967295u;  // general_definitions.hpp:230
 constexpr int BT_LAND = 0, BT_TIDE = 1, BT_FLOW = 2, BT_FUNCTION = 3, BT_OUTFLOW = 4;
 constexpr int BT_INTERNAL = 128;  // utilities/edge_types.hpp:4
 constexpr double DBL_EPS = 2.220446049250313e-16;
+constexpr double REF_PI = 3.14159265359;  // the reference's PI (general_definitions.hpp:227)
 
 // ------------------------------------------------------------------------------------------------
 // Jacobi polynomials, source/basis/polynomials/basis_polynomials.cpp:4-67
@@ -413,6 +414,9 @@ struct Elt {
     double sl_I = 0.0, sl_perimeter = 0.0;
     bool sl_troubled = false;
     bool limited = false;
+    // bottom friction (swe_data_source.hpp): Manning factor g * mean(n)^2
+    bool manning = false;
+    double g_manning_n_sq = 0.0;
 };
 
 struct Intf {
@@ -431,6 +435,10 @@ struct Bnd {
     vector<double> phi, ipf, int_fact;
     double n[2];
     vector<double> gpx, gpy;
+    // BC::Tide / BC::Flow data (rkdg_swe_bc_tide.hpp:9-71): constituents of the face's first node and
+    // amplitude / phase at the Gauss points
+    vector<double> frequency, forcing_fact, equilib_arg;
+    vector<vector<double>> amplitude_gp, phase_gp;
 };
 
 struct Problem {
@@ -447,6 +455,7 @@ struct Problem {
     int stage = 0;
     int step = 0;
     double t = 0.0;
+    double ramp = 1.0;  // ESSPRKStepper::ramp
     double h_o_threshold = 1.0e-6;
     int nthreads = 1;
     dgsw::Rule2D l2rule;
@@ -479,6 +488,53 @@ int get_ibtype(const orc_mesh* m, int32_t n0, int32_t n1) {
     return -1;
 }
 
+// Tide / flow data of one boundary face: create_boundaries (swe_pre_create_bound.hpp:33-96) takes the
+// first .bcis block of the face's type holding both of its nodes (TideBoundary::get_tide_data,
+// swe_inputs.hpp:34-49); the BC::Tide / BC::Flow constructors take the constituents of the face's first
+// node and the nodal amplitude / phase (rkdg_swe_bc_tide.hpp:33-52), Initialize interpolates them to the
+// Gauss points with GetBoundaryPsi's N1 = (1 - z) / 2, N2 = (1 + z) / 2 (shape_straighttriangle.cpp:215-227).
+void attach_forcing(const orc_mesh* m, const Elt& E, const dgsw::Rule1D& gl, Bnd& B) {
+    const int32_t nodes[2] = {E.node_idx[(B.bid + 1) % 3], E.node_idx[(B.bid + 2) % 3]};
+    for (int32_t b = 0; b < m->n_forcing; ++b) {
+        const orc_forcing_block& F = m->forcing[b];
+        if (F.type != B.type) continue;
+        int pos[2] = {-1, -1};
+        for (int k = 0; k < 2; ++k)
+            for (int j = 0; j < F.n_nodes; ++j)
+                if (F.nodes[j] == nodes[k]) {
+                    if (pos[k] >= 0) throw std::runtime_error("forcing block lists a node twice");
+                    pos[k] = j;
+                }
+        if (pos[0] < 0 || pos[1] < 0) continue;
+        const int ncon = F.n_constituents, ngb = (int)gl.z.size();
+        B.frequency.assign(F.frequency, F.frequency + ncon);
+        B.forcing_fact.assign(F.forcing_fact, F.forcing_fact + ncon);
+        B.equilib_arg.assign(F.equilib_arg, F.equilib_arg + ncon);
+        B.amplitude_gp.assign(ncon, vector<double>(ngb, 0.0));
+        B.phase_gp.assign(ncon, vector<double>(ngb, 0.0));
+        for (int con = 0; con < ncon; ++con) {
+            const double a[2] = {F.amplitude[(size_t)con * F.n_nodes + pos[0]], F.amplitude[(size_t)con * F.n_nodes + pos[1]]};
+            const double ph[2] = {F.phase[(size_t)con * F.n_nodes + pos[0]], F.phase[(size_t)con * F.n_nodes + pos[1]]};
+            for (int gp = 0; gp < ngb; ++gp) {
+                const double psi[2] = {(1 - gl.z[gp]) / 2, (1 + gl.z[gp]) / 2};
+                double sa = 0, sp = 0;
+                for (int n = 0; n < 2; ++n) {
+                    sa += a[n] * psi[n];
+                    sp += ph[n] * psi[n];
+                }
+                B.amplitude_gp[con][gp] = sa;
+                B.phase_gp[con][gp] = sp;
+            }
+        }
+        return;
+    }
+    throw std::runtime_error(B.type == BT_TIDE ? "Fatal Error: unable to find tide data!\n"
+                                               : "Fatal Error: unable to find flow data!\n");
+}
+
+// Utilities::almost_equal(a, 0) (utilities/almost_equal.hpp:16-22) with its default factor 100
+bool almost_zero(double a) { return std::abs(a) < DBL_EPS * 100; }
+
 int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
     P.cfg = *cfg;
     P.p = cfg->p;
@@ -489,6 +545,12 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
         throw std::runtime_error("Fatal Error: invalid Runge-Kutta method entered!");
     P.ns = cfg->rk_nstages;
     P.nthreads = cfg->n_threads > 0 ? cfg->n_threads : 1;
+    // ESSPRKStepper ctor (explicit_ssp_rk_stepper.cpp:12): ramp 1 if ramp_duration is almost zero, else 0
+    P.ramp = almost_zero(cfg->ramp_duration) ? 1.0 : 0.0;
+    if (cfg->bottom_friction < 0 || cfg->bottom_friction > 2) throw std::runtime_error("unknown bottom friction type");
+    if (cfg->bottom_friction != 0 && cfg->friction_cf < 0.)
+        throw std::runtime_error("Fatal Error: Chezy friction coefficient must be postive!");
+    if (cfg->bottom_friction == 2 && !m->node_manning_n) throw std::runtime_error("Manning friction needs node n");
     if (cfg->wetting_drying) P.h_o_threshold = 1.0e6 * cfg->h_o * DBL_EPS;  // swe_pre_init_prob_params.hpp:36
     const int ne = (int)m->n_elems;
     // elements in ascending ID order (element storage is an ordered map keyed by ID)
@@ -659,8 +721,6 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
     for (int bt : {BT_LAND, BT_TIDE, BT_FLOW, BT_FUNCTION}) {
         auto it = raw_bound.find(bt);
         if (it == raw_bound.end()) continue;
-        if (bt == BT_TIDE) throw std::runtime_error("tide boundaries need .bcis tide data (not supported)");
-        if (bt == BT_FLOW) throw std::runtime_error("flow boundaries need .bcis flow data (not supported)");
         for (auto& kv : it->second) {
             Bnd B;
             B.elt = kv.second.first;
@@ -681,6 +741,7 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
             for (int dof = 0; dof < nd; ++dof)
                 for (int gp = 0; gp < ngb; ++gp) B.ipf[gp * nd + dof] = B.phi[dof * ngb + gp] * (gl.w[gp] * sJ);
             E.shape.normal(B.bid, B.n);
+            if (bt == BT_TIDE || bt == BT_FLOW) attach_forcing(m, E, gl, B);
             P.bnds.push_back(std::move(B));
         }
     }
@@ -895,6 +956,14 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
             }
         }
     }
+    // Manning n per element (swe_pre_init_data.hpp:165-196): g * (mean of the three nodal n)^2
+    if (cfg->bottom_friction == 2)
+        for (auto& E : P.elts) {
+            double n[3];
+            for (int v = 0; v < 3; ++v) n[v] = m->node_manning_n[E.node_idx[v]];
+            E.manning = true;
+            E.g_manning_n_sq = cfg->g * std::pow(std::accumulate(n, n + 3, 0.0) / 3, 2);
+        }
     // L2-error rule (Element::ComputeResidualL2 asks for degree 20)
     P.l2rule = dgsw::triangle_rule(20);
     P.l2phi = get_phi(P.p, P.l2rule.z1, P.l2rule.z2);
@@ -954,6 +1023,20 @@ void volume_source(Problem& P, Elt& E) {  // rkdg_swe_proc_volume.hpp:9-35, rkdg
             S[0][gp] += f.ze;
             S[1][gp] += f.qx;
             S[2][gp] += f.qy;
+        }
+    }
+    if (P.cfg.bottom_friction != 0) {  // swe_source.hpp:29-51
+        for (int gp = 0; gp < ngp; ++gp) {
+            double Cf = P.cfg.friction_cf;
+            const double h = qg[0][gp] + E.bath_gp[gp];
+            const double u = qg[1][gp] / h, v = qg[2][gp] / h;
+            if (E.manning) {
+                Cf = E.g_manning_n_sq / std::pow(h, 1.0 / 3.0);
+                if (Cf < P.cfg.friction_cf) Cf = P.cfg.friction_cf;
+            }
+            const double stress = Cf * std::hypot(u, v) / h;
+            S[1][gp] -= stress * qg[1][gp];
+            S[2][gp] -= stress * qg[2][gp];
         }
     }
     for (int v = 0; v < 3; ++v)
@@ -1020,7 +1103,7 @@ void interface_flux(Problem& P, Intf& I) {
     }
 }
 
-// boundary flux, rkdg_swe_proc_bound.hpp:7-20 + BC::Land (:41-66) / BC::Function (:27-60)
+// boundary flux, rkdg_swe_proc_bound.hpp:7-20 + BC::Land (:41-66) / BC::Tide / BC::Flow / BC::Function (:27-60)
 void boundary_flux(Problem& P, Bnd& B) {
     Elt& E = P.elts[B.elt];
     if (!E.wet) return;
@@ -1034,6 +1117,23 @@ void boundary_flux(Problem& P, Bnd& B) {
         for (int v = 0; v < 3; ++v) qi[v] = F.q_at_gp[v * ngb + gp];
         if (B.type == BT_LAND) {
             land_flux(g, B.n, qi, F.bath[gp], F.sp[gp], Fh);
+        } else if (B.type == BT_TIDE || B.type == BT_FLOW) {
+            // BC::Tide / BC::Flow ComputeFlux (rkdg_swe_bc_tide.hpp:73-100, rkdg_swe_bc_flow.hpp:72-102)
+            double forced = 0.0;
+            for (size_t con = 0; con < B.frequency.size(); ++con)
+                forced += P.ramp * B.forcing_fact[con] * B.amplitude_gp[con][gp] *
+                          cos(B.frequency[con] * t + (B.equilib_arg[con] - B.phase_gp[con][gp]) * REF_PI / 180);
+            double qe[3];
+            if (B.type == BT_TIDE) {
+                qe[0] = forced;
+                qe[1] = qi[1];
+                qe[2] = qi[2];
+            } else {
+                qe[0] = qi[0];
+                qe[1] = forced * B.n[0];
+                qe[2] = forced * B.n[1];
+            }
+            LLF_flux(g, qi, qe, F.bath[gp], F.sp[gp], B.n, Fh);
         } else {
             dgsw_fn3 f = dgsw_fn_ic(P.cfg.function_set, P.cfg.fn_params, t, B.gpx[gp], B.gpy[gp]);
             double qe[3] = {f.ze, f.qx, f.qy};
@@ -1375,6 +1475,7 @@ int do_stage(Problem& P) {
         P.t += dt;
         P.step++;
     }
+    if (!almost_zero(P.cfg.ramp_duration)) P.ramp = std::tanh(2 * (P.stage_time() / 86400) / P.cfg.ramp_duration);
     if (P.cfg.wetting_drying) {
         OMP_FOR
         for (int k = 0; k < ne; ++k) {

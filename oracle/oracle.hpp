@@ -35,6 +35,22 @@ struct orc_config {
     int32_t spherical;    // spherical projection on/off
     double sp_lat0_deg, sp_R;
     int32_t n_threads;    // OpenMP threads for the element/edge sweeps (1 = serial)
+    int32_t bottom_friction;  // 0 none, 1 Chezy, 2 Manning (swe_definitions.hpp:92)
+    double friction_cf;       // bottom_friction.coefficient
+    double ramp_duration;     // timestepping.ramp_duration (days)
+};
+
+// one tide / flow block of the .bcis file (read_bcis, swe_inputs.cpp:211-290)
+struct orc_forcing_block {
+    int32_t type;  // 1 tide, 2 flow
+    int32_t n_nodes;
+    int32_t n_constituents;
+    const int32_t* nodes;        // [n_nodes] node indices
+    const double* frequency;     // [n_constituents]
+    const double* forcing_fact;  // [n_constituents]
+    const double* equilib_arg;   // [n_constituents]
+    const double* amplitude;     // [n_constituents][n_nodes]
+    const double* phase;         // [n_constituents][n_nodes]
 };
 
 // mesh: node coordinates (x,y,z = bathymetry depth), element node triples (0-based node indices,
@@ -50,6 +66,9 @@ struct orc_mesh {
     const int32_t* seg_type;
     const int64_t* seg_offsets;  // n_segments+1
     const int32_t* seg_nodes;
+    const double* node_manning_n;  // [n_nodes] Manning's n (bottom_friction 2), or null
+    int32_t n_forcing;
+    const orc_forcing_block* forcing;
 };
 
 typedef struct orc_handle_s* orc_handle;

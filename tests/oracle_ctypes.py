@@ -3,7 +3,7 @@ import ctypes as C
 
 import numpy as np
 
-
+from dgswemv2_b200._lib import forcing_blocks
 
 
 class OrcConfig(C.Structure):
@@ -27,6 +27,23 @@ class OrcConfig(C.Structure):
         ("sp_lat0_deg", C.c_double),
         ("sp_R", C.c_double),
         ("n_threads", C.c_int32),
+        ("bottom_friction", C.c_int32),
+        ("friction_cf", C.c_double),
+        ("ramp_duration", C.c_double),
+    ]
+
+
+class OrcForcingBlock(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("n_nodes", C.c_int32),
+        ("n_constituents", C.c_int32),
+        ("nodes", C.POINTER(C.c_int32)),
+        ("frequency", C.POINTER(C.c_double)),
+        ("forcing_fact", C.POINTER(C.c_double)),
+        ("equilib_arg", C.POINTER(C.c_double)),
+        ("amplitude", C.POINTER(C.c_double)),
+        ("phase", C.POINTER(C.c_double)),
     ]
 
 
@@ -41,6 +58,9 @@ class OrcMesh(C.Structure):
         ("seg_type", C.POINTER(C.c_int32)),
         ("seg_offsets", C.POINTER(C.c_int64)),
         ("seg_nodes", C.POINTER(C.c_int32)),
+        ("node_manning_n", C.POINTER(C.c_double)),
+        ("n_forcing", C.c_int32),
+        ("forcing", C.POINTER(OrcForcingBlock)),
     ]
 
 
@@ -73,6 +93,9 @@ class OracleProblem:
         c.sp_lat0_deg = cfg.sp_lat0_deg
         c.sp_R = cfg.sp_R
         c.n_threads = n_threads
+        c.bottom_friction = int(getattr(cfg, "bottom_friction", 0))
+        c.friction_cf = float(getattr(cfg, "friction_cf", 0.0))
+        c.ramp_duration = float(getattr(cfg, "ramp_duration", 0.0))
         self._keep = [np.ascontiguousarray(mesh.node_xyz, np.float64), np.ascontiguousarray(mesh.elem_nodes, np.int32),
                       None if mesh.elem_ids is None else np.ascontiguousarray(mesh.elem_ids, np.uint32),
                       np.ascontiguousarray(mesh.seg_type, np.int32), np.ascontiguousarray(mesh.seg_offsets, np.int64),
@@ -87,6 +110,15 @@ class OracleProblem:
         m.seg_type = _ptr(self._keep[3], C.c_int32)
         m.seg_offsets = _ptr(self._keep[4], C.c_int64)
         m.seg_nodes = _ptr(self._keep[5], C.c_int32)
+        mann = getattr(mesh, "node_manning_n", None)
+        if mann is not None:
+            mann = np.ascontiguousarray(mann, np.float64)
+            self._keep.append(mann)
+            m.node_manning_n = _ptr(mann, C.c_double)
+        arr, nf, fkeep = forcing_blocks(mesh, OrcForcingBlock)
+        self._keep.append(fkeep)
+        m.n_forcing = nf
+        m.forcing = arr
         h = C.c_void_p()
         rc = lib.orc_create(C.byref(c), C.byref(m), C.byref(h))
         if rc != 0:

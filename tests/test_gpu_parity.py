@@ -178,3 +178,69 @@ def test_trouble_indicator_matches_oracle(oracle, p):
         assert np.array_equal(tg[~near] != 0, to[~near] != 0)
         seen += int(to.sum())
     assert seen > 0
+
+
+TIDE_CASES = [
+    # p, rk, dt, friction, lower bound cf, ramp (days), river flow
+    (1, (2, 2), 2.0, "chezy", 0.0025, 0.01, True),
+    (2, (3, 3), 1.0, "manning", 0.0005, 0.01, True),
+    (1, (3, 3), 2.0, None, 0.0, 0.0, False),
+    (2, (2, 2), 1.0, "chezy", 0.004, 0.0, True),
+]
+
+
+@pytest.mark.parametrize("case", TIDE_CASES, ids=lambda c: "p%d-%s-ramp%g" % (c[0], c[3], c[5]))
+def test_tidal_channel_matches_oracle(oracle, case):
+    """Tide and flow boundaries (M2 + K1 tide with amplitude/phase varying along the open end, steady +
+    periodic river flow), the forcing ramp and Chezy / Manning friction, FP64: per-variable state within
+    1e-12 of the oracle's scale after 300 steps."""
+    p, rk, dt, fr, cf, ramp, flow = case
+    mesh, cfg = configs.tidal_channel(p=p, rk=rk, dt=dt, friction=fr, cf=cf, ramp_days=ramp, flow=flow)
+    P, O = run_pair(oracle, mesh, cfg, 300)
+    q = O.get_state()
+    assert np.abs(q[:, 0, 0]).max() > 0.05  # the tide has entered the channel
+    e = rel_err(P.get_state(), q)
+    assert e <= 1e-12, e
+    assert P.time()[0] == O.time()
+
+
+def test_tidal_channel_fp32_bulk(oracle):
+    """FP32 bulk arithmetic with FP64 forcing evaluation and states: within 1e-4 of the FP64 oracle's
+    per-variable scale after 300 steps."""
+    mesh, cfg = configs.tidal_channel(p=2, rk=(3, 3), dt=1.0, friction="manning", cf=0.0005, precision="fp32")
+    P = Problem(cfg, mesh)
+    cfg64 = configs.tidal_channel(p=2, rk=(3, 3), dt=1.0, friction="manning", cf=0.0005)[1]
+    O = oracle.problem(cfg64, mesh, n_threads=8)
+    P.step_serial(300)
+    O.step(300)
+    e = rel_err(P.get_state(), O.get_state())
+    assert e < 1e-4, e
+
+
+def test_tidal_channel_ensemble_matches_single_runs(oracle):
+    """Members with their own tide / flow data and Manning n in one ensemble handle give each member's
+    single-handle result."""
+    from dgswemv2_b200 import ensemble
+
+    cases = [configs.tidal_channel(nx=12, ny=4, friction="manning", cf=0.0005, seed=s, jitter=0.1 * s)
+             for s in (1, 2, 3)]
+    meshes = [m for m, _ in cases]
+    cfg = cases[0][1]
+    E = ensemble(cfg, meshes, tile=0)
+    E.step_serial(100)
+    q = E.get_state()
+    for k, m in enumerate(meshes):
+        first, n = E.member_range(k)
+        P = Problem(cfg, m)
+        P.step_serial(100)
+        assert rel_err(q[first:first + n], P.get_state()) <= 1e-12, k
+
+
+def test_tide_face_without_data_is_a_mesh_error():
+    from dgswemv2_b200._lib import DgswError
+
+    mesh, cfg = configs.tidal_channel(nx=6, ny=3, flow=False)
+    mesh.forcing = []
+    with pytest.raises(DgswError, match="unable to find tide data") as ei:
+        Problem(cfg, mesh)
+    assert ei.value.status == 2

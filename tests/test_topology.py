@@ -61,3 +61,32 @@ def test_boundary_lookup_error():
     with pytest.raises(DgswError) as ei:
         mesh_topology(mesh)
     assert ei.value.status == 2
+
+
+def test_tide_and_flow_boundaries_follow_land_in_creation_order(oracle):
+    """Tide and flow faces are boundaries of their own types, created between land and function faces
+    (ProblemBoundaryTypes order Land, Tide, Flow, Function)."""
+    from dgswemv2_b200 import configs
+    from dgswemv2_b200.types import FLOW, TIDE
+
+    mesh, _ = configs.tidal_channel(nx=9, ny=4)
+    a = mesh_topology(mesh)
+    b = _oracle_topology(oracle, mesh)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    types = a[3][:, 2]
+    assert set(types) == {LAND, TIDE, FLOW}
+    assert np.all(np.diff(types) >= 0)  # grouped in type order
+    assert int((types == TIDE).sum()) == 4 and int((types == FLOW).sum()) == 4
+
+
+def test_tide_face_without_data_is_an_error(oracle):
+    """A tide face whose nodes are in no tide block: create_boundaries' "unable to find tide data"."""
+    from dgswemv2_b200 import configs
+
+    mesh, cfg = configs.tidal_channel(nx=6, ny=3, flow=False)
+    mesh.forcing[0].nodes = mesh.forcing[0].nodes[:2]
+    mesh.forcing[0].amplitude = mesh.forcing[0].amplitude[:, :2]
+    mesh.forcing[0].phase = mesh.forcing[0].phase[:, :2]
+    with pytest.raises(RuntimeError, match="unable to find tide data"):
+        oracle.problem(cfg, mesh)
