@@ -106,9 +106,15 @@ def quad_mesh(m, n, corners=((0, 0), (1, 0), (1, 1), (0, 1)), bc=(LAND, LAND, LA
 
 
 def write_adcirc(mesh, path):
-    """Write the mesh as ADCIRC fort.14 (+ nothing for .bcis: land/function/outflow need no data).
-    Boundary chains become land-boundary segments with IBTYPE 0 (land), 77 (function), 88 (outflow)."""
-    ib = {0: 0, 3: 77, 4: 88}
+    """Write the mesh as ADCIRC fort.14. Tide chains become open boundaries; the other chains become
+    land-boundary segments with IBTYPE 0 (land), 2 (flow), 77 (function), 88 (outflow)."""
+    from .types import TIDE
+
+    ib = {0: 0, 2: 2, 3: 77, 4: 88}
+    chains = [(int(mesh.seg_type[s]), mesh.seg_nodes[mesh.seg_offsets[s]:mesh.seg_offsets[s + 1]])
+              for s in range(len(mesh.seg_type))]
+    open_ch = [c for t, c in chains if t == TIDE]
+    land_ch = [(t, c) for t, c in chains if t != TIDE]
     with open(path, "w") as f:
         f.write(mesh.name + "\n")
         f.write("%d    %d\n" % (mesh.n_elems, mesh.n_nodes))
@@ -117,13 +123,38 @@ def write_adcirc(mesh, path):
         ids = mesh.elem_ids if mesh.elem_ids is not None else np.arange(mesh.n_elems)
         for k, (a, b, c) in enumerate(mesh.elem_nodes):
             f.write("%d 3 %d %d %d\n" % (ids[k], a, b, c))
-        f.write("0 = Number of open boundaries\n0 = Total number of open boundary nodes\n")
-        nseg = len(mesh.seg_type)
-        f.write("%d = Number of land boundaries\n" % nseg)
-        f.write("%d = Total number of land boundary nodes\n" % int(mesh.seg_offsets[-1]))
-        for s in range(nseg):
-            chain = mesh.seg_nodes[mesh.seg_offsets[s]:mesh.seg_offsets[s + 1]]
-            f.write("%d %d = Number of nodes for land boundary %d\n" % (len(chain), ib[int(mesh.seg_type[s])], s + 1))
+        f.write("%d = Number of open boundaries\n" % len(open_ch))
+        f.write("%d = Total number of open boundary nodes\n" % sum(len(c) for c in open_ch))
+        for s, chain in enumerate(open_ch):
+            f.write("%d = Number of nodes for open boundary %d\n" % (len(chain), s + 1))
+            for nd in chain:
+                f.write("%d\n" % nd)
+        f.write("%d = Number of land boundaries\n" % len(land_ch))
+        f.write("%d = Total number of land boundary nodes\n" % sum(len(c) for _, c in land_ch))
+        for s, (t, chain) in enumerate(land_ch):
+            f.write("%d %d = Number of nodes for land boundary %d\n" % (len(chain), ib[t], s + 1))
             for nd in chain:
                 f.write("%d\n" % nd)
         f.write("0 = Number of generic boundaries\n0 = Total number of generic boundary nodes\n")
+
+
+def write_bcis(mesh, path):
+    """Write the mesh's tide / flow forcing blocks as a `.bcis` file in the layout SWE::Inputs::read_bcis
+    reads (swe_inputs.cpp:211-290): "type nnodes", the constituent count, then per constituent
+    "frequency forcing_fact equilib_arg" and one "node amplitude phase" line per node."""
+    with open(path, "w") as f:
+        for b in mesh.forcing:
+            nodes = np.asarray(b.nodes)
+            f.write("%d %d = %s boundary\n" % (int(b.type), len(nodes), "tide" if int(b.type) == 1 else "flow"))
+            f.write("%d = number of constituents\n" % len(b.frequency))
+            for c in range(len(b.frequency)):
+                f.write("%.17g %.17g %.17g\n" % (b.frequency[c], b.forcing_fact[c], b.equilib_arg[c]))
+                for j, nd in enumerate(nodes):
+                    f.write("%d %.17g %.17g\n" % (nd, b.amplitude[c][j], b.phase[c][j]))
+
+
+def write_manning(mesh, path):
+    """Write the mesh's Manning n as "node n" lines (the file swe_pre_init_data.hpp:165-182 reads)."""
+    with open(path, "w") as f:
+        for k, n in enumerate(mesh.node_manning_n):
+            f.write("%d %.17g\n" % (k, n))

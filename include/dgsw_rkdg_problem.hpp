@@ -303,8 +303,36 @@ struct AdcircMesh {
     int64_t n_nodes() const { return (int64_t)node_names.size(); }
     int64_t n_elems() const { return (int64_t)elem_names.size(); }
 
-    dgsw_mesh view() const {
+    // SWE::preprocess_mesh_data inputs: Manning's n per node and the .bcis tide / flow blocks
+    std::vector<double> node_manning_n;
+    struct Block {
+        int32_t type = DGSW_BC_TIDE;
+        std::vector<int32_t> nodes;  // indices into node_names
+        std::vector<double> frequency, forcing_fact, equilib_arg;
+        std::vector<double> amplitude, phase;  // [constituent][node]
+    };
+    std::vector<Block> forcing;
+    std::vector<dgsw_forcing_block> forcing_view;
+
+    dgsw_mesh view() {
+        forcing_view.clear();
+        for (const Block& b : forcing) {
+            dgsw_forcing_block f{};
+            f.type = b.type;
+            f.n_nodes = (int32_t)b.nodes.size();
+            f.n_constituents = (int32_t)b.frequency.size();
+            f.nodes = b.nodes.data();
+            f.frequency = b.frequency.data();
+            f.forcing_fact = b.forcing_fact.data();
+            f.equilib_arg = b.equilib_arg.data();
+            f.amplitude = b.amplitude.data();
+            f.phase = b.phase.data();
+            forcing_view.push_back(f);
+        }
         dgsw_mesh m{};
+        m.node_manning_n = node_manning_n.empty() ? nullptr : node_manning_n.data();
+        m.n_forcing = (int32_t)forcing_view.size();
+        m.forcing = forcing_view.empty() ? nullptr : forcing_view.data();
         m.n_nodes = n_nodes();
         m.node_xyz = node_xyz.data();
         m.n_elems = n_elems();
@@ -447,6 +475,103 @@ inline AdcircMesh read_adcirc(const std::string& path) {
     return M;
 }
 
+/* SWE::Inputs::read_bcis (swe_inputs.cpp:211-290): tide and flow blocks, each a "btype nnodes" line, the
+ * constituent count, then per constituent "frequency forcing_fact equilib_arg" and nnodes lines
+ * "node_ID amplitude phase". Levee blocks (nnodes "front back H C_sub C_super" lines) are read past:
+ * internal-barrier boundaries are rejected with the mesh. Other lines are skipped. A missing file gives no
+ * blocks, as in the reference (its existence check is commented out); a tide or flow face without data
+ * then fails in create_boundaries' "unable to find ... data". A node ID the mesh does not have can match
+ * no face and is dropped. Where the reference would append a node listed twice in one constituent to the
+ * same per-node lists (shifting its constituents), or index past a node missing from a constituent, this
+ * reader raises an error instead. */
+inline void read_bcis(const std::string& path, AdcircMesh& M) {
+    std::ifstream file(path);
+    if (!file) return;
+    std::map<uint32_t, int32_t> index;
+    for (size_t i = 0; i < M.node_names.size(); ++i) index[M.node_names[i]] = (int32_t)i;
+    constexpr unsigned levee = DGSW_BC_INTERNAL + 1;
+    std::string line;
+    while (std::getline(file, line)) {
+        std::stringstream head(line);
+        unsigned btype = 0, nnodes = 0;
+        head >> btype >> nnodes;
+        if (btype == DGSW_BC_TIDE || btype == DGSW_BC_FLOW) {
+            AdcircMesh::Block b;
+            b.type = (int32_t)btype;
+            unsigned ncon = 0;
+            std::getline(file, line);
+            std::stringstream(line) >> ncon;
+            std::vector<uint32_t> ids;                                   // first-appearance order
+            std::vector<std::map<uint32_t, std::pair<double, double>>> val(ncon);
+            for (unsigned con = 0; con < ncon; ++con) {
+                double fr = 0, ff = 0, eq = 0;
+                std::getline(file, line);
+                std::stringstream(line) >> fr >> ff >> eq;
+                b.frequency.push_back(fr);
+                b.forcing_fact.push_back(ff);
+                b.equilib_arg.push_back(eq);
+                for (unsigned k = 0; k < nnodes; ++k) {
+                    std::getline(file, line);
+                    std::stringstream st(line);
+                    uint32_t id = 0;
+                    double amp = 0, ph = 0;
+                    st >> id >> amp >> ph;
+                    if (con == 0) ids.push_back(id);
+                    if (!val[con].emplace(id, std::make_pair(amp, ph)).second)
+                        throw std::logic_error("Fatal Error: .bcis block lists node " + std::to_string(id) +
+                                               " twice for one constituent\n");
+                }
+            }
+            std::vector<uint32_t> kept;
+            for (uint32_t id : ids) {
+                auto it = index.find(id);
+                if (it == index.end()) continue;
+                kept.push_back(id);
+                b.nodes.push_back(it->second);
+            }
+            b.amplitude.resize((size_t)ncon * kept.size());
+            b.phase.resize((size_t)ncon * kept.size());
+            for (unsigned con = 0; con < ncon; ++con)
+                for (size_t j = 0; j < kept.size(); ++j) {
+                    auto it = val[con].find(kept[j]);
+                    if (it == val[con].end())
+                        throw std::logic_error("Fatal Error: .bcis node " + std::to_string(kept[j]) +
+                                               " has no data for constituent " + std::to_string(con) + "\n");
+                    b.amplitude[(size_t)con * kept.size() + j] = it->second.first;
+                    b.phase[(size_t)con * kept.size() + j] = it->second.second;
+                }
+            M.forcing.push_back(std::move(b));
+        } else if (btype == levee) {
+            for (unsigned k = 0; k < nnodes; ++k) std::getline(file, line);
+        }
+    }
+}
+
+/* Manning's n (swe_pre_init_data.hpp:165-182): "node_ID n" lines up to the first that does not parse;
+ * a node the file does not list gets n = 0 (the reference's std::map default). */
+inline void read_manning(const std::string& path, AdcircMesh& M) {
+    std::ifstream file(path);
+    if (!file)
+        throw std::logic_error("Fatal Error: manning factor data file " + path + " was not found!\n");
+    std::map<uint32_t, int32_t> index;
+    for (size_t i = 0; i < M.node_names.size(); ++i) index[M.node_names[i]] = (int32_t)i;
+    M.node_manning_n.assign(M.node_names.size(), 0.0);
+    std::string line;
+    while (std::getline(file, line)) {
+        std::istringstream st(line);
+        uint32_t id;
+        double n;
+        if (!(st >> id >> n)) break;
+        auto it = index.find(id);
+        if (it != index.end()) M.node_manning_n[it->second] = n;
+    }
+}
+
+/* a path from the input file, relative to the input file's directory unless absolute */
+inline std::string input_relative(const std::string& dir, const std::string& path) {
+    return (!path.empty() && path[0] == '/') ? path : dir + path;
+}
+
 /* ------------------------------------------------------------------------------------------------ */
 /* input parameters                                                                                 */
 
@@ -465,6 +590,9 @@ struct SWEInputs {
     double h_o = 0.1;
     bool slope_limiting = false;
     double sl_M = 1.0e-8, sl_nu = 1.5;
+    int bottom_friction = DGSW_FRICTION_NONE;  // BottomFrictionType None / Chezy / Manning
+    double friction_coefficient = 0.0;
+    std::string manning_data_file;
 
     SWEInputs() = default;
     /* SWE::Inputs::Inputs (swe_inputs.cpp:4-205): malformed optional nodes warn and keep defaults */
@@ -512,11 +640,21 @@ struct SWEInputs {
             else
                 std::cerr << "Warning: function source is mal-formatted. Using default parameters.\n";
         }
-        if (const YamlNode& bf = n["bottom_friction"]) {
-            if (bf["type"])
-                throw Error(DGSW_ERR_UNSUPPORTED, "bottom friction (" + bf["type"].as<std::string>() +
-                                                      ") is not supported by this build");
-            std::cerr << "Warning: bottom friction is mal-formatted. Using default parameters.\n";
+        if (const YamlNode& bf = n["bottom_friction"]) {  // swe_inputs.cpp:86-123
+            const std::string w = "Warning: bottom friction is mal-formatted. Using default parameters.\n";
+            const std::string t = bf["type"] ? bf["type"].as<std::string>() : std::string();
+            if (t == "Chezy" && bf["coefficient"]) {
+                bottom_friction = DGSW_FRICTION_CHEZY;
+                friction_coefficient = bf["coefficient"].as<double>();
+            } else if (t == "Manning" && bf["coefficient"] && bf["input_file"]) {
+                bottom_friction = DGSW_FRICTION_MANNING;
+                friction_coefficient = bf["coefficient"].as<double>();
+                manning_data_file = bf["input_file"].as<std::string>();
+            } else {
+                std::cerr << w;
+            }
+            if (bottom_friction != DGSW_FRICTION_NONE && friction_coefficient < 0.)
+                throw std::logic_error("Fatal Error: Chezy friction coefficient must be postive!\n");
         }
         if (n["meteo_forcing"] && n["meteo_forcing"]["type"])
             throw Error(DGSW_ERR_UNSUPPORTED, "meteo forcing is not supported by this build");
@@ -734,7 +872,11 @@ struct GpuDiscretization {
     Handle handle;
 
     void initialize(const InputParameters& input) {
-        mesh = read_adcirc(input.input_dir + input.mesh_input.mesh_file_name);
+        mesh = read_adcirc(input_relative(input.input_dir, input.mesh_input.mesh_file_name));
+        // Simulation ctor: input.read_bcis(); initialize_data_serial: the Manning n file
+        read_bcis(input_relative(input.input_dir, input.mesh_input.bc_is_file_name), mesh);
+        if (input.problem_input.bottom_friction == DGSW_FRICTION_MANNING)
+            read_manning(input_relative(input.input_dir, input.problem_input.manning_data_file), mesh);
         dgsw_config_default(&config);
         const SWEInputs& pi = input.problem_input;
         config.p = (int32_t)input.polynomial_order;
@@ -758,6 +900,9 @@ struct GpuDiscretization {
         config.spherical = pi.spherical;
         config.sp_lat0_deg = pi.latitude_o;
         config.sp_R = pi.R;
+        config.bottom_friction = pi.bottom_friction;
+        config.friction_cf = pi.friction_coefficient;
+        config.ramp_duration = input.stepper_input.ramp_duration;
         config.precision = input.b200.precision;
         config.device = input.b200.device;
         config.tile = input.b200.tile;
@@ -827,7 +972,8 @@ struct GpuProblem {
      * handle's configuration instead of process-wide statics */
     static void initialize_problem_parameters(const ProblemInputType&) {}
 
-    /* SWE::preprocess_mesh_data: .bcis forcing data (tide, flow, levee) is not supported */
+    /* SWE::preprocess_mesh_data: the spherical projection is applied by the library; the .bcis tide / flow
+     * data and the Manning n file are read when the discretization is initialised (GpuDiscretization) */
     static void preprocess_mesh_data(ProblemInputParametersType&) {}
 
     /* swe_pre_serial.hpp: initial projections, wet/dry and limiter initialisation on the device */

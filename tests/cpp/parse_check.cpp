@@ -44,8 +44,26 @@ int main(int argc, char** argv) {
                   << in.writer_input.modal_output_freq_step << "\n"
                   << "function_set " << in.b200.function_set << "\n"
                   << "precision " << in.b200.precision << "\n"
-                  << "n_params " << in.b200.function_parameters.size() << "\n";
-        const dgsw::AdcircMesh M = dgsw::read_adcirc(in.input_dir + in.mesh_input.mesh_file_name);
+                  << "n_params " << in.b200.function_parameters.size() << "\n"
+                  << "bottom_friction " << pi.bottom_friction << " " << pi.friction_coefficient << "\n"
+                  << "manning_file " << pi.manning_data_file << "\n"
+                  << "ramp_duration " << in.stepper_input.ramp_duration << "\n";
+        dgsw::AdcircMesh M = dgsw::read_adcirc(dgsw::input_relative(in.input_dir, in.mesh_input.mesh_file_name));
+        dgsw::read_bcis(dgsw::input_relative(in.input_dir, in.mesh_input.bc_is_file_name), M);
+        if (pi.bottom_friction == DGSW_FRICTION_MANNING)
+            dgsw::read_manning(dgsw::input_relative(in.input_dir, pi.manning_data_file), M);
+        std::cout << "n_forcing " << M.forcing.size() << "\n";
+        for (size_t b = 0; b < M.forcing.size(); ++b) {
+            const auto& F = M.forcing[b];
+            std::cout << "forcing_" << b << " " << F.type << " " << F.nodes.size() << " " << F.frequency.size() << " "
+                      << fnv(F.nodes.data(), F.nodes.size() * 4) << " "
+                      << fnv(F.frequency.data(), F.frequency.size() * 8,
+                             fnv(F.forcing_fact.data(), F.forcing_fact.size() * 8,
+                                 fnv(F.equilib_arg.data(), F.equilib_arg.size() * 8)))
+                      << " " << fnv(F.amplitude.data(), F.amplitude.size() * 8) << " "
+                      << fnv(F.phase.data(), F.phase.size() * 8) << "\n";
+        }
+        std::cout << "manning_hash " << fnv(M.node_manning_n.data(), M.node_manning_n.size() * 8) << "\n";
         std::cout << "mesh_name " << M.name << "\n"
                   << "n_nodes " << M.n_nodes() << "\n"
                   << "n_elems " << M.n_elems() << "\n"

@@ -173,8 +173,9 @@ def test_parse_bowl_style_input(parse_check, tmp_path):
     (lambda s: s.replace("  dt: 1.0\n", ""), "-1", "Timestepping YAML node is malformatted"),
     (lambda s: s.replace("format: Adcirc", "format: Gmsh"), "-1", "Unsupported mesh format: Gmsh"),
     (lambda s: s.replace("cartesian", "conic"), "-1", "Unsupported coordinate system: conic"),
-    (lambda s: s.replace("  function_source: Enable\n", "  bottom_friction:\n    type: Chezy\n    coefficient: 0.1\n"),
-     "5", "bottom friction"),
+    (lambda s: s.replace("  function_source: Enable\n", "  bottom_friction:\n    type: Chezy\n    coefficient: -0.1\n"),
+     "-1", "Chezy friction coefficient must be postive"),
+    (lambda s: s.replace("  function_source: Enable\n", "  meteo_forcing:\n    type: Enable\n"), "5", "meteo forcing"),
     (lambda s: s.replace("function_set: manufactured_sine", "function_set: tsunami"), "-1", "unknown b200.function_set"),
     (lambda s: s.replace("name: rkdg_swe", "name: ehdg_swe"), "5", "is not rkdg_swe"),
 ])
@@ -224,3 +225,120 @@ def test_serial_driver_runs_config1(tmp_path, oracle):
     P = Problem(cfg, mesh)
     P.step_serial(1000)
     assert abs(P.compute_residual_L2() - l2_cli) <= 1e-13 * l2_ref
+
+
+TIDE_15 = """mesh:
+  format: Adcirc
+  file_name: @MESH@
+  coordinate_system: cartesian
+
+timestepping:
+  start_time: 01-01-2000 00:00:00
+  end_time: 01-01-2000 00:05:00
+  dt: 1.0
+  order: 3
+  nstages: 3
+  ramp_duration: 0.01
+
+polynomial_order: 2
+
+problem:
+  name: rkdg_swe
+  gravity: 9.81
+  bottom_friction:
+    type: Manning
+    coefficient: 0.0005
+    input_file: manning.dat
+  initial_conditions:
+    type: Constant
+    initial_surface_height: 0.0
+    initial_momentum_x: 0.0
+    initial_momentum_y: 0.0
+
+output:
+  path: out/
+  modal:
+    frequency: 300
+"""
+
+
+def write_tide_input(d, mesh):
+    path = write_input(d, mesh, TIDE_15, mesh_name="channel.14")
+    meshgen.write_bcis(mesh, os.path.join(d, "channel.bcis"))
+    meshgen.write_manning(mesh, os.path.join(d, "manning.dat"))
+    return path
+
+
+def test_parse_tide_flow_and_manning_input(parse_check, tmp_path):
+    """Open boundaries read as tide, IBTYPE 2 as flow; the .bcis blocks, the Manning n file, bottom
+    friction and the ramp duration come through bit for bit."""
+    mesh, cfg = configs.tidal_channel(p=2, rk=(3, 3), dt=1.0, friction="manning", cf=0.0005)
+    rc, out, err = run_check(parse_check, write_tide_input(str(tmp_path), mesh))
+    assert rc == 0, (out, err)
+    assert out["bottom_friction"] == "2 0.00050000000000000001" and out["manning_file"] == "manning.dat"
+    assert float(out["ramp_duration"]) == 0.01
+    assert out["n_forcing"] == "2"
+    for k, b in enumerate(mesh.forcing):
+        fields = out["forcing_%d" % k].split()
+        assert fields[:3] == [str(b.type), str(len(b.nodes)), str(len(b.frequency))]
+        assert fields[3] == fnv(np.asarray(b.nodes, np.int32))
+        h = fnv(np.asarray(b.equilib_arg, np.float64))
+        h2 = int(h)
+        for arr in (np.asarray(b.forcing_fact, np.float64), np.asarray(b.frequency, np.float64)):
+            for byte in arr.tobytes():
+                h2 = ((h2 ^ byte) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+        assert fields[4] == str(h2)
+        assert fields[5] == fnv(np.asarray(b.amplitude, np.float64)) and fields[6] == fnv(np.asarray(b.phase, np.float64))
+    assert out["manning_hash"] == fnv(np.asarray(mesh.node_manning_n, np.float64))
+    nbr, bt, intf, bnd = mesh_topology(mesh)
+    assert out["boundaries_hash"] == fnv(bnd)
+
+
+def test_bcis_reader_skips_levees_and_unknown_nodes(parse_check, tmp_path):
+    """A levee block is read past, a node ID the mesh lacks is dropped, and a node listed twice for one
+    constituent is an error (the reference would shift that node's constituents)."""
+    mesh, cfg = configs.tidal_channel(friction="manning", cf=0.0005)
+    path = write_tide_input(str(tmp_path), mesh)
+    bpath = os.path.join(str(tmp_path), "channel.bcis")
+    b = mesh.forcing[0]
+    n_tide = len(b.nodes)
+    lines = open(bpath).read().split("\n")
+    flow_block = "\n".join(lines[2 + len(b.frequency) * (1 + n_tide):])
+    tide = ["1 %d = tide boundary" % (n_tide + 1), "%d" % len(b.frequency)]
+    for c in range(len(b.frequency)):
+        tide.append("%.17g %.17g %.17g" % (b.frequency[c], b.forcing_fact[c], b.equilib_arg[c]))
+        tide += ["%d %.17g %.17g" % (nd, b.amplitude[c][j], b.phase[c][j]) for j, nd in enumerate(b.nodes)]
+        tide.append("99999 1.0 2.0")
+    levee = "129 2 = levee\n5 6 1.0 0.5 0.5\n7 8 1.0 0.5 0.5\n"
+    open(bpath, "w").write(levee + "\n".join(tide) + "\n" + flow_block)
+    rc, out, err = run_check(parse_check, path)
+    assert rc == 0, (out, err)
+    assert out["n_forcing"] == "2"
+    fields = out["forcing_0"].split()
+    assert fields[:3] == ["1", str(n_tide), str(len(b.frequency))]
+    assert fields[5] == fnv(np.asarray(b.amplitude, np.float64))
+    dup = tide[:3] + tide[3:4] + tide[3:]
+    open(bpath, "w").write("\n".join(dup) + "\n")
+    rc, out, _ = run_check(parse_check, path)
+    assert rc == 3 and "twice" in out["error"]
+
+
+@pytest.mark.gpu
+def test_serial_driver_runs_tidal_channel(tmp_path):
+    """dgswemv2-b200-serial on a tidal channel input (tide + flow from the .bcis file, Manning n from its
+    file, ramp): the modal output after 300 steps equals the Python API's state bit for bit."""
+    mesh, cfg = configs.tidal_channel(p=2, rk=(3, 3), dt=1.0, friction="manning", cf=0.0005)
+    d = str(tmp_path)
+    path = write_tide_input(d, mesh)
+    os.makedirs(os.path.join(d, "out"), exist_ok=True)
+    r = subprocess.run([CLI, path], capture_output=True, text=True, timeout=300, cwd=d)
+    assert r.returncode == 0, r.stdout + r.stderr
+    P = Problem(cfg, mesh)
+    P.step_serial(300)
+    q = P.get_state()
+    lines = open(os.path.join(d, "out", "modal_ze.txt")).read().split("\n")
+    t_idx = [i for i, l in enumerate(lines) if l and len(l.split()) == 1]
+    last = lines[t_idx[-1] + 1: t_idx[-1] + 1 + mesh.n_elems]
+    ze = np.array([[float(v) for v in l.split()[1:]] for l in last])
+    assert abs(float(lines[t_idx[-1]]) - 300.0) < 1e-9
+    assert np.allclose(ze, q[:, 0, :], rtol=1e-14, atol=1e-15)
