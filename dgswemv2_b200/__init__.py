@@ -80,6 +80,12 @@ def _mesh_struct(mesh):
     keep.append(fkeep)
     m.n_forcing = nf
     m.forcing = arr
+    nl, lp, ld = _lib.levee_arrays(mesh)
+    if nl:
+        keep += [lp, ld]
+        m.n_levee_pairs = nl
+        m.levee_nodes = _lib.ptr(lp, C.c_int32)
+        m.levee_data = _lib.ptr(ld, C.c_double)
     return m, keep
 
 

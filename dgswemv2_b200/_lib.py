@@ -95,6 +95,9 @@ class Mesh(C.Structure):
         ("node_manning_n", C.POINTER(C.c_double)),
         ("n_forcing", C.c_int32),
         ("forcing", C.POINTER(ForcingBlock)),
+        ("n_levee_pairs", C.c_int32),
+        ("levee_nodes", C.POINTER(C.c_int32)),
+        ("levee_data", C.POINTER(C.c_double)),
     ]
 
 
@@ -124,6 +127,18 @@ def forcing_blocks(mesh, block_type=None):
         arr[k].phase = ptr(ph, C.c_double)
     keep.append(arr)
     return (arr if blocks else None), len(blocks), keep
+
+
+def levee_arrays(mesh):
+    """(n, front/back node pairs, data) of the mesh's .bcis levee lines, as contiguous arrays or Nones."""
+    pairs = getattr(mesh, "levee_pairs", None)
+    if pairs is None or len(pairs) == 0:
+        return 0, None, None
+    pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 2)
+    data = np.ascontiguousarray(mesh.levee_data, np.float64).reshape(-1, 3)
+    if data.shape[0] != pairs.shape[0]:
+        raise ValueError("levee_data needs one (H, C_sub, C_super) row per levee pair")
+    return pairs.shape[0], pairs, data
 
 
 class Info(C.Structure):

@@ -158,3 +158,40 @@ def tidal_channel(nx=24, ny=6, p=1, rk=(2, 2), dt=2.0, friction="chezy", cf=0.00
     cfg = ProblemConfig(p=p, rk_nstages=rk[0], rk_order=rk[1], dt=dt, g=9.81, ic_type=0, ic_const=(0.0, 0.0, 0.0),
                         bottom_friction=kind, friction_cf=cf, ramp_duration=ramp_days, precision=precision)
     return mesh, cfg
+
+
+def levee_channel(nx=24, ny=6, p=1, rk=(2, 2), dt=1.0, crest=0.1, c_sub=0.8, c_super=0.6, dry_right=False,
+                  friction="chezy", cf=0.0025, ramp_days=0.005, precision="fp64", jitter=0.1, seed=4,
+                  length=10000.0, width=2000.0, depth=10.0):
+    """The tidal channel cut across its middle by a levee (an internal barrier of coincident but distinct
+    nodes) with crest elevation `crest` and discharge coefficients c_sub / c_super: the tide (M2 + K1) on
+    x = 0 overtops it into the right half. dry_right: the right half is land 0.05 m above datum (with
+    wetting/drying, h_o = 0.01 m) that the overtopping floods; else it is 0.6 `depth` deep with a
+    river flow on x = length."""
+    def bath(x, y):
+        b = depth - 0.4 * depth * x / length
+        return np.where(x > length / 2 + 1e-9, -0.05, b) if dry_right else b
+
+    right_bc = LAND if dry_right else FLOW
+    mesh = meshgen.barrier_channel(nx, ny, length, width, bc_left=TIDE, bc_right=right_bc, jitter=jitter, seed=seed,
+                                   bathymetry=bath, name="levee_channel_%dx%d" % (nx, ny))
+    x, y = mesh.node_xyz[:, 0], mesh.node_xyz[:, 1]
+    left = mesh.seg_nodes[mesh.seg_offsets[2]:mesh.seg_offsets[3]]
+    yl = y[left] / width
+    forcing = [ForcingBlock(TIDE, left, np.array([M2_FREQ, K1_FREQ]), np.array([1.0, 0.9]), np.array([30.0, 120.0]),
+                            np.stack([0.4 + 0.1 * yl, 0.15 + 0.0 * yl]), np.stack([10.0 + 20.0 * yl, 50.0 + 0.0 * yl]))]
+    if not dry_right:
+        right = mesh.seg_nodes[mesh.seg_offsets[4]:mesh.seg_offsets[5]]
+        forcing.append(ForcingBlock(FLOW, right, np.array([0.0]), np.array([1.0]), np.array([0.0]),
+                                    np.full((1, len(right)), -0.2), np.zeros((1, len(right)))))
+    mesh.forcing = forcing
+    npair = len(mesh.levee_pairs)
+    yb = y[mesh.levee_pairs[:, 0]] / width
+    mesh.levee_data = np.stack([crest + 0.05 * yb, np.full(npair, c_sub), np.full(npair, c_super)], 1)
+    kind = {None: FRICTION_NONE, "chezy": FRICTION_CHEZY, "manning": FRICTION_MANNING}[friction]
+    if kind == FRICTION_MANNING:
+        mesh.node_manning_n = 0.02 + 0.01 * x / length
+    cfg = ProblemConfig(p=p, rk_nstages=rk[0], rk_order=rk[1], dt=dt, g=9.81, ic_type=0, ic_const=(0.0, 0.0, 0.0),
+                        bottom_friction=kind, friction_cf=cf, ramp_duration=ramp_days, precision=precision,
+                        wetting_drying=dry_right, h_o=0.01)
+    return mesh, cfg

@@ -20,6 +20,7 @@
 #include "reduce_kernels.cuh"
 #include "stage_kernel.cuh"
 #include "trouble.cuh"
+#include "levee.cuh"
 
 using namespace dgsw;
 
@@ -108,6 +109,10 @@ struct dgsw_rkdg_s {
     Forcing forcing;
     DBuf<int2> fface;      // tide / flow forcing records
     DBuf<double> fcon;
+    int64_t n_levee = 0;   // levee interfaces
+    DBuf<int4> lev;        // in element, in face, ex element, ex face (device order)
+    DBuf<double> ldat;     // normal, crest height and coefficients at the Gauss points, spherical factors
+    DBuf<double> levF;     // this stage's levee fluxes
     DBuf<int2> halo;
     DBuf<int> tile_halo_off;
     DBuf<int> enodes, tile_edge_off, ref_of_dev;
@@ -243,6 +248,22 @@ cudaError_t launch_stage(dgsw_rkdg_s* h, int s) {
     fill_stage_args<Real>(h, s, A);
     A.wet_in = h->wet[h->wet_cur].p;
     A.wet_out = h->wet[1 - h->wet_cur].p;
+    if (h->n_levee) {
+        // the levee interfaces' fluxes of this stage, ahead of the stage kernel that lifts them
+        LeveeArgs<Real> L;
+        L.q = (const double*)h->Q[s];
+        L.bath = (const Real*)h->bath;
+        L.wet = A.wet_in;
+        L.lev = h->lev.p;
+        L.ldat = h->ldat.p;
+        L.F = h->levF.p;
+        L.n = (int)h->n_levee;
+        L.ne_pad = (int)h->ne_pad;
+        L.g = h->cfg.g;
+        cudaError_t e = launch_levee<Real>(L, h->cfg.p, h->stream);
+        if (e != cudaSuccess) return e;
+        A.levF = h->levF.p;
+    }
     const int mode = (h->cfg.wetting_drying ? 1 : 0) | (h->cfg.function_source ? 2 : 0) |
                      (h->cfg.bottom_friction != DGSW_FRICTION_NONE ? 4 : 0);
     return launch_stage_any(h, A, mode);
@@ -335,7 +356,7 @@ __global__ void record_labels_kernel(const unsigned char* limited, const int* re
 cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageRecord* rec = nullptr) {
     cudaError_t e = h->fp32 ? launch_stage<float>(h, s) : launch_stage<double>(h, s);
     if (e != cudaSuccess) return e;
-    ++launches;
+    launches += h->n_levee ? 2 : 1;
     h->wet_cur = 1 - h->wet_cur;
     int s_out = s + 1;
     if (s + 1 == h->ns) {
@@ -726,6 +747,31 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
             upload_real(h->manning, mdev);
             h->device_bytes += (int64_t)h->ne_pad * h->real_size;
         }
+        static_assert(LEVEE_STRIDE == LEVEE_STRIDE_DEV, "levee record layout");
+        {
+            std::vector<double> ld;
+            std::string e2;
+            const int lrc = build_levees(mesh, h->topo, cfg->p, h->node_xyz.data(), *cfg, ld, e2);
+            if (lrc) {
+                dgsw_rkdg_destroy(h);
+                return fail(lrc, e2);
+            }
+            h->n_levee = (int64_t)h->topo.intf.size() / 4 - h->topo.n_intf_internal;
+            if (h->n_levee) {
+                std::vector<int4> lv(h->n_levee);
+                for (int64_t l = 0; l < h->n_levee; ++l) {
+                    const int32_t* I = &h->topo.intf[4 * (h->topo.n_intf_internal + l)];
+                    lv[l] = make_int4(h->tiling.dev_of_ref[I[0]], I[2], h->tiling.dev_of_ref[I[1]], I[3]);
+                }
+                if ((e = h->lev.alloc(h->n_levee)) != cudaSuccess || (e = h->ldat.alloc(ld.size())) != cudaSuccess ||
+                    (e = h->levF.alloc((size_t)h->n_levee * 6 * MAX_NG)) != cudaSuccess)
+                    return cleanup_fail("alloc", e);
+                cudaMemcpy(h->lev.p, lv.data(), lv.size() * sizeof(int4), cudaMemcpyHostToDevice);
+                cudaMemcpy(h->ldat.p, ld.data(), ld.size() * sizeof(double), cudaMemcpyHostToDevice);
+                cudaMemset(h->levF.p, 0, (size_t)h->n_levee * 6 * MAX_NG * sizeof(double));
+                h->device_bytes += (int64_t)(lv.size() * 16 + ld.size() * 8 + h->n_levee * 6 * MAX_NG * 8);
+            }
+        }
         static_assert(FORCE_STRIDE == FORCE_STRIDE_DEV, "forcing record layout");
         const size_t nff = h->forcing.face.size() / 2, nfc = h->forcing.con.size();
         if (nff) {
@@ -1090,6 +1136,9 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     if (h->manning) cudaFree(h->manning);
     h->fface.release();
     h->fcon.release();
+    h->lev.release();
+    h->ldat.release();
+    h->levF.release();
     h->halo.release();
     h->tile_halo_off.release();
     h->enodes.release();

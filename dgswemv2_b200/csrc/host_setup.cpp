@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <numeric>
 #include <unordered_map>
 
@@ -232,22 +233,53 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
     T.nbr.assign(3 * ne, -1);
     T.nbr_face.assign(3 * ne, -1);
     T.btype.assign(3 * ne, 255);
-    // boundary chain lookup: first occurrence of each node in each chain
-    std::unordered_map<uint64_t, int64_t> first_pos;
-    for (int32_t s = 0; s < m->n_segments; ++s)
-        for (int64_t i = m->seg_offsets[s]; i < m->seg_offsets[s + 1]; ++i) {
-            uint64_t k = (uint64_t)(uint32_t)s << 32 | (uint32_t)m->seg_nodes[i];
-            if (!first_pos.count(k)) first_pos[k] = i;
+    // boundary chain lookup (AdcircFormat::get_ibtype, adcirc_format.cpp:214-259): the first chain, in
+    // the given order, in which the face's two nodes are consecutive (has_edge looks at every occurrence
+    // of the first node); a levee chain holds its front and back node strings, searched separately
+    // (:230-234); faces joining the two strings at a barrier end are land (is_levee_end, :338-352)
+    auto ukey = [](int32_t a, int32_t b) -> uint64_t {
+        return (uint64_t)(uint32_t)std::min(a, b) << 32 | (uint32_t)std::max(a, b);
+    };
+    std::unordered_map<uint64_t, int32_t> edge_seg;   // node pair -> first chain holding it
+    std::unordered_map<uint64_t, uint64_t> mirror;    // levee node pair -> node pair across the barrier
+    std::unordered_map<uint64_t, int> levee_end;
+    for (int32_t s = 0; s < m->n_segments; ++s) {
+        const int64_t b = m->seg_offsets[s], e = m->seg_offsets[s + 1];
+        for (int64_t i = b; i < e; ++i)
+            if (m->seg_nodes[i] < 0 || m->seg_nodes[i] >= m->n_nodes) {
+                err = "Fatal Error: boundary node index out of range";
+                return DGSW_ERR_MESH;
+            }
+        if (m->seg_type[s] == DGSW_BC_LEVEE) {
+            const int64_t n = (e - b) / 2;
+            if ((e - b) % 2 != 0 || n < 2) {
+                err = "levee chain " + std::to_string(s) + " must hold n >= 2 front nodes followed by n back nodes";
+                return DGSW_ERR_INVALID_ARGUMENT;
+            }
+            const int32_t* fr = m->seg_nodes + b;
+            const int32_t* bk = m->seg_nodes + b + n;
+            for (int64_t i = 0; i + 1 < n; ++i) edge_seg.emplace(ukey(fr[i], fr[i + 1]), s);
+            for (int64_t i = 0; i + 1 < n; ++i) edge_seg.emplace(ukey(bk[i], bk[i + 1]), s);
+            // AdcircFormat::get_internal_node_pair (:261-318): front pair <-> back pair
+            for (int64_t i = 0; i + 1 < n; ++i) mirror.emplace(ukey(fr[i], fr[i + 1]), ukey(bk[i], bk[i + 1]));
+            for (int64_t i = 0; i + 1 < n; ++i) mirror.emplace(ukey(bk[i], bk[i + 1]), ukey(fr[i], fr[i + 1]));
+            levee_end.emplace(ukey(fr[0], bk[0]), 1);
+            levee_end.emplace(ukey(fr[n - 1], bk[n - 1]), 1);
+        } else {
+            for (int64_t i = b; i + 1 < e; ++i) edge_seg.emplace(ukey(m->seg_nodes[i], m->seg_nodes[i + 1]), s);
         }
+    }
     auto lookup_type = [&](int32_t n0, int32_t n1) -> int {
-        for (int32_t s = 0; s < m->n_segments; ++s) {
-            auto it = first_pos.find((uint64_t)(uint32_t)s << 32 | (uint32_t)n0);
-            if (it == first_pos.end()) continue;
-            int64_t i = it->second;
-            if (i + 1 < m->seg_offsets[s + 1] && m->seg_nodes[i + 1] == n1) return m->seg_type[s];
-            if (i > m->seg_offsets[s] && m->seg_nodes[i - 1] == n1) return m->seg_type[s];
-        }
+        auto it = edge_seg.find(ukey(n0, n1));
+        if (it != edge_seg.end()) return m->seg_type[it->second];
+        if (levee_end.count(ukey(n0, n1))) return DGSW_BC_LAND;
         return -1;
+    };
+    // levee faces: the element across the barrier (first element holding the mirrored edge)
+    std::vector<int32_t> lev_nbr(3 * ne, -1);
+    auto first_holder = [&](uint64_t key) -> int32_t {
+        auto it = std::lower_bound(fk.begin(), fk.end(), key, [](const FK& x, uint64_t k) { return x.key < k; });
+        return (it != fk.end() && it->key == key) ? it->r : -1;
     };
     for (size_t i = 0; i < fk.size();) {
         size_t j = i + 1;
@@ -279,43 +311,73 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
                 return DGSW_ERR_MESH;
             }
             if (bt != DGSW_BC_LAND && bt != DGSW_BC_TIDE && bt != DGSW_BC_FLOW && bt != DGSW_BC_FUNCTION &&
-                bt != DGSW_BC_OUTFLOW) {
+                bt != DGSW_BC_OUTFLOW && bt != DGSW_BC_LEVEE) {
                 err = "unsupported boundary type " + std::to_string(bt);
                 return DGSW_ERR_UNSUPPORTED;
             }
             T.btype[3 * A.r + A.f] = (uint8_t)bt;
+            if (bt == DGSW_BC_LEVEE) {
+                const int32_t across = first_holder(mirror.at(ukey(n0, n1)));
+                if (across < 0) {
+                    err = "Fatal Error: no element across the barrier from node pair (" + std::to_string(n0) + ", " +
+                          std::to_string(n1) + ")";
+                    return DGSW_ERR_MESH;
+                }
+                lev_nbr[3 * A.r + A.f] = across;
+            }
         }
         i = j;
     }
+    // levee interfaces pair the raw boundaries keyed (element, element across) with their mirror image
+    // (swe_pre_create_intface.hpp:38-78); a key seen twice keeps its first face, as std::map::emplace does
+    for (int64_t r = 0; r < ne; ++r)
+        for (int f = 0; f < 3; ++f) {
+            const int32_t b = lev_nbr[3 * r + f];
+            if (b < 0) continue;
+            bool first = true;
+            for (int g = 0; g < f; ++g) first = first && lev_nbr[3 * r + g] != b;
+            int fb = -1;
+            for (int g = 0; g < 3 && fb < 0; ++g)
+                if (lev_nbr[3 * (int64_t)b + g] == (int32_t)r) fb = g;
+            if (first && fb >= 0) {
+                T.nbr[3 * r + f] = b;
+                T.nbr_face[3 * r + f] = (int8_t)fb;
+            }
+        }
     // two faces of one element against the same neighbour would collide in the reference's
-    // (element, neighbour) keyed map; reject such meshes
+    // (element, neighbour) keyed maps; reject such meshes
     for (int64_t r = 0; r < ne; ++r)
         for (int f = 0; f < 3; ++f)
             for (int g = f + 1; g < 3; ++g)
-                if (T.nbr[3 * r + f] >= 0 && T.nbr[3 * r + f] == T.nbr[3 * r + g]) {
+                if (T.nbr[3 * r + f] >= 0 && T.nbr[3 * r + f] == T.nbr[3 * r + g] &&
+                    T.btype[3 * r + f] == T.btype[3 * r + g]) {
                     err = "Fatal Error: two elements share more than one edge";
                     return DGSW_ERR_MESH;
                 }
-    // interfaces in (in, ex) order, in = smaller reference ID (swe_pre_create_intface.hpp:14-34)
+    // interfaces in (in, ex) order, in = smaller reference ID (swe_pre_create_intface.hpp:14-34): the
+    // internal ones, then the levee ones (ProblemInterfaceTypes order)
     T.intf.clear();
     std::vector<int64_t> intf_of_face(3 * ne, -1);
-    for (int64_t r = 0; r < ne; ++r) {
-        // faces of r with a larger neighbour, ordered by the neighbour
-        int fs[3], n = 0;
-        for (int f = 0; f < 3; ++f)
-            if (T.nbr[3 * r + f] > r) fs[n++] = f;
-        std::sort(fs, fs + n, [&](int a, int b) { return T.nbr[3 * r + a] < T.nbr[3 * r + b]; });
-        for (int k = 0; k < n; ++k) {
-            int f = fs[k];
-            int32_t e = T.nbr[3 * r + f];
-            int fe = T.nbr_face[3 * r + f];
-            int64_t idx = (int64_t)T.intf.size() / 4;
-            T.intf.push_back((int32_t)r);
-            T.intf.push_back(e);
-            T.intf.push_back(f);
-            T.intf.push_back(fe);
-            intf_of_face[3 * r + f] = idx;
-            intf_of_face[3 * (int64_t)e + fe] = idx;
+    for (int kind : {(int)DGSW_BC_INTERNAL, (int)DGSW_BC_LEVEE}) {
+        if (kind == DGSW_BC_LEVEE) T.n_intf_internal = (int64_t)T.intf.size() / 4;
+        for (int64_t r = 0; r < ne; ++r) {
+            // faces of r with a larger neighbour, ordered by the neighbour
+            int fs[3], n = 0;
+            for (int f = 0; f < 3; ++f)
+                if (T.nbr[3 * r + f] > r && T.btype[3 * r + f] == kind) fs[n++] = f;
+            std::sort(fs, fs + n, [&](int a, int b) { return T.nbr[3 * r + a] < T.nbr[3 * r + b]; });
+            for (int k = 0; k < n; ++k) {
+                int f = fs[k];
+                int32_t e = T.nbr[3 * r + f];
+                int fe = T.nbr_face[3 * r + f];
+                int64_t idx = (int64_t)T.intf.size() / 4;
+                T.intf.push_back((int32_t)r);
+                T.intf.push_back(e);
+                T.intf.push_back(f);
+                T.intf.push_back(fe);
+                intf_of_face[3 * r + f] = idx;
+                intf_of_face[3 * (int64_t)e + fe] = idx;
+            }
         }
     }
     // boundaries grouped by type (Land, Tide, Flow, Function tuple order), each by (element, face)
@@ -498,7 +560,10 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
                     const int fin = T.intf[4 * ii + 2], fex = T.intf[4 * ii + 3];
                     te.push_back(trace_slot(in, fin));
                     te.push_back(trace_slot(ex, fex));
-                    te.push_back(fin | fex << 2 | EK_INTERIOR << 4);
+                    // levee interfaces carry their index among the levee interfaces above bit 8
+                    const bool lev = ii >= T.n_intf_internal;
+                    te.push_back(lev ? (fin | fex << 2 | EK_LEVEE << 4 | (int32_t)(ii - T.n_intf_internal) << 8)
+                                     : (fin | fex << 2 | EK_INTERIOR << 4));
                     te.push_back(out.dev_of_ref[in]);
                     double nx, ny, sJ;
                     face_geometry(X, &T.enodes[3 * (int64_t)in], fin, nx, ny, sJ);
@@ -628,6 +693,67 @@ int build_forcing(const dgsw_mesh* m, Topology& T, int p, Forcing& out, std::str
                 rec[3 + MAX_NG + g] = B.phase[row + p0] * N1 + B.phase[row + p1] * N2;
             }
             out.con.insert(out.con.end(), rec, rec + FORCE_STRIDE);
+        }
+    }
+    return DGSW_OK;
+}
+
+int build_levees(const dgsw_mesh* m, const Topology& T, int p, const double* X, const dgsw_config& cfg,
+                 std::vector<double>& out, std::string& err) {
+    out.clear();
+    const int64_t n_lev = (int64_t)T.intf.size() / 4 - T.n_intf_internal;
+    if (n_lev <= 0) return DGSW_OK;
+    if (n_lev >= ((int64_t)1 << 23)) {
+        err = "too many levee interfaces";
+        return DGSW_ERR_UNSUPPORTED;
+    }
+    if (m->n_levee_pairs < 0 || (m->n_levee_pairs > 0 && (!m->levee_nodes || !m->levee_data))) {
+        err = "invalid levee pair list";
+        return DGSW_ERR_INVALID_ARGUMENT;
+    }
+    // levee_is_data: keyed by the ordered (front, back) pair; a repeated key keeps the last line
+    std::map<std::pair<int32_t, int32_t>, int32_t> data;
+    for (int32_t k = 0; k < m->n_levee_pairs; ++k) data[{m->levee_nodes[2 * k], m->levee_nodes[2 * k + 1]}] = k;
+    const Rule1D gl = gauss_legendre_degree(2 * p + 1);
+    const int ng = (int)gl.z.size();
+    const double cos_lat0 = std::cos(cfg.sp_lat0_deg * M_PI / 180.0);
+    out.assign((size_t)LEVEE_STRIDE * n_lev, 0.0);
+    for (int64_t l = 0; l < n_lev; ++l) {
+        const int64_t i = T.n_intf_internal + l;
+        const int32_t in = T.intf[4 * i], ex = T.intf[4 * i + 1], fin = T.intf[4 * i + 2], fex = T.intf[4 * i + 3];
+        const int32_t ni[2] = {T.enodes[3 * (int64_t)in + (fin + 1) % 3], T.enodes[3 * (int64_t)in + (fin + 2) % 3]};
+        const int32_t nx_[2] = {T.enodes[3 * (int64_t)ex + (fex + 1) % 3], T.enodes[3 * (int64_t)ex + (fex + 2) % 3]};
+        double v[3][2];
+        for (int k = 0; k < 2; ++k) {
+            auto it = data.find({ni[k], nx_[1 - k]});
+            if (it == data.end()) it = data.find({nx_[1 - k], ni[k]});
+            if (it == data.end()) {
+                err = "Fatal Error: unable to find levee data!";
+                return DGSW_ERR_MESH;
+            }
+            for (int c = 0; c < 3; ++c) v[c][k] = m->levee_data[3 * (int64_t)it->second + c];
+        }
+        double* o = &out[(size_t)LEVEE_STRIDE * l];
+        double nx, ny, sJ;
+        face_geometry(X, &T.enodes[3 * (int64_t)in], fin, nx, ny, sJ);
+        o[0] = nx;
+        o[1] = ny;
+        for (int g = 0; g < ng; ++g) {
+            // ComputeBoundaryNodalUgpIN: (1 - z)/2, (1 + z)/2 on the in side's face nodes
+            const double N1 = (1.0 - gl.z[g]) / 2.0, N2 = (1.0 + gl.z[g]) / 2.0;
+            for (int c = 0; c < 3; ++c) o[2 + c * MAX_NG + g] = v[c][0] * N1 + v[c][1] * N2;
+        }
+        // spherical correction at the in side's Gauss points, for both sides: the ex side's value at its
+        // Gauss point ng-1-g is the in side's at g (swe_pre_init_data.hpp:80-101)
+        for (int g = 0; g < ng; ++g) {
+            double sp = 1.0;
+            if (cfg.spherical) {
+                const double wa = (1.0 - gl.z[g]) / 2.0, wb = (1.0 + gl.z[g]) / 2.0;
+                const double y = X[3 * (int64_t)ni[0] + 1] * wa + X[3 * (int64_t)ni[1] + 1] * wb;
+                sp = cos_lat0 / std::cos(y / cfg.sp_R);
+            }
+            o[2 + 3 * MAX_NG + g] = sp;
+            o[2 + 4 * MAX_NG + (ng - 1 - g)] = sp;
         }
     }
     return DGSW_OK;

@@ -17,7 +17,7 @@ constexpr int MAX_NQ = 6;
 constexpr int MAX_NG = 3;
 
 // Edge kinds in the per-tile edge lists
-enum EdgeKind { EK_INTERIOR = 0, EK_LAND = 1, EK_FUNCTION = 2, EK_TIDE = 3, EK_FLOW = 4 };
+enum EdgeKind { EK_INTERIOR = 0, EK_LAND = 1, EK_FUNCTION = 2, EK_TIDE = 3, EK_FLOW = 4, EK_LEVEE = 5 };
 
 struct Topology {
     int64_t ne = 0, nn = 0;
@@ -28,6 +28,7 @@ struct Topology {
     std::vector<int8_t> nbr_face;   // [3*ne] neighbor's local face or -1
     std::vector<uint8_t> btype;     // [3*ne] DGSW_BC_* (128 interior)
     std::vector<int32_t> intf;      // [4*n_intf] in, ex, face_in, face_ex in creation order
+    int64_t n_intf_internal = 0;    // the internal interfaces come first, then the levee ones
     std::vector<int32_t> bnd;       // [3*n_bnd] elem, face, type in traversal order
     // per element: faces in accumulation order (interfaces by creation order, then boundaries)
     std::vector<uint8_t> order_count;  // [ne]
@@ -54,6 +55,15 @@ struct Forcing {
 // matches tide/flow faces to their .bcis blocks (create_boundaries, swe_pre_create_bound.hpp:33-96) and
 // interpolates amplitude and phase to the face's Gauss points; fills T.bnd_force
 int build_forcing(const dgsw_mesh* m, Topology& T, int p, Forcing& out, std::string& err);
+
+// Levee interfaces (ISP::Levee constructor + Initialize, rkdg_swe_is_levee.hpp:36-62): per levee interface
+// (T.intf from n_intf_internal on) the in face's outward normal, then crest height, subcritical and
+// supercritical coefficients at the edge Gauss points (in side order) from the .bcis pairs of its nodes
+// (swe_pre_create_intface.hpp:50-66), then the spherical correction at the in side's and at the ex side's
+// Gauss points (each in its own order)
+constexpr int LEVEE_STRIDE = 2 + 5 * MAX_NG;
+int build_levees(const dgsw_mesh* m, const Topology& T, int p, const double* node_xyz, const dgsw_config& cfg,
+                 std::vector<double>& out, std::string& err);
 
 // Manning friction: per element g * (mean of its three nodes' n)^2 (swe_pre_init_data.hpp:165-196),
 // in reference element order

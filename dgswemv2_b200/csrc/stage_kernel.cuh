@@ -104,6 +104,8 @@ struct StageArgs {
     const double* fcon;
     int ramp_on;           // ramp_duration not almost zero
     double ramp_duration;  // days
+    // levee interface fluxes of this stage, [n_levee][2][3][NG] (levee.cu): in side, then ex side
+    const double* levF;
 };
 
 constexpr int FORCE_STRIDE_DEV = 9;
@@ -764,9 +766,20 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             const int kind = (rec.z >> 4) & 7;
             const bool wa = swet[sa] != 0;
             const bool wb = sb >= 0 && swet[sb] != 0;
-            const bool compute = (kind == 0) ? (wa || wb) : wa;
-            sflag[le] = compute ? 1 : 0;
+            const bool compute = (kind == 0 || kind == 5) ? (wa || wb) : wa;
+            // 2 marks a levee interface: its ex-side flux is not -F and is read in phase 3
+            sflag[le] = compute ? (kind == 5 ? 2 : 1) : 0;
             if (!compute) continue;
+            if (kind == 5) {
+                // the in-side flux as for any edge; the ex-side flux over the ex face's own trace slot,
+                // which no other edge reads
+                const double* Fl = A.levF + (size_t)(rec.z >> 8) * (6 * NG);
+#pragma unroll
+                for (int c = 0; c < 3 * NG; ++c) sF[c * max_edges + le] = (Real)Fl[c];
+#pragma unroll
+                for (int c = 0; c < 3 * NG; ++c) str[c * NS + sb] = (Real)Fl[3 * NG + c];
+                continue;
+            }
             Real sp = Real(1);
             double xa = 0, ya = 0, xb = 0, yb = 0;
             if (kind == 2 || A.spherical) {
@@ -865,7 +878,8 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     for (int i = 0; i < cnt; ++i) {
         const int f = (ord >> (2 + 2 * i)) & 3;
         const int slot = (es.x >> (10 * f)) & 1023;
-        if (!sflag[slot]) continue;
+        const int sfl = sflag[slot];
+        if (!sfl) continue;
         const bool is_in = (roles >> f) & 1;
         const Real sJe = ssJ[slot] * iaJ;  // edge half length over |J|
         Real F[3][NG];
@@ -874,6 +888,9 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
             if (is_in) {
 #pragma unroll
                 for (int v = 0; v < 3; ++v) F[v][gp] = sF[(v * NG + gp) * max_edges + slot];
+            } else if (sfl == 2) {  // levee ex side: its own flux, left in its face's trace slot
+#pragma unroll
+                for (int v = 0; v < 3; ++v) F[v][gp] = str[(v * NG + (NG - 1 - gp)) * NS + 3 * tid + f];
             } else {
                 const int ga = NG - 1 - gp;
 #pragma unroll

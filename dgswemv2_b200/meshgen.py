@@ -8,7 +8,7 @@ cell size, boundary nodes fixed) and a choice of bathymetry functions evaluated 
 """
 import numpy as np
 
-from .types import MeshArrays, LAND
+from .types import LAND, LEVEE, MeshArrays
 
 SIMPLE, ZIGZAG, CHECKER = 0, 1, 2
 
@@ -105,12 +105,45 @@ def quad_mesh(m, n, corners=((0, 0), (1, 0), (1, 1), (0, 1)), bc=(LAND, LAND, LA
     return MeshArrays(nodes, tri, seg_type, seg_offsets, seg_nodes, None, name)
 
 
+def barrier_channel(nx, ny, length, width, xb=None, bc_left=LAND, bc_right=LAND, jitter=0.0, seed=0,
+                    bathymetry=None, name="barrier_channel"):
+    """Channel [0, length] x [0, width] cut at x = xb by an internal barrier: two quad meshes (nx // 2 and
+    nx - nx // 2 columns) whose facing node columns coincide but stay distinct nodes, joined by a LEVEE
+    chain (front = the left part's column, back = the right part's, both bottom to top). Chains: left
+    part bottom, top, left (bc_left); right part bottom, right (bc_right), top; then the barrier."""
+    xb = length / 2 if xb is None else xb
+    nl, nr = nx // 2, nx - nx // 2
+    A = quad_mesh(nl, ny, corners=((0, 0), (xb, 0), (xb, width), (0, width)), bc=(LAND, LAND, LAND, bc_left),
+                  jitter=jitter, seed=seed, bathymetry=bathymetry)
+    B = quad_mesh(nr, ny, corners=((xb, 0), (length, 0), (length, width), (xb, width)), bc=(LAND, bc_right, LAND, LAND),
+                  jitter=jitter, seed=seed + 1, bathymetry=bathymetry)
+    off = A.n_nodes
+    chains, types = [], []
+    for k in (0, 2, 3):  # bottom, top, left of the left part
+        chains.append(A.seg_nodes[A.seg_offsets[k]:A.seg_offsets[k + 1]])
+        types.append(int(A.seg_type[k]))
+    for k in (0, 1, 2):  # bottom, right, top of the right part
+        chains.append(B.seg_nodes[B.seg_offsets[k]:B.seg_offsets[k + 1]] + off)
+        types.append(int(B.seg_type[k]))
+    front = A.seg_nodes[A.seg_offsets[1]:A.seg_offsets[2]]
+    back = B.seg_nodes[B.seg_offsets[3]:B.seg_offsets[4]] + off
+    chains.append(np.concatenate([front, back]))
+    types.append(LEVEE)
+    nodes = np.concatenate([A.node_xyz, B.node_xyz])
+    tri = np.concatenate([A.elem_nodes, B.elem_nodes + off]).astype(np.int32)
+    seg_offsets = np.concatenate([[0], np.cumsum([len(c) for c in chains])]).astype(np.int64)
+    mesh = MeshArrays(nodes, tri, np.array(types, np.int32), seg_offsets, np.concatenate(chains).astype(np.int32),
+                      None, name)
+    mesh.levee_pairs = np.stack([front, back], 1).astype(np.int32)
+    return mesh
+
+
 def write_adcirc(mesh, path):
     """Write the mesh as ADCIRC fort.14. Tide chains become open boundaries; the other chains become
     land-boundary segments with IBTYPE 0 (land), 2 (flow), 77 (function), 88 (outflow)."""
     from .types import TIDE
 
-    ib = {0: 0, 2: 2, 3: 77, 4: 88}
+    ib = {0: 0, 2: 2, 3: 77, 4: 88, LEVEE: 4}
     chains = [(int(mesh.seg_type[s]), mesh.seg_nodes[mesh.seg_offsets[s]:mesh.seg_offsets[s + 1]])
               for s in range(len(mesh.seg_type))]
     open_ch = [c for t, c in chains if t == TIDE]
@@ -130,8 +163,15 @@ def write_adcirc(mesh, path):
             for nd in chain:
                 f.write("%d\n" % nd)
         f.write("%d = Number of land boundaries\n" % len(land_ch))
-        f.write("%d = Total number of land boundary nodes\n" % sum(len(c) for _, c in land_ch))
+        f.write("%d = Total number of land boundary nodes\n" %
+                sum(len(c) // 2 if t == LEVEE else len(c) for t, c in land_ch))
         for s, (t, chain) in enumerate(land_ch):
+            if t == LEVEE:  # NBVV IBCONN BARINTH BARINCFSB BARINCFSP (the RKDG step takes these from .bcis)
+                n = len(chain) // 2
+                f.write("%d %d = Number of nodes for land boundary %d\n" % (n, ib[t], s + 1))
+                for a, b in zip(chain[:n], chain[n:]):
+                    f.write("%d %d 0.0 1.0 1.0\n" % (a, b))
+                continue
             f.write("%d %d = Number of nodes for land boundary %d\n" % (len(chain), ib[t], s + 1))
             for nd in chain:
                 f.write("%d\n" % nd)
@@ -143,6 +183,10 @@ def write_bcis(mesh, path):
     reads (swe_inputs.cpp:211-290): "type nnodes", the constituent count, then per constituent
     "frequency forcing_fact equilib_arg" and one "node amplitude phase" line per node."""
     with open(path, "w") as f:
+        if getattr(mesh, "levee_pairs", None) is not None and len(mesh.levee_pairs):
+            f.write("%d %d = levee pairs\n" % (LEVEE, len(mesh.levee_pairs)))
+            for (a, b), (H, cs, cp) in zip(mesh.levee_pairs, mesh.levee_data):
+                f.write("%d %d %.17g %.17g %.17g\n" % (a, b, H, cs, cp))
         for b in mesh.forcing:
             nodes = np.asarray(b.nodes)
             f.write("%d %d = %s boundary\n" % (int(b.type), len(nodes), "tide" if int(b.type) == 1 else "flow"))

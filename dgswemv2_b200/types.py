@@ -9,6 +9,7 @@ import numpy as np
 # boundary types (source/problem/SWE/swe_definitions.hpp:61-69)
 LAND, TIDE, FLOW, FUNCTION, OUTFLOW = 0, 1, 2, 3, 4
 INTERNAL = 128
+LEVEE = 129  # an internal barrier chain: n front nodes, then the n back nodes across the barrier
 
 # bottom friction types (source/problem/SWE/swe_definitions.hpp:92)
 FRICTION_NONE, FRICTION_CHEZY, FRICTION_MANNING = 0, 1, 2
@@ -66,6 +67,8 @@ class MeshArrays:
     name: str = "mesh"
     node_manning_n: Optional[np.ndarray] = None  # (n_nodes,) Manning's n (FRICTION_MANNING)
     forcing: List[ForcingBlock] = field(default_factory=list)  # tide / flow data
+    levee_pairs: Optional[np.ndarray] = None  # (n, 2) front, back node of each .bcis levee line
+    levee_data: Optional[np.ndarray] = None  # (n, 3) H_barrier, C_subcritical, C_supercritical
 
     @property
     def n_elems(self):

@@ -41,7 +41,7 @@ enum { DGSW_FRICTION_NONE = 0, DGSW_FRICTION_CHEZY = 1, DGSW_FRICTION_MANNING = 
 
 /* Boundary condition / edge types, source/problem/SWE/swe_definitions.hpp:61-69 */
 enum { DGSW_BC_LAND = 0, DGSW_BC_TIDE = 1, DGSW_BC_FLOW = 2, DGSW_BC_FUNCTION = 3, DGSW_BC_OUTFLOW = 4,
-       DGSW_BC_INTERNAL = 128 };
+       DGSW_BC_INTERNAL = 128, DGSW_BC_LEVEE = 129 };
 
 /* Problem configuration: the `.15` input surface read by InputParameters
  * (source/preprocessor/input_parameters.hpp:95-261) and SWE::Inputs (problem_input/swe_inputs.cpp:4-205)
@@ -99,7 +99,13 @@ typedef struct {
 /* Mesh: node coordinates (x, y, bathymetry depth), element node triples (0-based node indices), the
  * reference element IDs (the order the reference iterates elements in; NULL = 0..n-1), and ADCIRC-style
  * boundary node chains with their types, searched in the given order like AdcircFormat::get_ibtype
- * (source/preprocessor/ADCIRC_reader/adcirc_format.cpp), then the optional Manning and tide/flow data. */
+ * (source/preprocessor/ADCIRC_reader/adcirc_format.cpp:214-259), then the optional Manning and tide/flow
+ * data. A DGSW_BC_LEVEE chain is an ADCIRC internal barrier (IBTYPE % 10 == 4, :89-102): its n front
+ * nodes (NBVV) followed by its n back nodes (IBCONN), so 2n entries; the faces along either side become
+ * levee interfaces to the element across the barrier (MeshMetaData, mesh_metadata.cpp:65-83), with the
+ * crest height and the sub- / supercritical discharge coefficients of the .bcis levee lines
+ * (levee_nodes: front, back per pair; levee_data: H_barrier, C_subcritical, C_supercritical per pair;
+ * swe_inputs.cpp:274-287, swe_pre_create_intface.hpp:38-78). */
 typedef struct {
     int64_t n_nodes;
     const double* node_xyz;     /* [3*n_nodes] */
@@ -113,6 +119,9 @@ typedef struct {
     const double* node_manning_n;        /* [n_nodes] Manning's n per node (DGSW_FRICTION_MANNING), or NULL */
     int32_t n_forcing;                   /* tide / flow forcing blocks */
     const dgsw_forcing_block* forcing;   /* [n_forcing] */
+    int32_t n_levee_pairs;               /* .bcis levee lines */
+    const int32_t* levee_nodes;          /* [2 * n_levee_pairs] front, back node indices */
+    const double* levee_data;            /* [3 * n_levee_pairs] H_barrier, C_subcritical, C_supercritical */
 } dgsw_mesh;
 
 typedef struct {

@@ -313,6 +313,8 @@ struct AdcircMesh {
     };
     std::vector<Block> forcing;
     std::vector<dgsw_forcing_block> forcing_view;
+    std::vector<int32_t> levee_nodes;  // .bcis levee lines: front, back node indices
+    std::vector<double> levee_data;    // H_barrier, C_subcritical, C_supercritical
 
     dgsw_mesh view() {
         forcing_view.clear();
@@ -333,6 +335,9 @@ struct AdcircMesh {
         m.node_manning_n = node_manning_n.empty() ? nullptr : node_manning_n.data();
         m.n_forcing = (int32_t)forcing_view.size();
         m.forcing = forcing_view.empty() ? nullptr : forcing_view.data();
+        m.n_levee_pairs = (int32_t)(levee_nodes.size() / 2);
+        m.levee_nodes = levee_nodes.empty() ? nullptr : levee_nodes.data();
+        m.levee_data = levee_data.empty() ? nullptr : levee_data.data();
         m.n_nodes = n_nodes();
         m.node_xyz = node_xyz.data();
         m.n_elems = n_elems();
@@ -347,9 +352,9 @@ struct AdcircMesh {
 };
 
 /* Reads a fort.14 like AdcircFormat::AdcircFormat (adcirc_format.cpp:3-130). IBTYPE mapping as in
- * get_ibtype (:214-254): open boundaries -> tide, IBTYPE%10==0 -> land, %10==2 -> flow, 77 -> function,
- * 88 -> outflow; island segments (%10==1) are read but never matched, so they are not emitted; internal
- * barriers (%10==4, levees) are rejected as unsupported. */
+ * get_ibtype (:214-259): open boundaries -> tide, IBTYPE%10==0 -> land, %10==2 -> flow, 77 -> function,
+ * 88 -> outflow, %10==4 -> an internal barrier (levee) chain of its front then its back nodes; island
+ * segments (%10==1) are read but never matched, so they are not emitted. */
 inline AdcircMesh read_adcirc(const std::string& path) {
     std::ifstream ifs(path);
     if (!ifs) throw std::logic_error("Fatal Error: ADCIRC mesh file " + path + " was not found!\n");
@@ -436,8 +441,20 @@ inline AdcircMesh read_adcirc(const std::string& path) {
         ifs >> n >> ibtype;
         skip_line();
         std::vector<long> chain(n);
-        if (ibtype % 10 == 4)
-            throw Error(DGSW_ERR_UNSUPPORTED, "ADCIRC internal barrier (levee) boundaries are not supported");
+        if (ibtype % 10 == 4) {
+            // internal barrier: NBVV IBCONN BARINTH BARINCFSB BARINCFSP per line (adcirc_format.cpp:89-102);
+            // the barrier heights and coefficients the RKDG step uses come from the .bcis levee lines
+            std::vector<long> back(n);
+            for (long i = 0; i < n; ++i) {
+                double h, cs, cp;
+                ifs >> chain[i] >> back[i] >> h >> cs >> cp;
+                skip_line();
+            }
+            if (!ifs) fail("truncated internal barrier segment");
+            chain.insert(chain.end(), back.begin(), back.end());
+            add_segment(DGSW_BC_LEVEE, chain);
+            continue;
+        }
         if (!(ibtype % 10 == 0 || ibtype % 10 == 1 || ibtype % 10 == 2 || ibtype == 77 || ibtype == 88))
             throw std::logic_error("Fatal Error: undefined boundary type in ADCIRC mesh: " + std::to_string(ibtype) +
                                    "!\n");
@@ -477,8 +494,8 @@ inline AdcircMesh read_adcirc(const std::string& path) {
 
 /* SWE::Inputs::read_bcis (swe_inputs.cpp:211-290): tide and flow blocks, each a "btype nnodes" line, the
  * constituent count, then per constituent "frequency forcing_fact equilib_arg" and nnodes lines
- * "node_ID amplitude phase". Levee blocks (nnodes "front back H C_sub C_super" lines) are read past:
- * internal-barrier boundaries are rejected with the mesh. Other lines are skipped. A missing file gives no
+ * "node_ID amplitude phase"; levee blocks, nnodes lines "front back H_barrier C_subcritical
+ * C_supercritical" (levee_is_data). Other lines are skipped. A missing file gives no
  * blocks, as in the reference (its existence check is commented out); a tide or flow face without data
  * then fails in create_boundaries' "unable to find ... data". A node ID the mesh does not have can match
  * no face and is dropped. Where the reference would append a node listed twice in one constituent to the
@@ -542,7 +559,21 @@ inline void read_bcis(const std::string& path, AdcircMesh& M) {
                 }
             M.forcing.push_back(std::move(b));
         } else if (btype == levee) {
-            for (unsigned k = 0; k < nnodes; ++k) std::getline(file, line);
+            // "front back H_barrier C_subcritical C_supercritical"; pairs of unknown nodes match no face
+            for (unsigned k = 0; k < nnodes; ++k) {
+                std::getline(file, line);
+                std::stringstream st(line);
+                uint32_t a = 0, b = 0;
+                double H = 0, cs = 0, cp = 0;
+                st >> a >> b >> H >> cs >> cp;
+                auto ia = index.find(a), ib = index.find(b);
+                if (ia == index.end() || ib == index.end()) continue;
+                M.levee_nodes.push_back(ia->second);
+                M.levee_nodes.push_back(ib->second);
+                M.levee_data.push_back(H);
+                M.levee_data.push_back(cs);
+                M.levee_data.push_back(cp);
+            }
         }
     }
 }

@@ -32,7 +32,7 @@ using std::vector;
 thread_local std::string g_err;
 
 constexpr uint32_t DEFAULT_ID = 4294967295u;  // general_definitions.hpp:230
-constexpr int BT_LAND = 0, BT_TIDE = 1, BT_FLOW = 2, BT_FUNCTION = 3, BT_OUTFLOW = 4;
+constexpr int BT_LAND = 0, BT_TIDE = 1, BT_FLOW = 2, BT_FUNCTION = 3, BT_OUTFLOW = 4, BT_LEVEE = 129;
 constexpr int BT_INTERNAL = 128;  // utilities/edge_types.hpp:4
 constexpr double DBL_EPS = 2.220446049250313e-16;
 constexpr double REF_PI = 3.14159265359;  // the reference's PI (general_definitions.hpp:227)
@@ -427,6 +427,9 @@ struct Intf {
     vector<double> int_fact_in, int_fact_ex;
     double n_in[2];
     vector<double> gpx_in, gpy_in;
+    // ISP::Levee (rkdg_swe_is_levee.hpp:36-62): crest height and discharge coefficients at the gp
+    bool levee = false;
+    vector<double> H_bar_gp, C_subcrit_gp, C_supercrit_gp;
 };
 
 struct Bnd {
@@ -470,22 +473,64 @@ struct Problem {
 // Mesh metadata (preprocessor/mesh_metadata.cpp:3-85) and boundary type lookup
 // (ADCIRC_reader/adcirc_format.cpp get_ibtype / has_edge)
 // ------------------------------------------------------------------------------------------------
+// AdcircFormat::has_edge (adcirc_format.cpp:320-336): looks at every occurrence of n0
 bool has_edge(const int32_t* b, const int32_t* e, int32_t n0, int32_t n1) {
     const int32_t* it = std::find(b, e, n0);
     if (it != e) {
         if ((it + 1) != e && *(it + 1) == n1) return true;
         if (it != b && *(it - 1) == n1) return true;
+        return has_edge(it + 1, e, n0, n1);
     }
     return false;
 }
 
+// AdcircFormat::get_ibtype (adcirc_format.cpp:214-259) over the chains in search order; a levee chain
+// (type 129) is its front string then its back string, each searched on its own; a face joining the
+// two strings at a barrier end is land (is_levee_end, :338-352)
 int get_ibtype(const orc_mesh* m, int32_t n0, int32_t n1) {
     for (int s = 0; s < m->n_segments; ++s) {
         const int32_t* b = m->seg_nodes + m->seg_offsets[s];
         const int32_t* e = m->seg_nodes + m->seg_offsets[s + 1];
-        if (has_edge(b, e, n0, n1)) return m->seg_type[s];
+        if (m->seg_type[s] == BT_LEVEE) {
+            const int32_t* mid = b + (e - b) / 2;
+            if (has_edge(b, mid, n0, n1) || has_edge(mid, e, n0, n1)) return BT_LEVEE;
+        } else if (has_edge(b, e, n0, n1)) {
+            return m->seg_type[s];
+        }
+    }
+    const int32_t lo = std::min(n0, n1), hi = std::max(n0, n1);
+    for (int s = 0; s < m->n_segments; ++s) {
+        if (m->seg_type[s] != BT_LEVEE) continue;
+        const int32_t* b = m->seg_nodes + m->seg_offsets[s];
+        const int64_t n = (m->seg_offsets[s + 1] - m->seg_offsets[s]) / 2;
+        const int32_t *fr = b, *bk = b + n;
+        if ((lo == std::min(fr[0], bk[0]) && hi == std::max(fr[0], bk[0])) ||
+            (lo == std::min(fr[n - 1], bk[n - 1]) && hi == std::max(fr[n - 1], bk[n - 1])))
+            return BT_LAND;
     }
     return -1;
+}
+
+// AdcircFormat::get_internal_node_pair (adcirc_format.cpp:261-318): the node pair across the barrier
+std::pair<int32_t, int32_t> internal_node_pair(const orc_mesh* m, int32_t n0, int32_t n1) {
+    for (int s = 0; s < m->n_segments; ++s) {
+        if (m->seg_type[s] != BT_LEVEE) continue;
+        const int64_t n = (m->seg_offsets[s + 1] - m->seg_offsets[s]) / 2;
+        const int32_t* fr = m->seg_nodes + m->seg_offsets[s];
+        const int32_t* bk = fr + n;
+        for (int side = 0; side < 2; ++side) {
+            const int32_t* a = side == 0 ? fr : bk;
+            const int32_t* o = side == 0 ? bk : fr;
+            if (a[0] == n0 && a[1] == n1) return {o[1], o[0]};
+            for (int64_t k = 1; k < n - 1; ++k)
+                if (a[k] == n0) {
+                    if (a[k + 1] == n1) return {o[k + 1], o[k]};
+                    if (a[k - 1] == n1) return {o[k - 1], o[k]};
+                }
+            if (a[n - 1] == n0 && a[n - 2] == n1) return {o[n - 2], o[n - 1]};
+        }
+    }
+    throw std::runtime_error("Fatal Error: back nodes not found to given node_pair");
 }
 
 // Tide / flow data of one boundary face: create_boundaries (swe_pre_create_bound.hpp:33-96) takes the
@@ -606,6 +651,15 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
                 throw std::runtime_error("Fatal Error: boundary not found, unable to assign BOUNDARY_TYPE to given node_pair");
             E.neighbor_ID[f] = DEFAULT_ID;
             E.btype[f] = (uint8_t)bt;
+            // the element across an internal barrier (mesh_metadata.cpp:75-82)
+            if (bt == BT_LEVEE) {
+                auto np = internal_node_pair(m, n0, n1);
+                uint64_t key = (uint64_t)(uint32_t)std::min(np.first, np.second) << 32 |
+                               (uint32_t)std::max(np.first, np.second);
+                auto it = dict.find(key);
+                if (it == dict.end()) throw std::runtime_error("Fatal Error: no element across the barrier");
+                E.neighbor_ID[f] = it->second.first.first;
+            }
         }
     }
     for (auto& E : P.elts)
@@ -654,12 +708,15 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
 
     // raw boundaries and interface/boundary creation (swe_pre_create_intface.hpp, swe_pre_create_bound.hpp)
     std::map<std::pair<uint32_t, uint32_t>, std::pair<int, int>> raw_internal;  // (id, neigh id) -> (elt, face)
+    std::map<std::pair<uint32_t, uint32_t>, std::pair<int, int>> raw_levee;
     std::map<int, std::map<std::pair<uint32_t, uint32_t>, std::pair<int, int>>> raw_bound;
     for (int k = 0; k < ne; ++k) {
         Elt& E = P.elts[k];
         for (int f = 0; f < 3; ++f) {
             if (E.btype[f] == BT_INTERNAL)
                 raw_internal.emplace(std::make_pair(E.id, E.neighbor_ID[f]), std::make_pair(k, f));
+            else if (E.btype[f] == BT_LEVEE)
+                raw_levee.emplace(std::make_pair(E.id, E.neighbor_ID[f]), std::make_pair(k, f));
             else
                 raw_bound[E.btype[f]].emplace(std::make_pair(E.id, (uint32_t)f), std::make_pair(k, f));
         }
@@ -676,12 +733,16 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
     };
     for (auto& E : P.elts)
         for (int f = 0; f < 3; ++f) make_face_data(E, f);
-    {
-        auto it = raw_internal.begin();
-        while (it != raw_internal.end()) {
+    // levee_is_data keyed (front, back); swe_pre_create_intface.hpp:50-66 looks a face's node pair up in
+    // both orders
+    std::map<std::pair<int32_t, int32_t>, int32_t> levee_data;
+    for (int32_t k = 0; k < m->n_levee_pairs; ++k) levee_data[{m->levee_nodes[2 * k], m->levee_nodes[2 * k + 1]}] = k;
+    auto create_interfaces = [&](std::map<std::pair<uint32_t, uint32_t>, std::pair<int, int>>& raw, bool levee) {
+        auto it = raw.begin();
+        while (it != raw.end()) {
             auto key_ex = std::make_pair(it->first.second, it->first.first);
-            auto jt = raw_internal.find(key_ex);
-            if (jt != raw_internal.end()) {
+            auto jt = raw.find(key_ex);
+            if (jt != raw.end()) {
                 Intf I;
                 I.in = it->second.first;
                 I.bin = it->second.second;
@@ -711,11 +772,38 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
                         I.ipf_ex[gp * nd + dof] = I.phi_ex[dof * ngb + gp] * (gl.w[gp] * sJ);
                     }
                 Ein.shape.normal(I.bin, I.n_in);
+                if (levee) {
+                    const Elt& Eex = P.elts[I.ex];
+                    const int32_t ni[2] = {Ein.node_idx[(I.bin + 1) % 3], Ein.node_idx[(I.bin + 2) % 3]};
+                    const int32_t nx[2] = {Eex.node_idx[(I.bex + 1) % 3], Eex.node_idx[(I.bex + 2) % 3]};
+                    double H[2], Cs[2], Cp[2];
+                    for (int node = 0; node < 2; ++node) {
+                        auto d = levee_data.find({ni[node], nx[1 - node]});
+                        if (d == levee_data.end()) d = levee_data.find({nx[1 - node], ni[node]});
+                        if (d == levee_data.end()) throw std::runtime_error("Fatal Error: unable to find levee data!\n");
+                        H[node] = m->levee_data[3 * d->second];
+                        Cs[node] = m->levee_data[3 * d->second + 1];
+                        Cp[node] = m->levee_data[3 * d->second + 2];
+                    }
+                    I.levee = true;
+                    I.H_bar_gp.resize(ngb);
+                    I.C_subcrit_gp.resize(ngb);
+                    I.C_supercrit_gp.resize(ngb);
+                    for (int gp = 0; gp < ngb; ++gp) {  // ComputeBoundaryNodalUgpIN
+                        const double psi[2] = {(1 - gl.z[gp]) / 2, (1 + gl.z[gp]) / 2};
+                        I.H_bar_gp[gp] = H[0] * psi[0] + H[1] * psi[1];
+                        I.C_subcrit_gp[gp] = Cs[0] * psi[0] + Cs[1] * psi[1];
+                        I.C_supercrit_gp[gp] = Cp[0] * psi[0] + Cp[1] * psi[1];
+                    }
+                }
                 P.intfs.push_back(std::move(I));
             }
-            it = raw_internal.erase(it);
+            it = raw.erase(it);
         }
-    }
+    };
+    // internal interfaces, then levee interfaces (swe_pre_create_intface.hpp:13-82)
+    create_interfaces(raw_internal, false);
+    create_interfaces(raw_levee, true);
     // boundaries grouped by condition type in the order Land, Tide, Flow, Function
     // (ProblemBoundaryTypes tuple order, rkdg_swe_problem.hpp:46); outflow faces get no boundary object
     for (int bt : {BT_LAND, BT_TIDE, BT_FLOW, BT_FUNCTION}) {
@@ -748,7 +836,7 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
     for (auto& kv : raw_bound)
         if (kv.first != BT_LAND && kv.first != BT_FUNCTION && kv.first != BT_OUTFLOW)
             if (kv.first != BT_TIDE && kv.first != BT_FLOW)
-                throw std::runtime_error("unsupported boundary type (levee / island)");
+                throw std::runtime_error("unsupported boundary type");
 
     // per-element contribution order: interfaces in creation order, then boundaries
     P.contrib.assign(ne, {});
@@ -1057,6 +1145,80 @@ void trace(const double* q, const vector<double>& phi, int nd, int ngb, double* 
 }
 
 // interface flux, rkdg_swe_proc_intface.hpp:7-27 + rkdg_swe_is_internal.hpp:26-95
+// BC::Land::GetEX (rkdg_swe_bc_land.hpp:88-104)
+void land_ex(const double n[2], const double q[3], double qe[3]) {
+    const double tx = -n[1], ty = n[0];
+    const double qn = -(q[1] * n[0] + q[2] * n[1]);
+    const double qt = q[1] * tx + q[2] * ty;
+    qe[0] = q[0];
+    qe[1] = qn * n[0] + qt * tx;
+    qe[2] = qn * n[1] + qt * ty;
+}
+
+// ISP::Levee::ComputeFlux (rkdg_swe_is_levee.hpp:64-175)
+void levee_flux(Problem& P, Intf& I, FaceData& Bi, FaceData& Be, const double n_in[2], const double n_ex[2],
+                bool wet_in, bool wet_ex) {
+    const int ngb = I.ngp;
+    const double H_tolerance = 0.01, G = P.cfg.g;
+    double q_in_ex[3] = {0, 0, 0}, q_ex_ex[3] = {0, 0, 0};
+    for (int gp = 0; gp < ngb; ++gp) {
+        const int gp_ex = ngb - gp - 1;
+        const double H = I.H_bar_gp[gp], Csub = I.C_subcrit_gp[gp], Csup = I.C_supercrit_gp[gp];
+        double gravity_in = G, gravity_ex = G;
+        double qi[3], qe[3];
+        for (int v = 0; v < 3; ++v) {
+            qi[v] = Bi.q_at_gp[v * ngb + gp];
+            qe[v] = Be.q_at_gp[v * ngb + gp_ex];
+        }
+        const double h_in = qi[0] - H, h_ex = qe[0] - H;
+        if ((h_in <= H_tolerance && h_ex <= H_tolerance) || std::abs(h_in - h_ex) <= H_tolerance) {
+            land_ex(n_in, qi, q_in_ex);
+            land_ex(n_ex, qe, q_ex_ex);
+        } else if (h_in > h_ex) {
+            const double nx = n_in[0], ny = n_in[1], tx = -ny, ty = nx;
+            double qn, qt;
+            if (h_ex > 2.0 * h_in / 3.0) {
+                qn = Csub * h_ex * std::sqrt(2.0 * G * (h_in - h_ex));
+                qt = 0.0;
+            } else {
+                qn = Csup * (2.0 * h_in / 3.0) * std::sqrt(G * (2.0 * h_in / 3.0));
+                qt = 0.0;
+            }
+            q_in_ex[0] = qi[0];
+            q_in_ex[1] = qn * nx + qt * tx;
+            q_in_ex[2] = qn * ny + qt * ty;
+            q_ex_ex[0] = qe[0];
+            q_ex_ex[1] = q_in_ex[1];
+            q_ex_ex[2] = q_in_ex[2];
+            if (!wet_ex) gravity_ex = 0.0;
+        } else if (h_in < h_ex) {
+            const double nx = n_ex[0], ny = n_ex[1], tx = -ny, ty = nx;
+            double qn, qt;
+            if (h_in > 2.0 * h_ex / 3.0) {
+                qn = Csub * h_in * std::sqrt(2.0 * G * (h_ex - h_in));
+                qt = 0.0;
+            } else {
+                qn = Csup * (2.0 * h_ex / 3.0) * std::sqrt(G * (2.0 * h_ex / 3.0));
+                qt = 0.0;
+            }
+            q_ex_ex[0] = qe[0];
+            q_ex_ex[1] = qn * nx + qt * tx;
+            q_ex_ex[2] = qn * ny + qt * ty;
+            q_in_ex[0] = qi[0];
+            q_in_ex[1] = q_ex_ex[1];
+            q_in_ex[2] = q_ex_ex[2];
+            if (!wet_in) gravity_in = 0.0;
+        }
+        double Fi[3], Fe[3];
+        LLF_flux(gravity_in, qi, q_in_ex, Bi.bath[gp], Bi.sp[gp], n_in, Fi);
+        LLF_flux(gravity_ex, qe, q_ex_ex, Be.bath[gp_ex], Be.sp[gp_ex], n_ex, Fe);
+        for (int v = 0; v < 3; ++v) {
+            Bi.F_hat[v * ngb + gp] = Fi[v];
+            Be.F_hat[v * ngb + gp_ex] = Fe[v];
+        }
+    }
+}
+
 void interface_flux(Problem& P, Intf& I) {
     Elt& Ei = P.elts[I.in];
     Elt& Ee = P.elts[I.ex];
@@ -1070,6 +1232,10 @@ void interface_flux(Problem& P, Intf& I) {
     const bool wet_in = Ei.wet, wet_ex = Ee.wet;
     const double n_in[2] = {I.n_in[0], I.n_in[1]};
     const double n_ex[2] = {-I.n_in[0], -I.n_in[1]};
+    if (I.levee) {
+        levee_flux(P, I, Bi, Be, n_in, n_ex, wet_in, wet_ex);
+        return;
+    }
     for (int gp = 0; gp < ngb; ++gp) {
         int ge = ngb - gp - 1;
         double qi[3], qe[3], Fi[3], Fe[3];

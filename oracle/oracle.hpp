@@ -69,6 +69,11 @@ struct orc_mesh {
     const double* node_manning_n;  // [n_nodes] Manning's n (bottom_friction 2), or null
     int32_t n_forcing;
     const orc_forcing_block* forcing;
+    // internal barriers: a segment of type 129 holds n front nodes then n back nodes; the .bcis levee
+    // lines give (front, back) pairs with H_barrier, C_subcritical, C_supercritical
+    int32_t n_levee_pairs;
+    const int32_t* levee_nodes;  // [2 * n_levee_pairs]
+    const double* levee_data;    // [3 * n_levee_pairs]
 };
 
 typedef struct orc_handle_s* orc_handle;

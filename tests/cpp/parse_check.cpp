@@ -63,7 +63,10 @@ int main(int argc, char** argv) {
                       << " " << fnv(F.amplitude.data(), F.amplitude.size() * 8) << " "
                       << fnv(F.phase.data(), F.phase.size() * 8) << "\n";
         }
-        std::cout << "manning_hash " << fnv(M.node_manning_n.data(), M.node_manning_n.size() * 8) << "\n";
+        std::cout << "manning_hash " << fnv(M.node_manning_n.data(), M.node_manning_n.size() * 8) << "\n"
+                  << "n_levee_pairs " << M.levee_nodes.size() / 2 << "\n"
+                  << "levee_hash " << fnv(M.levee_nodes.data(), M.levee_nodes.size() * 4) << " "
+                  << fnv(M.levee_data.data(), M.levee_data.size() * 8) << "\n";
         std::cout << "mesh_name " << M.name << "\n"
                   << "n_nodes " << M.n_nodes() << "\n"
                   << "n_elems " << M.n_elems() << "\n"

@@ -3,7 +3,7 @@ import ctypes as C
 
 import numpy as np
 
-from dgswemv2_b200._lib import forcing_blocks
+from dgswemv2_b200._lib import forcing_blocks, levee_arrays
 
 
 class OrcConfig(C.Structure):
@@ -61,6 +61,9 @@ class OrcMesh(C.Structure):
         ("node_manning_n", C.POINTER(C.c_double)),
         ("n_forcing", C.c_int32),
         ("forcing", C.POINTER(OrcForcingBlock)),
+        ("n_levee_pairs", C.c_int32),
+        ("levee_nodes", C.POINTER(C.c_int32)),
+        ("levee_data", C.POINTER(C.c_double)),
     ]
 
 
@@ -119,6 +122,12 @@ class OracleProblem:
         self._keep.append(fkeep)
         m.n_forcing = nf
         m.forcing = arr
+        nl, lp, ld = levee_arrays(mesh)
+        if nl:
+            self._keep += [lp, ld]
+            m.n_levee_pairs = nl
+            m.levee_nodes = _ptr(lp, C.c_int32)
+            m.levee_data = _ptr(ld, C.c_double)
         h = C.c_void_p()
         rc = lib.orc_create(C.byref(c), C.byref(m), C.byref(h))
         if rc != 0:

@@ -244,3 +244,37 @@ def test_tide_face_without_data_is_a_mesh_error():
     with pytest.raises(DgswError, match="unable to find tide data") as ei:
         Problem(cfg, mesh)
     assert ei.value.status == 2
+
+
+@pytest.mark.parametrize("p, rk, dt, steps", [(1, (2, 2), 2.0, 600), (2, (3, 3), 1.0, 1000)])
+def test_levee_channel_matches_oracle(oracle, p, rk, dt, steps):
+    """Levee interfaces (ISP::Levee): the tide overtops a barrier across the channel (reflective,
+    subcritical and supercritical weir branches); FP64 state within 1e-12 of the oracle's scale."""
+    mesh, cfg = configs.levee_channel(p=p, rk=rk, dt=dt)
+    P, O = run_pair(oracle, mesh, cfg, steps)
+    q = O.get_state()
+    xc = mesh.node_xyz[mesh.elem_nodes, 0].mean(1)
+    assert q[xc > 5000, 0, 0].mean() > 0.05  # water has come over the levee
+    e = rel_err(P.get_state(), q)
+    assert e <= 1e-12, e
+
+
+def test_levee_floods_dry_land(oracle):
+    """Overtopping onto dry land (wetting/drying, gravity dropped on the dry receiving side): wet-cell
+    counts within 0.5 %, state within 1e-9 of the variable scale."""
+    mesh, cfg = configs.levee_channel(p=1, dt=2.0, dry_right=True)
+    P, O = run_pair(oracle, mesh, cfg, 600)
+    wg, wo = P.get_wet(), O.get_wet()
+    assert int(wo.sum()) > mesh.n_elems // 2 + 10  # the dry half has started to flood
+    assert abs(int(wg.sum()) - int(wo.sum())) <= max(2, 0.005 * mesh.n_elems)
+    assert rel_err(P.get_state(), O.get_state()) <= 1e-9
+
+
+def test_levee_channel_fp32_bulk(oracle):
+    mesh, cfg = configs.levee_channel(p=2, rk=(3, 3), dt=1.0, precision="fp32")
+    P = Problem(cfg, mesh)
+    O = oracle.problem(configs.levee_channel(p=2, rk=(3, 3), dt=1.0)[1], mesh, n_threads=8)
+    P.step_serial(1000)
+    O.step(1000)
+    e = rel_err(P.get_state(), O.get_state())
+    assert e < 1e-3, e

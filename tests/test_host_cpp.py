@@ -194,10 +194,10 @@ def test_mesh_errors(parse_check, tmp_path):
     open(mpath, "w").write(src.replace("77 = Number of nodes for land boundary 1", "5 = Number of nodes for land boundary 1"))
     rc, out, _ = run_check(parse_check, path)
     assert rc == 3 and "undefined boundary type in ADCIRC mesh: 5" in out["error"]
-    # internal barriers (levees) are unsupported
+    # an internal barrier segment needs five columns per line (NBVV IBCONN BARINTH BARINCFSB BARINCFSP)
     open(mpath, "w").write(src.replace("77 = Number of nodes for land boundary 1", "4 = Number of nodes for land boundary 1"))
     rc, out, _ = run_check(parse_check, path)
-    assert rc == 3 and out["error"].startswith("5 ") and "levee" in out["error"]
+    assert rc == 3 and "error" in out
     # an island segment (IBTYPE 1) is read but never matched: its edges then have no boundary type
     open(mpath, "w").write(src.replace("77 = Number of nodes for land boundary 1", "1 = Number of nodes for land boundary 1"))
     rc, out, _ = run_check(parse_check, path)
@@ -341,4 +341,50 @@ def test_serial_driver_runs_tidal_channel(tmp_path):
     last = lines[t_idx[-1] + 1: t_idx[-1] + 1 + mesh.n_elems]
     ze = np.array([[float(v) for v in l.split()[1:]] for l in last])
     assert abs(float(lines[t_idx[-1]]) - 300.0) < 1e-9
+    assert np.allclose(ze, q[:, 0, :], rtol=1e-14, atol=1e-15)
+
+
+LEVEE_15 = TIDE_15.replace("  bottom_friction:\n    type: Manning\n    coefficient: 0.0005\n    input_file: manning.dat\n",
+                           "  bottom_friction:\n    type: Chezy\n    coefficient: 0.0025\n").replace(
+    "polynomial_order: 2", "polynomial_order: 1").replace("order: 3\n  nstages: 3", "order: 2\n  nstages: 2").replace(
+    "ramp_duration: 0.01", "ramp_duration: 0.005")
+
+
+def test_parse_internal_barrier_and_levee_data(parse_check, tmp_path):
+    """IBTYPE 4 segments become levee chains (front then back nodes) and the .bcis levee lines come
+    through as (front, back) pairs with their crest height and coefficients, bit for bit; the host
+    topology of the parsed mesh equals the Python mesh's."""
+    mesh, cfg = configs.levee_channel()
+    d = str(tmp_path)
+    path = write_input(d, mesh, LEVEE_15, mesh_name="channel.14")
+    meshgen.write_bcis(mesh, os.path.join(d, "channel.bcis"))
+    rc, out, err = run_check(parse_check, path)
+    assert rc == 0, (out, err)
+    assert out["n_levee_pairs"] == str(len(mesh.levee_pairs))
+    h_nodes, h_data = out["levee_hash"].split()
+    assert h_nodes == fnv(np.asarray(mesh.levee_pairs, np.int32)) and h_data == fnv(np.asarray(mesh.levee_data, np.float64))
+    nbr, bt, intf, bnd = mesh_topology(mesh)
+    assert out["neighbors_hash"] == fnv(nbr) and out["interfaces_hash"] == fnv(intf)
+    assert out["boundaries_hash"] == fnv(bnd) and out["btype_hash"] == fnv(bt)
+    assert int((bt == 129).sum()) == 2 * (len(mesh.levee_pairs) - 1)
+
+
+@pytest.mark.gpu
+def test_serial_driver_runs_levee_channel(tmp_path):
+    """dgswemv2-b200-serial on the levee channel (IBTYPE 4 barrier + .bcis levee and tide/flow data):
+    the modal output after 300 steps equals the Python API's state."""
+    mesh, cfg = configs.levee_channel()
+    d = str(tmp_path)
+    path = write_input(d, mesh, LEVEE_15, mesh_name="channel.14")
+    meshgen.write_bcis(mesh, os.path.join(d, "channel.bcis"))
+    os.makedirs(os.path.join(d, "out"), exist_ok=True)
+    r = subprocess.run([CLI, path], capture_output=True, text=True, timeout=300, cwd=d)
+    assert r.returncode == 0, r.stdout + r.stderr
+    P = Problem(cfg, mesh)
+    P.step_serial(300)
+    q = P.get_state()
+    lines = open(os.path.join(d, "out", "modal_ze.txt")).read().split("\n")
+    t_idx = [i for i, l in enumerate(lines) if l and len(l.split()) == 1]
+    last = lines[t_idx[-1] + 1: t_idx[-1] + 1 + mesh.n_elems]
+    ze = np.array([[float(v) for v in l.split()[1:]] for l in last])
     assert np.allclose(ze, q[:, 0, :], rtol=1e-14, atol=1e-15)

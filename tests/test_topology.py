@@ -90,3 +90,44 @@ def test_tide_face_without_data_is_an_error(oracle):
     mesh.forcing[0].phase = mesh.forcing[0].phase[:, :2]
     with pytest.raises(RuntimeError, match="unable to find tide data"):
         oracle.problem(cfg, mesh)
+
+
+def test_levee_interfaces_pair_the_two_sides_of_a_barrier(oracle):
+    """Faces along an internal barrier become levee interfaces to the element across it (the node pair
+    mirrored through the barrier's front/back strings), created after all internal interfaces."""
+    from dgswemv2_b200 import configs
+    from dgswemv2_b200.types import LEVEE
+
+    mesh, _ = configs.levee_channel(nx=10, ny=4)
+    a = mesh_topology(mesh)
+    b = _oracle_topology(oracle, mesh)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    nbr, bt, intf, bnd = a
+    lev = bt == LEVEE
+    assert int(lev.sum()) == 2 * 4
+    # the levee interfaces are the last ones, and each pairs one element of each half
+    xc = mesh.node_xyz[mesh.elem_nodes, 0].mean(1)
+    n_lev = 4
+    for i_in, i_ex, f_in, f_ex in intf[-n_lev:]:
+        assert bt[i_in, f_in] == LEVEE and bt[i_ex, f_ex] == LEVEE
+        assert (xc[i_in] < 5000) != (xc[i_ex] < 5000)
+    assert not np.any(bt[intf[:-n_lev, 0], intf[:-n_lev, 2]] == LEVEE)
+
+
+def test_closed_chain_edge_is_found_at_any_occurrence(oracle):
+    """A closed land chain lists its first node again at the end; the edge joining the last two nodes
+    is found there (has_edge looks at every occurrence of a node)."""
+    mesh = meshgen.quad_mesh(4, 3, bc=(LAND, LAND, LAND, LAND))
+    m, n = 4, 3
+    ring = list(range(m + 1)) + [m + j * (m + 1) for j in range(1, n + 1)] + \
+        [m + n * (m + 1) - i for i in range(1, m + 1)] + [(n - j) * (m + 1) for j in range(1, n + 1)]
+    assert ring[0] == ring[-1]
+    mesh.seg_type = np.array([LAND], np.int32)
+    mesh.seg_offsets = np.array([0, len(ring)], np.int64)
+    mesh.seg_nodes = np.array(ring, np.int32)
+    a = mesh_topology(mesh)
+    b = _oracle_topology(oracle, mesh)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert len(a[3]) == 2 * (m + n)
