@@ -202,6 +202,19 @@ class Problem:
         assert q.shape == (self.ne, 3, self.nd)
         _lib.check(_lib.load().dgsw_rkdg_set_state(self._h, _lib.ptr(q, C.c_double)))
 
+    def postprocess(self):
+        """Writer values (dgsw_rkdg_postprocess): point data [ne][3][ze, qx, qy, bath] at the vertices,
+        cell data [ne][ze, qx, qy, bath] at the centroids, wet and went-completely-dry flags, in ascending
+        element-ID order."""
+        lib = _lib.load()
+        pt = np.empty((self.ne, 3, 4), np.float64)
+        cell = np.empty((self.ne, 4), np.float64)
+        wet = np.empty(self.ne, np.uint8)
+        wd = np.empty(self.ne, np.uint8)
+        _lib.check(lib.dgsw_rkdg_postprocess(self._h, _lib.ptr(pt, C.c_double), _lib.ptr(cell, C.c_double),
+                                             _lib.ptr(wet, C.c_uint8), _lib.ptr(wd, C.c_uint8)))
+        return pt, cell, wet, wd
+
     def get_wet(self):
         w = np.empty(self.ne, np.uint8)
         _lib.check(_lib.load().dgsw_rkdg_get_wet(self._h, _lib.ptr(w, C.c_uint8)))

@@ -179,6 +179,9 @@ SIGNATURES = {
     "dgsw_rkdg_get_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "dgsw_rkdg_set_wet": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint8)]),
     "dgsw_rkdg_get_wet": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "dgsw_rkdg_get_bathymetry": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "dgsw_rkdg_postprocess": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
     "dgsw_rkdg_set_state_device": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_get_state_device": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_step": (C.c_int32, [C.c_void_p, C.c_int32]),

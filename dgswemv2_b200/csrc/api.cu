@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <limits>
 #include <map>
 #include <mutex>
@@ -21,6 +22,7 @@
 #include "stage_kernel.cuh"
 #include "trouble.cuh"
 #include "levee.cuh"
+#include "postprocess.cuh"
 
 using namespace dgsw;
 
@@ -113,6 +115,9 @@ struct dgsw_rkdg_s {
     DBuf<int4> lev;        // in element, in face, ex element, ex face (device order)
     DBuf<double> ldat;     // normal, crest height and coefficients at the Gauss points, spherical factors
     DBuf<double> levF;     // this stage's levee fluxes
+    DBuf<unsigned char> went_dry;  // wet_dry_state.went_completely_dry (wetting/drying only)
+    DBuf<double> post;             // output values for the writers (allocated on first use)
+    DBuf<unsigned char> post_flags;
     DBuf<int2> halo;
     DBuf<int> tile_halo_off;
     DBuf<int> enodes, tile_edge_off, ref_of_dev;
@@ -229,6 +234,7 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     // ESSPRKStepper keeps ramp = 1 when Utilities::almost_equal(ramp_duration, 0)
     A.ramp_on = std::fabs(h->cfg.ramp_duration) < std::numeric_limits<double>::epsilon() * 100 ? 0 : 1;
     A.ramp_duration = h->cfg.ramp_duration;
+    A.went_dry = h->went_dry.p;
 }
 
 cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, int mode) {
@@ -818,6 +824,10 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
             h->device_bytes += (int64_t)3 * h->ne_pad * 8;
         }
         cudaMemset(h->limited.p, 0, h->ne_pad);
+        if (cfg->wetting_drying) {
+            if ((e = h->went_dry.alloc(h->ne_pad)) != cudaSuccess) return cleanup_fail("alloc", e);
+            cudaMemset(h->went_dry.p, 0, h->ne_pad);
+        }
         if ((e = h->status.alloc(1)) != cudaSuccess) return cleanup_fail("alloc", e);
         DevStatus z;
         std::memset(&z, 0, sizeof(z));
@@ -1139,6 +1149,9 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     h->lev.release();
     h->ldat.release();
     h->levF.release();
+    h->went_dry.release();
+    h->post.release();
+    h->post_flags.release();
     h->halo.release();
     h->tile_halo_off.release();
     h->enodes.release();
@@ -1225,6 +1238,61 @@ int32_t dgsw_rkdg_get_state(dgsw_handle h, double* q) {
     if (!h || !q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
     return download_state(h, q);
+}
+
+int32_t dgsw_rkdg_postprocess(dgsw_handle h, double* point_data, double* cell_data, uint8_t* wet, uint8_t* went_dry) {
+    if (!h || !point_data || !cell_data) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->device);
+    cudaError_t e;
+    if (!h->post.p) {
+        if ((e = h->post.alloc((size_t)h->ne * 16)) != cudaSuccess || (e = h->post_flags.alloc((size_t)h->ne * 2)) != cudaSuccess)
+            return fail(DGSW_ERR_CUDA, std::string("postprocess buffers: ") + cudaGetErrorString(e));
+        h->device_bytes += h->ne * 130;
+    }
+    // the master element's modes at the VTK points (Triangle::VTKPostPoint / VTKPostCell, N_DIV = 1)
+    const double dz = 2.0;
+    const double z1[4] = {-1.0, -1.0 + dz, -1.0, -1.0 + dz / 3.0};
+    const double z2[4] = {-1.0, -1.0, -1.0 + dz, -1.0 + dz / 3.0};
+    double phi[6 * 4];
+    eval_basis(h->cfg.p, z1, z2, 4, phi);
+    auto run = [&](auto bath_ptr) {
+        using R = typename std::remove_cv<typename std::remove_pointer<decltype(bath_ptr)>::type>::type;
+        PostArgs<R> A;
+        std::memset(&A, 0, sizeof(A));
+        A.q = (const double*)h->Q[h->stage];
+        A.bath = bath_ptr;
+        A.wet = h->wet[h->wet_cur].p;
+        A.went_dry = h->went_dry.p;
+        A.ref_of_dev = h->ref_of_dev.p;
+        for (int pt = 0; pt < 4; ++pt)
+            for (int k = 0; k < h->nd; ++k) A.phi[pt][k] = phi[k * 4 + pt];
+        A.point = h->post.p;
+        A.cell = h->post.p + (size_t)h->ne * 12;
+        A.wet_out = h->post_flags.p;
+        A.went_dry_out = h->post_flags.p + h->ne;
+        A.ne = (int)h->ne;
+        A.ne_pad = (int)h->ne_pad;
+        A.nd = h->nd;
+        return launch_postprocess<R>(A, h->stream);
+    };
+    e = h->fp32 ? run((const float*)h->bath) : run((const double*)h->bath);
+    if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("postprocess: ") + cudaGetErrorString(e));
+    CUDA_TRY(cudaMemcpyAsync(point_data, h->post.p, (size_t)h->ne * 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(cell_data, h->post.p + (size_t)h->ne * 12, (size_t)h->ne * 4 * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->stream));
+    if (wet) CUDA_TRY(cudaMemcpyAsync(wet, h->post_flags.p, (size_t)h->ne, cudaMemcpyDeviceToHost, h->stream));
+    if (went_dry)
+        CUDA_TRY(cudaMemcpyAsync(went_dry, h->post_flags.p + h->ne, (size_t)h->ne, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_get_bathymetry(dgsw_handle h, double* modes) {
+    if (!h || !modes) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<double> b;
+    project_bathymetry(h->topo, h->node_xyz.data(), h->tb, b);
+    std::memcpy(modes, b.data(), b.size() * sizeof(double));
+    return DGSW_OK;
 }
 
 int32_t dgsw_rkdg_set_wet(dgsw_handle h, const uint8_t* wet) {

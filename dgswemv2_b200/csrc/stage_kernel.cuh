@@ -106,6 +106,7 @@ struct StageArgs {
     double ramp_duration;  // days
     // levee interface fluxes of this stage, [n_levee][2][3][NG] (levee.cu): in side, then ex side
     const double* levF;
+    unsigned char* went_dry;  // [ne] wet_dry_state.went_completely_dry of the last wet/dry pass, or null
 };
 
 constexpr int FORCE_STRIDE_DEV = 9;
@@ -286,7 +287,7 @@ __device__ __forceinline__ void sine_src_eval(const SineSrc<Real>& S, Real x, Re
 // ------------------------------------------------------------------------------------------------
 template <int ND, typename Real>
 __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double bv[3], double bath_min, double h_o,
-                                               double thr, bool wet) {
+                                               double thr, bool wet, bool& went_dry) {
     double z[3], qx[3], qy[3], h[3];
     // ProjectBasisToLinear through T_basis_linear (basis_dubiner_2D.cpp:213-234)
     {
@@ -309,6 +310,7 @@ __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double b
         if (h[v] <= h_o + thr) ++ndry;
     }
     double h_avg = (0.0 + h[0] + h[1] + h[2]) / 3;
+    went_dry = h_avg <= thr;  // wet_dry_state.went_completely_dry
     if (h_avg <= thr) h_avg = thr;
     bool reproject = false, check = false;
     if (ndry == 0) {
@@ -941,7 +943,9 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     if (WD) {
         const double bv[3] = {A.nz[A.enodes[d]], A.nz[A.enodes[P_ + d]], A.nz[A.enodes[2 * P_ + d]]};
         const double bmin = fmin(bv[0], fmin(bv[1], bv[2]));
-        wet_new = wetting_drying<ND, double>(qn, bv, bmin, A.h_o, A.h_o_thr, wet);
+        bool went_dry = false;
+        wet_new = wetting_drying<ND, double>(qn, bv, bmin, A.h_o, A.h_o_thr, wet, went_dry);
+        if (A.went_dry) A.went_dry[d] = went_dry ? 1 : 0;
     }
     bool has_nan = false;
 #pragma unroll

@@ -173,6 +173,15 @@ int32_t dgsw_rkdg_init_state(dgsw_handle h);
  * they are; call dgsw_rkdg_set_wet to change them. */
 int32_t dgsw_rkdg_set_state(dgsw_handle h, const double* q);
 int32_t dgsw_rkdg_get_state(dgsw_handle h, double* q);
+/* Output values for the VTK / VTU writers (write_VTK_data / write_VTU_data,
+ * problem_postprocessor/swe_post_write_vtk.hpp:5-95, swe_post_write_vtu.hpp:5-104, N_DIV = 1), evaluated
+ * from the current state on the device, in ascending element-ID order: point_data [n_elems][3 vertices]
+ * [ze, qx, qy, bath], cell_data [n_elems][ze, qx, qy, bath] at the centroid, the wet flags and the
+ * went-completely-dry flags of the last wet/dry pass (wet and went_dry may be NULL). */
+int32_t dgsw_rkdg_postprocess(dgsw_handle h, double* point_data, double* cell_data, uint8_t* wet, uint8_t* went_dry);
+/* the bathymetry's modal L2 projection (state[0].aux, swe_pre_init_data.hpp:22-25), [n_elems][ndof] in
+ * ascending element-ID order, as the modal writer prints it (host computation, no device work) */
+int32_t dgsw_rkdg_get_bathymetry(dgsw_handle h, double* modes);
 int32_t dgsw_rkdg_set_wet(dgsw_handle h, const uint8_t* wet);
 int32_t dgsw_rkdg_get_wet(dgsw_handle h, uint8_t* wet);
 /* the same on device buffers of the library's device (layout [elem][var][dof], FP64 in both precisions:

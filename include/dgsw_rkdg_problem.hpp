@@ -78,11 +78,12 @@ class YamlNode {
     enum Kind { Null, Scalar, Map, Seq };
 
     Kind kind = Null;
+    bool defined = false;  // present in the document, even with an empty value (yaml-cpp's IsDefined)
     std::string value;
     std::vector<std::pair<std::string, YamlNode>> map;
     std::vector<YamlNode> seq;
 
-    explicit operator bool() const { return kind != Null; }
+    explicit operator bool() const { return defined || kind != Null; }
     bool IsNull() const { return kind == Null || (kind == Scalar && (value.empty() || value == "~" || value == "null")); }
 
     const YamlNode& operator[](const std::string& key) const {
@@ -193,7 +194,11 @@ inline YamlNode value_of(const std::string& raw) {
             if (!trim(item).empty()) n.seq.push_back(scalar(item));
         return n;
     }
-    if (v.empty()) return YamlNode();
+    if (v.empty()) {
+        YamlNode n;
+        n.defined = true;
+        return n;
+    }
     return scalar(v);
 }
 struct Line {
@@ -244,7 +249,9 @@ inline YamlNode parse_block(const std::vector<Line>& L, size_t& i, int indent) {
         } else if (i < L.size() && L[i].indent == indent && L[i].text.rfind("- ", 0) == 0) {
             node.map.emplace_back(key, parse_block(L, i, indent));  // "key:\n- a\n- b" at the same indent
         } else {
-            node.map.emplace_back(key, YamlNode());
+            YamlNode empty;
+            empty.defined = true;
+            node.map.emplace_back(key, empty);
         }
     }
     if (i < L.size() && L[i].indent > indent)
@@ -763,6 +770,12 @@ struct StepperInput {
 struct WriterInput {
     bool writing_output = false;
     std::string output_path;
+    bool writing_vtk_output = false;
+    double vtk_output_frequency = 0.0;
+    unsigned vtk_output_freq_step = 0;
+    bool writing_vtu_output = false;
+    double vtu_output_frequency = 0.0;
+    unsigned vtu_output_freq_step = 0;
     bool writing_modal_output = false;
     double modal_output_frequency = 0.0;
     unsigned modal_output_freq_step = 0;
@@ -820,6 +833,20 @@ struct InputParameters {
             writer_input.output_path = out["path"].as<std::string>();
             if (writer_input.output_path.empty() || writer_input.output_path.back() != '/')
                 writer_input.output_path += "/";
+            if (const YamlNode& vk = out["vtk"]) {
+                if (!vk["frequency"]) throw std::logic_error("Error: VTK YAML node is malformatted\n");
+                writer_input.writing_vtk_output = true;
+                writer_input.vtk_output_frequency = vk["frequency"].as<double>();
+                writer_input.vtk_output_freq_step =
+                    (unsigned)std::ceil(writer_input.vtk_output_frequency / stepper_input.dt);
+            }
+            if (const YamlNode& vu = out["vtu"]) {
+                if (!vu["frequency"]) throw std::logic_error("Error: VTU YAML node is malformatted\n");
+                writer_input.writing_vtu_output = true;
+                writer_input.vtu_output_frequency = vu["frequency"].as<double>();
+                writer_input.vtu_output_freq_step =
+                    (unsigned)std::ceil(writer_input.vtu_output_frequency / stepper_input.dt);
+            }
             if (const YamlNode& mo = out["modal"]) {
                 if (!mo["frequency"]) throw std::logic_error("Error: Modal YAML node is malformatted\n");
                 writer_input.writing_modal_output = true;
@@ -944,7 +971,11 @@ struct GpuDiscretization {
 
 struct GpuGlobalData {};  // SWE::GlobalData holds nothing the serial RKDG step needs
 
-/* modal output (swe_post_write_modal.hpp:6-88 writes one line per element per variable) */
+/* Writer (source/simulation/writer.hpp:100-193) with the SWE writers of problem_postprocessor/:
+ * modal (swe_post_write_modal.hpp:6-88), VTK (swe_post_write_vtk.hpp:5-95) and VTU
+ * (swe_post_write_vtu.hpp:5-104) at the reference's N_DIV = 1 (one cell per element, its three vertices as
+ * points). Field values are evaluated on the device (dgsw_rkdg_postprocess); the text formats, file names
+ * and cadence (step 0 through WriteFirstStep, then every freq_step steps) are the reference's. */
 class GpuWriter {
   public:
     GpuWriter() = default;
@@ -952,31 +983,170 @@ class GpuWriter {
     bool WritingOutput() const { return in_.writing_output; }
     bool WritingModalOutput() const { return in_.writing_modal_output; }
 
-    void WriteModal(const GpuDiscretization& d, const GpuStepper& stepper) {
-        dgsw_info info;
-        check(dgsw_rkdg_info(d.handle.get(), &info), "dgsw_rkdg_info");
-        std::vector<double> q((size_t)info.n_elems * 3 * info.ndof);
-        check(dgsw_rkdg_get_state(d.handle.get(), q.data()), "dgsw_rkdg_get_state");
-        const char* names[3] = {"ze", "qx", "qy"};
-        for (int v = 0; v < 3; ++v) {
-            std::ofstream f(in_.output_path + "modal_" + names[v] + ".txt", std::ios::app);
-            f.precision(15);
-            f << std::scientific << stepper.GetTimeAtCurrentStage() << '\n';
-            for (int64_t e = 0; e < info.n_elems; ++e) {
-                f << d.mesh.elem_names[e];
-                for (int k = 0; k < info.ndof; ++k) f << ' ' << q[((size_t)e * 3 + v) * info.ndof + k];
-                f << '\n';
-            }
-        }
-    }
+    void WriteFirstStep(const GpuDiscretization& d, const GpuStepper& stepper) { WriteOutput(d, stepper); }
 
-    void Tick(const GpuDiscretization& d, const GpuStepper& stepper) {
-        if (in_.writing_modal_output && in_.modal_output_freq_step &&
-            stepper.GetStep() % in_.modal_output_freq_step == 0)
+    void WriteOutput(const GpuDiscretization& d, const GpuStepper& stepper) {
+        const uint64_t step = (uint64_t)stepper.GetStep();
+        const bool vtk = in_.writing_vtk_output && in_.vtk_output_freq_step && step % in_.vtk_output_freq_step == 0;
+        const bool vtu = in_.writing_vtu_output && in_.vtu_output_freq_step && step % in_.vtu_output_freq_step == 0;
+        if (vtk || vtu) {
+            Fields F = fields(d);
+            if (vtk) WriteVTK(d, F, step);
+            if (vtu) WriteVTU(d, F, step);
+        }
+        if (in_.writing_modal_output && in_.modal_output_freq_step && step % in_.modal_output_freq_step == 0)
             WriteModal(d, stepper);
     }
 
+    /* write_modal_data: <mesh>_modal_{ze,qx,qy,bath}.txt, a time line (std::to_string) and one
+     * "ID value" line per element and mode; truncated at step 0, appended afterwards */
+    void WriteModal(const GpuDiscretization& d, const GpuStepper& stepper) {
+        dgsw_info info;
+        check(dgsw_rkdg_info(d.handle.get(), &info), "dgsw_rkdg_info");
+        const int nd = info.ndof;
+        std::vector<double> q((size_t)info.n_elems * 3 * nd), b((size_t)info.n_elems * nd);
+        check(dgsw_rkdg_get_state(d.handle.get(), q.data()), "dgsw_rkdg_get_state");
+        check(dgsw_rkdg_get_bathymetry(d.handle.get(), b.data()), "dgsw_rkdg_get_bathymetry");
+        const char* names[4] = {"ze", "qx", "qy", "bath"};
+        for (int v = 0; v < 4; ++v) {
+            const std::string name = in_.output_path + d.mesh.name + "_modal_" + names[v] + ".txt";
+            std::ofstream f(name, stepper.GetStep() == 0 ? std::ios::trunc : std::ios::app);
+            f << std::to_string(stepper.GetTimeAtCurrentStage()) << std::endl;
+            for (int64_t e = 0; e < info.n_elems; ++e)
+                for (int k = 0; k < nd; ++k)
+                    f << d.mesh.elem_names[e] << ' ' << std::scientific
+                      << (v < 3 ? q[((size_t)e * 3 + v) * nd + k] : b[(size_t)e * nd + k]) << std::endl;
+        }
+    }
+
+    void Tick(const GpuDiscretization& d, const GpuStepper& stepper) { WriteOutput(d, stepper); }
+
   private:
+    struct Fields {
+        std::vector<double> point, cell;  // [ne][3][4], [ne][4]: ze, qx, qy, bath
+        std::vector<uint8_t> wet, went_dry;
+    };
+
+    static Fields fields(const GpuDiscretization& d) {
+        const int64_t ne = d.mesh.n_elems();
+        Fields F;
+        F.point.resize((size_t)ne * 12);
+        F.cell.resize((size_t)ne * 4);
+        F.wet.resize((size_t)ne);
+        F.went_dry.resize((size_t)ne);
+        check(dgsw_rkdg_postprocess(d.handle.get(), F.point.data(), F.cell.data(), F.wet.data(), F.went_dry.data()),
+              "dgsw_rkdg_postprocess");
+        return F;
+    }
+
+    /* InitializeMeshGeometryVTK + write_VTK_data, merged into <mesh>_data_<step>.vtk */
+    void WriteVTK(const GpuDiscretization& d, const Fields& F, uint64_t step) {
+        const AdcircMesh& M = d.mesh;
+        const int64_t ne = M.n_elems();
+        std::ofstream f(in_.output_path + M.name + "_data_" + std::to_string(step) + ".vtk", std::ios::binary);
+        f << "# vtk DataFile Version 3.0\n";
+        f << "OUTPUT DATA\n";
+        f << "ASCII\n";
+        f << "DATASET UNSTRUCTURED_GRID\n";
+        f << "POINTS " << 3 * ne << " double\n";
+        for (int64_t e = 0; e < ne; ++e)
+            for (int k = 0; k < 3; ++k) {
+                const int32_t n = M.elem_nodes[3 * e + k];
+                f << M.node_xyz[3 * n] << '\t' << M.node_xyz[3 * n + 1] << '\t' << 0.0 << '\n';
+            }
+        f << "CELLS " << ne << ' ' << 4 * ne << '\n';
+        for (int64_t e = 0; e < ne; ++e) f << 3 << '\t' << 3 * e << '\t' << 3 * e + 1 << '\t' << 3 * e + 2 << '\t' << '\n';
+        f << "CELL_TYPES " << ne << '\n';
+        for (int64_t e = 0; e < ne; ++e) f << 5 << '\n';
+        f << "CELL_DATA " << ne << std::endl;
+        const char* cn[4] = {"ze_cell", "qx_cell", "qy_cell", "bath_cell"};
+        for (int c = 0; c < 4; ++c) {
+            f << "SCALARS " << cn[c] << " double 1" << std::endl << "LOOKUP_TABLE default" << std::endl;
+            for (int64_t e = 0; e < ne; ++e) f << (float)F.cell[(size_t)e * 4 + c] << std::endl;
+        }
+        f << "SCALARS ID unsigned_int 1" << std::endl << "LOOKUP_TABLE default" << std::endl;
+        for (int64_t e = 0; e < ne; ++e) f << M.elem_names[e] << std::endl;
+        f << "SCALARS wet_dry bit 1" << std::endl << "LOOKUP_TABLE default" << std::endl;
+        for (int64_t e = 0; e < ne; ++e) f << (F.wet[e] != 0) << std::endl;
+        f << "SCALARS went_completely_dry bit 1" << std::endl << "LOOKUP_TABLE default" << std::endl;
+        for (int64_t e = 0; e < ne; ++e) f << (F.went_dry[e] != 0) << std::endl;
+        f << "POINT_DATA " << 3 * ne << std::endl;
+        const char* pn[4] = {"ze_point", "qx_point", "qy_point", "bath_point"};
+        for (int c = 0; c < 4; ++c) {
+            f << "SCALARS " << pn[c] << " double 1" << std::endl << "LOOKUP_TABLE default" << std::endl;
+            for (size_t i = 0; i < (size_t)ne * 3; ++i) f << (float)F.point[i * 4 + c] << std::endl;
+        }
+    }
+
+    /* InitializeMeshGeometryVTU (head, foot) + write_VTU_data, merged into <mesh>_data_<step>.vtu */
+    void WriteVTU(const GpuDiscretization& d, const Fields& F, uint64_t step) {
+        const AdcircMesh& M = d.mesh;
+        const int64_t ne = M.n_elems();
+        std::ofstream f(in_.output_path + M.name + "_data_" + std::to_string(step) + ".vtu", std::ios::binary);
+        f << "<?xml version=\"1.0\"?>\n";
+        f << "<VTKFile type=\"UnstructuredGrid\">\n";
+        f << "\t<UnstructuredGrid>\n";
+        f << "\t\t<Piece NumberOfPoints=\"" << 3 * ne << "\" NumberOfCells=\"" << ne << "\">\n";
+        auto open = [&](const char* type, const char* name) {
+            f << "\t\t\t\t<DataArray type=\"" << type << "\" Name=\"" << name << "\" format=\"ascii\">\n\t\t\t\t\t";
+        };
+        auto close = [&]() { f << "\n\t\t\t\t</DataArray>\n"; };
+        f << "\t\t\t<PointData>\n";
+        const char* pn[4] = {"ze_point", "qx_point", "qy_point", "bath_point"};
+        for (int c = 0; c < 4; ++c) {
+            open("Float32", pn[c]);
+            for (size_t i = 0; i < (size_t)ne * 3; ++i) f << (float)F.point[i * 4 + c] << ' ';
+            close();
+        }
+        open("Float32", "velocity_point");
+        for (size_t i = 0; i < (size_t)ne * 3; ++i) {
+            const double* v = &F.point[i * 4];
+            f << (float)(std::hypot(v[1], v[2]) / (v[0] + v[3])) << ' ';
+        }
+        close();
+        f << "\t\t\t</PointData>\n";
+        f << "\t\t\t<CellData>\n";
+        const char* cn[4] = {"ze_cell", "qx_cell", "qy_cell", "bath_cell"};
+        for (int c = 0; c < 4; ++c) {
+            open("Float32", cn[c]);
+            for (int64_t e = 0; e < ne; ++e) f << (float)F.cell[(size_t)e * 4 + c] << ' ';
+            close();
+        }
+        open("UInt32", "ID");
+        for (int64_t e = 0; e < ne; ++e) f << M.elem_names[e] << ' ';
+        close();
+        open("Int8", "wet_dry");
+        for (int64_t e = 0; e < ne; ++e) f << (F.wet[e] != 0) << ' ';
+        close();
+        open("Int8", "went_completely_dry");
+        for (int64_t e = 0; e < ne; ++e) f << (F.went_dry[e] != 0) << ' ';
+        close();
+        f << "\t\t\t</CellData>\n";
+        f << "\t\t\t<Points>\n";
+        f << "\t\t\t\t<DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n\t\t\t\t\t";
+        for (int64_t e = 0; e < ne; ++e)
+            for (int k = 0; k < 3; ++k) {
+                const int32_t n = M.elem_nodes[3 * e + k];
+                f << M.node_xyz[3 * n] << ' ' << M.node_xyz[3 * n + 1] << ' ' << 0.0 << ' ';
+            }
+        f << "\n\t\t\t\t</DataArray>\n";
+        f << "\t\t\t</Points>\n";
+        f << "\t\t\t<Cells>\n";
+        f << "\t\t\t\t<DataArray type=\"Int32\" Name=\"connectivity\" format=\"ascii\">\n\t\t\t\t\t";
+        for (int64_t e = 0; e < ne; ++e) f << 3 * e << ' ' << 3 * e + 1 << ' ' << 3 * e + 2 << ' ';
+        f << "\n\t\t\t\t</DataArray>\n";
+        f << "\t\t\t\t<DataArray type=\"Int32\" Name=\"offsets\" format=\"ascii\">\n\t\t\t\t\t";
+        for (int64_t e = 0; e < ne; ++e) f << 3 * (e + 1) << ' ';
+        f << "\n\t\t\t\t</DataArray>\n";
+        f << "\t\t\t\t<DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\">\n\t\t\t\t\t";
+        for (int64_t e = 0; e < ne; ++e) f << 5 << ' ';
+        f << "\n\t\t\t\t</DataArray>\n";
+        f << "\t\t\t</Cells>\n";
+        f << "\t\t</Piece>\n";
+        f << "\t</UnstructuredGrid>\n";
+        f << "</VTKFile>\n";
+    }
+
     WriterInput in_;
 };
 
@@ -1057,6 +1227,7 @@ class GpuSimulation {
 
     void Run() {
         ProblemType::preprocessor_serial(discretization_, global_data_, stepper_, input_.problem_input);
+        if (writer_.WritingOutput()) writer_.WriteFirstStep(discretization_, stepper_);
         for (uint64_t step = 1; step <= n_steps_; ++step)
             ProblemType::step_serial(discretization_, global_data_, stepper_, writer_);
     }

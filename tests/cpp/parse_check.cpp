@@ -40,6 +40,10 @@ int main(int argc, char** argv) {
                   << "sl_M " << pi.sl_M << "\n"
                   << "sl_nu " << pi.sl_nu << "\n"
                   << "spherical " << pi.spherical << "\n"
+                  << "writing_vtk " << in.writer_input.writing_vtk_output << " "
+                  << in.writer_input.vtk_output_freq_step << "\n"
+                  << "writing_vtu " << in.writer_input.writing_vtu_output << " "
+                  << in.writer_input.vtu_output_freq_step << "\n"
                   << "writing_modal " << in.writer_input.writing_modal_output << " "
                   << in.writer_input.modal_output_freq_step << "\n"
                   << "function_set " << in.b200.function_set << "\n"

@@ -262,6 +262,17 @@ output:
 """
 
 
+def read_modal_last(path, ne, nd):
+    """The last block of a write_modal_data file: its time and the modes [ne][nd] (elements in file order)."""
+    lines = [l for l in open(path).read().split("\n") if l]
+    block = ne * nd + 1
+    assert len(lines) % block == 0, (len(lines), block)
+    last = lines[-block:]
+    vals = np.array([float(l.split()[1]) for l in last[1:]]).reshape(ne, nd)
+    ids = np.array([int(l.split()[0]) for l in last[1:]]).reshape(ne, nd)
+    return float(last[0]), vals, ids
+
+
 def write_tide_input(d, mesh):
     path = write_input(d, mesh, TIDE_15, mesh_name="channel.14")
     meshgen.write_bcis(mesh, os.path.join(d, "channel.bcis"))
@@ -336,12 +347,10 @@ def test_serial_driver_runs_tidal_channel(tmp_path):
     P = Problem(cfg, mesh)
     P.step_serial(300)
     q = P.get_state()
-    lines = open(os.path.join(d, "out", "modal_ze.txt")).read().split("\n")
-    t_idx = [i for i, l in enumerate(lines) if l and len(l.split()) == 1]
-    last = lines[t_idx[-1] + 1: t_idx[-1] + 1 + mesh.n_elems]
-    ze = np.array([[float(v) for v in l.split()[1:]] for l in last])
-    assert abs(float(lines[t_idx[-1]]) - 300.0) < 1e-9
-    assert np.allclose(ze, q[:, 0, :], rtol=1e-14, atol=1e-15)
+    t, ze, ids = read_modal_last(os.path.join(d, "out", mesh.name + "_modal_ze.txt"), mesh.n_elems, P.nd)
+    assert t == 300.0 and np.array_equal(ids[:, 0], np.arange(mesh.n_elems))
+    # six significant digits (std::scientific), as the reference prints them
+    assert np.allclose(ze, q[:, 0, :], rtol=2e-6, atol=1e-6 * np.abs(q[:, 0, :]).max())
 
 
 LEVEE_15 = TIDE_15.replace("  bottom_friction:\n    type: Manning\n    coefficient: 0.0005\n    input_file: manning.dat\n",
@@ -383,8 +392,86 @@ def test_serial_driver_runs_levee_channel(tmp_path):
     P = Problem(cfg, mesh)
     P.step_serial(300)
     q = P.get_state()
-    lines = open(os.path.join(d, "out", "modal_ze.txt")).read().split("\n")
-    t_idx = [i for i, l in enumerate(lines) if l and len(l.split()) == 1]
-    last = lines[t_idx[-1] + 1: t_idx[-1] + 1 + mesh.n_elems]
-    ze = np.array([[float(v) for v in l.split()[1:]] for l in last])
-    assert np.allclose(ze, q[:, 0, :], rtol=1e-14, atol=1e-15)
+    t, ze, _ = read_modal_last(os.path.join(d, "out", mesh.name + "_modal_ze.txt"), mesh.n_elems, P.nd)
+    assert t == 300.0
+    assert np.allclose(ze, q[:, 0, :], rtol=2e-6, atol=1e-6 * np.abs(q[:, 0, :]).max())
+
+
+VTK_15 = LEVEE_15.replace("  modal:\n    frequency: 300\n", "  vtk:\n    frequency: 300\n  vtu:\n    frequency: 300\n  modal:\n    frequency: 300\n").replace(
+    "    initial_momentum_y: 0.0\n", "    initial_momentum_y: 0.0\n  wetting_drying:\n    h_o: 0.01\n")
+
+
+def test_parse_vtk_vtu_output_nodes(parse_check, tmp_path):
+    mesh, cfg = configs.levee_channel(dry_right=True)
+    d = str(tmp_path)
+    path = write_input(d, mesh, VTK_15.replace("  vtu:\n    frequency: 300\n", "  vtu:\n    frequency: 150.5\n"),
+                       mesh_name="channel.14")
+    rc, out, err = run_check(parse_check, path)
+    assert rc == 0, (out, err)
+    assert out["writing_vtk"] == "1 300" and out["writing_vtu"] == "1 151" and out["writing_modal"] == "1 300"
+    rc, out, _ = run_check(parse_check, write_input(d, mesh, VTK_15.replace("  vtk:\n    frequency: 300\n", "  vtk:\n")))
+    assert rc == 3 and "VTK YAML node is malformatted" in out["error"]
+
+
+def _vtk_sections(path):
+    lines = open(path).read().split("\n")
+    out, i = {}, 0
+    while i < len(lines):
+        l = lines[i]
+        if l.startswith("SCALARS "):
+            name = l.split()[1]
+            j = i + 2
+            vals = []
+            while j < len(lines) and lines[j] and not lines[j][0].isalpha():
+                vals.append(float(lines[j]))
+                j += 1
+            out[name] = np.array(vals)
+            i = j
+        else:
+            i += 1
+    return out, lines
+
+
+@pytest.mark.gpu
+def test_serial_driver_writes_vtk_vtu_and_modal(tmp_path, oracle):
+    """VTK / VTU / modal output of dgswemv2-b200-serial on the levee channel flooding dry land: files at
+    steps 0 and 300 named like the reference's; the VTK cell and point values equal the state evaluated
+    with the oracle's Dubiner basis at the centroids and vertices (to the printed float digits); IDs,
+    wet flags and the VTU arrays agree."""
+    mesh, cfg = configs.levee_channel(dry_right=True)
+    d = str(tmp_path)
+    path = write_input(d, mesh, VTK_15, mesh_name="channel.14")
+    meshgen.write_bcis(mesh, os.path.join(d, "channel.bcis"))
+    os.makedirs(os.path.join(d, "out"), exist_ok=True)
+    r = subprocess.run([CLI, path], capture_output=True, text=True, timeout=300, cwd=d)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for step in (0, 300):
+        for ext in ("vtk", "vtu"):
+            assert os.path.exists(os.path.join(d, "out", "%s_data_%d.%s" % (mesh.name, step, ext)))
+    for v in ("ze", "qx", "qy", "bath"):
+        assert os.path.exists(os.path.join(d, "out", "%s_modal_%s.txt" % (mesh.name, v)))
+    P = Problem(cfg, mesh)
+    P.step_serial(300)
+    q = P.get_state()
+    nd = P.nd
+    phi_c = oracle.dubiner(cfg.p, np.array([[-1.0 + 2.0 / 3.0, -1.0 + 2.0 / 3.0]]))[0][:, 0]
+    phi_v = oracle.dubiner(cfg.p, np.array([[-1.0, -1.0], [1.0, -1.0], [-1.0, 1.0]]))[0]
+    sec, lines = _vtk_sections(os.path.join(d, "out", "%s_data_300.vtk" % mesh.name))
+    ne = mesh.n_elems
+    for k, v in enumerate(("ze", "qx", "qy")):
+        cell = q[:, k, :] @ phi_c[:nd]
+        scale = max(np.abs(cell).max(), 1e-30)
+        assert np.allclose(sec[v + "_cell"], cell, rtol=1e-5, atol=1e-6 * scale), v
+        pts = (q[:, k, :] @ phi_v[:nd, :]).reshape(-1)
+        assert np.allclose(sec[v + "_point"], pts, rtol=1e-5, atol=1e-6 * max(np.abs(pts).max(), 1e-30)), v
+    assert np.array_equal(sec["ID"], np.arange(ne))
+    assert np.array_equal(sec["wet_dry"].astype(np.uint8), P.get_wet())
+    assert 0 < P.get_wet().sum() < ne
+    assert "POINTS %d double" % (3 * ne) in lines and "CELL_TYPES %d" % ne in lines
+    vtu = open(os.path.join(d, "out", "%s_data_300.vtu" % mesh.name)).read()
+    assert '<Piece NumberOfPoints="%d" NumberOfCells="%d">' % (3 * ne, ne) in vtu
+    ze_cell = np.array(vtu.split('Name="ze_cell" format="ascii">')[1].split("</DataArray>")[0].split(), float)
+    assert np.allclose(ze_cell, sec["ze_cell"])
+    pt, cell, wet, wd = P.postprocess()
+    assert np.allclose(cell[:, 0], sec["ze_cell"], rtol=1e-5, atol=1e-6)
+    assert np.array_equal(wet, P.get_wet())
