@@ -7,6 +7,9 @@ config2: manufactured sine, 524,288 jittered triangles, p = 2, SSP-RK3
 config3: Thacker bowl, 131,072 triangles, p = 1, SSP-RK2, wetting/drying + Cockburn-Shu limiter
 config3_nolim: the same without the limiter
 config4: Thacker bowl, 2,097,152 triangles, p = 1, SSP-RK2, wetting/drying + limiter
+tidal_p1 / tidal_p2: 100 km x 25 km tidal channel, 524,288 triangles, M2 + K1 tide, river flow, Manning
+  friction, forcing ramp (p = 1 SSP-RK2 dt = 0.5 s / p = 2 SSP-RK3 dt = 0.25 s)
+levee_p1: the same channel cut across by a levee (256 levee interfaces), p = 1, SSP-RK2, dt = 0.5 s
 Prints one JSON line per (configuration, precision): device ms per step after warm-up (CUDA events on
 the handle's stream around graph-replayed steps), element-DOF updates per second per RK stage, and the
 L2 error against the analytic solution at the end.
@@ -28,6 +31,13 @@ def build(name, precision):
         return configs.config3(precision=precision, limiter=False)
     if name == "config4":
         return configs.config3(nq=1024, dt=0.06, precision=precision)
+    big = dict(nx=1024, ny=256, length=1.0e5, width=2.5e4, precision=precision)
+    if name == "tidal_p1":
+        return configs.tidal_channel(p=1, rk=(2, 2), dt=0.5, friction="manning", cf=0.0005, **big)
+    if name == "tidal_p2":
+        return configs.tidal_channel(p=2, rk=(3, 3), dt=0.25, friction="manning", cf=0.0005, **big)
+    if name == "levee_p1":
+        return configs.levee_channel(p=1, rk=(2, 2), dt=0.5, **big)
     raise ValueError(name)
 
 
@@ -48,7 +58,8 @@ def measure(name, precision, steps, warmup=5):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("configs", nargs="*", default=["config1", "config2", "config3", "config3_nolim", "config4"])
+    ap.add_argument("configs", nargs="*", default=["config1", "config2", "config3", "config3_nolim", "config4", "tidal_p1",
+                                                   "tidal_p2", "levee_p1"])
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--precisions", default="fp32,fp64")
     a = ap.parse_args()
