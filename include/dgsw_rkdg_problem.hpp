@@ -2,11 +2,14 @@
  *
  * Mirrors the reference's serial driver stack for the `rkdg_swe` problem:
  *   InputParameters        source/preprocessor/input_parameters.hpp:72-261 (the `.15` YAML file)
- *   SWE::Inputs            source/problem/SWE/problem_input/swe_inputs.{hpp:125-158, cpp:4-205}
+ *   SWE::Inputs            source/problem/SWE/problem_input/swe_inputs.{hpp:125-158, cpp:4-205}, read_bcis
+ *                          (cpp:211-290), the Manning n file (swe_pre_init_data.hpp:165-182)
  *   AdcircFormat           source/preprocessor/ADCIRC_reader/adcirc_format.cpp:3-130, 214-254
  *   ESSPRKStepper queries  source/simulation/stepper/explicit_ssp_rk_stepper.hpp:36-65
  *   SWE::RKDG::Problem     source/problem/SWE/discretization_RKDG/rkdg_swe_problem.hpp:34-194
  *   Serial::Simulation     source/simulation/serial/simulation.hpp:14-93
+ *   Writer                 source/simulation/writer.hpp:100-193 with the modal / VTK / VTU writers of
+ *                          source/problem/SWE/problem_postprocessor/
  * so that a caller of SWE::RKDG::Problem / Serial::Simulation<SWE::RKDG::Problem> switches to
  * SWE::RKDG::GpuProblem / Serial::GpuSimulation<SWE::RKDG::GpuProblem>. All arithmetic of the step runs
  * in libdgsw_rkdg.so on the GPU; this header only parses input, owns the handle and forwards calls.
