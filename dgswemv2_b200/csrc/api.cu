@@ -224,7 +224,7 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.fn_set = h->cfg.function_set;
     for (int i = 0; i < 16; ++i) A.fn_params[i] = h->cfg.fn_params[i];
     A.spherical = h->cfg.spherical;
-    A.sp_cos_lat0 = std::cos(h->cfg.sp_lat0_deg * M_PI / 180.0);
+    A.sp_cos_lat0 = std::cos(h->cfg.sp_lat0_deg * 3.14159265359 / 180.0);  // the reference's PI
     A.sp_R = h->cfg.sp_R;
     A.friction = h->cfg.bottom_friction;
     A.friction_cf = h->cfg.friction_cf;

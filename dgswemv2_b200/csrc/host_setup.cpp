@@ -716,7 +716,7 @@ int build_levees(const dgsw_mesh* m, const Topology& T, int p, const double* X, 
     for (int32_t k = 0; k < m->n_levee_pairs; ++k) data[{m->levee_nodes[2 * k], m->levee_nodes[2 * k + 1]}] = k;
     const Rule1D gl = gauss_legendre_degree(2 * p + 1);
     const int ng = (int)gl.z.size();
-    const double cos_lat0 = std::cos(cfg.sp_lat0_deg * M_PI / 180.0);
+    const double cos_lat0 = std::cos(cfg.sp_lat0_deg * 3.14159265359 / 180.0);  // the reference's PI
     out.assign((size_t)LEVEE_STRIDE * n_lev, 0.0);
     for (int64_t l = 0; l < n_lev; ++l) {
         const int64_t i = T.n_intf_internal + l;

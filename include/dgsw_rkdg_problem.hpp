@@ -926,6 +926,24 @@ class GpuStepper {
     dgsw_handle h_ = nullptr;
 };
 
+/* SWE::preprocess_mesh_data (swe_pre_preprocess_mesh.hpp:6-27): a mesh in spherical coordinates
+ * (longitude, latitude in degrees) is projected onto the cylinder through (longitude_o, latitude_o),
+ * with the reference's PI = 3.14159265359 */
+inline void project_spherical(const InputParameters& input, AdcircMesh& mesh) {
+    if (input.mesh_input.coordinate_system != "spherical") return;
+    const SWEInputs& pi = input.problem_input;
+    if (!pi.spherical) {
+        std::cerr << "Warning: Spherical projection input not provided! Using default values to perfrom projection!\n";
+        std::cerr << "Consider using spherical projection to account for geometric distortion!\n";
+    }
+    constexpr double PI = 3.14159265359;
+    const double R_o = pi.R * std::cos(pi.latitude_o * PI / 180.0);
+    for (size_t n = 0; n < mesh.node_names.size(); ++n) {
+        mesh.node_xyz[3 * n] = R_o * (mesh.node_xyz[3 * n] - pi.longitude_o) * PI / 180.0;
+        mesh.node_xyz[3 * n + 1] = pi.R * mesh.node_xyz[3 * n + 1] * PI / 180.0;
+    }
+}
+
 /* DGDiscretization<Problem>: the mesh plus the library handle that holds all element data */
 struct GpuDiscretization {
     AdcircMesh mesh;
@@ -934,6 +952,7 @@ struct GpuDiscretization {
 
     void initialize(const InputParameters& input) {
         mesh = read_adcirc(input_relative(input.input_dir, input.mesh_input.mesh_file_name));
+        project_spherical(input, mesh);
         // Simulation ctor: input.read_bcis(); initialize_data_serial: the Manning n file
         read_bcis(input_relative(input.input_dir, input.mesh_input.bc_is_file_name), mesh);
         if (input.problem_input.bottom_friction == DGSW_FRICTION_MANNING)
@@ -1176,8 +1195,9 @@ struct GpuProblem {
      * handle's configuration instead of process-wide statics */
     static void initialize_problem_parameters(const ProblemInputType&) {}
 
-    /* SWE::preprocess_mesh_data: the spherical projection is applied by the library; the .bcis tide / flow
-     * data and the Manning n file are read when the discretization is initialised (GpuDiscretization) */
+    /* SWE::preprocess_mesh_data: the node projection of spherical meshes, the .bcis tide / flow / levee
+     * data and the Manning n file are applied / read when the discretization is initialised
+     * (GpuDiscretization::initialize) */
     static void preprocess_mesh_data(ProblemInputParametersType&) {}
 
     /* swe_pre_serial.hpp: initial projections, wet/dry and limiter initialisation on the device */

@@ -847,7 +847,7 @@ int build(Problem& P, const orc_config* cfg, const orc_mesh* m) {
     for (int i = 0; i < (int)P.bnds.size(); ++i) P.contrib[P.bnds[i].elt].push_back({1, i, 0});
 
     // ---------------- initialize_data_serial, swe_pre_init_data.hpp:9-327 ----------------
-    const double cos_phi_o = std::cos(cfg->sp_lat0_deg * M_PI / 180.0);
+    const double cos_phi_o = std::cos(cfg->sp_lat0_deg * REF_PI / 180.0);  // swe_pre_init_data.hpp:40
     auto sp_of = [&](double y) { return cfg->spherical ? cos_phi_o / std::cos(y / cfg->sp_R) : 1.0; };
     vector<double> psi_gp(3 * ngp);  // shape.psi_gp (node x gp)
     for (int gp = 0; gp < ngp; ++gp) {

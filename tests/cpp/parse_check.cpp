@@ -54,6 +54,8 @@ int main(int argc, char** argv) {
                   << "ramp_duration " << in.stepper_input.ramp_duration << "\n";
         dgsw::AdcircMesh M = dgsw::read_adcirc(dgsw::input_relative(in.input_dir, in.mesh_input.mesh_file_name));
         dgsw::read_bcis(dgsw::input_relative(in.input_dir, in.mesh_input.bc_is_file_name), M);
+        dgsw::project_spherical(in, M);
+        std::cout << "projected_xyz_hash " << fnv(M.node_xyz.data(), M.node_xyz.size() * 8) << "\n";
         if (pi.bottom_friction == DGSW_FRICTION_MANNING)
             dgsw::read_manning(dgsw::input_relative(in.input_dir, pi.manning_data_file), M);
         std::cout << "n_forcing " << M.forcing.size() << "\n";

@@ -475,3 +475,23 @@ def test_serial_driver_writes_vtk_vtu_and_modal(tmp_path, oracle):
     pt, cell, wet, wd = P.postprocess()
     assert np.allclose(cell[:, 0], sec["ze_cell"], rtol=1e-5, atol=1e-6)
     assert np.array_equal(wet, P.get_wet())
+
+
+def test_spherical_mesh_is_projected(parse_check, tmp_path):
+    """coordinate_system: spherical projects (longitude, latitude) onto the cylinder through
+    (longitude_o, latitude_o) as SWE::preprocess_mesh_data does, with the reference's PI."""
+    mesh, _ = configs.config1()
+    lon = -95.0 + mesh.node_xyz[:, 0] / 40000.0
+    lat = 28.0 + mesh.node_xyz[:, 1] / 40000.0
+    mesh.node_xyz = np.stack([lon, lat, mesh.node_xyz[:, 2]], 1)
+    body = CONFIG1_15.replace("cartesian", "spherical").replace(
+        "  gravity: 9.81\n", "  gravity: 9.81\n  spherical_projection:\n    longitude_o: -94.5\n    latitude_o: 28.5\n    R: 6378200.0\n")
+    rc, out, err = run_check(parse_check, write_input(str(tmp_path), mesh, body))
+    assert rc == 0, (out, err)
+    PI = 3.14159265359
+    R_o = 6378200.0 * np.cos(28.5 * PI / 180.0)
+    xyz = mesh.node_xyz.copy()
+    xyz[:, 0] = R_o * (lon - (-94.5)) * PI / 180.0
+    xyz[:, 1] = 6378200.0 * lat * PI / 180.0
+    assert out["projected_xyz_hash"] == fnv(xyz)
+    assert out["spherical"] == "1"
