@@ -711,6 +711,7 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         std::vector<double> bdev((size_t)3 * h->ne_pad, 0.0);
         std::vector<double> gdev((size_t)5 * h->ne_pad, 0.0);
         std::vector<int> nb((size_t)3 * h->ne_pad, -1);
+#pragma omp parallel for schedule(static)
         for (int64_t d = 0; d < h->ne; ++d) {
             int64_t r = h->tiling.ref_of_dev[d];
             for (int v = 0; v < 3; ++v) {
@@ -731,11 +732,14 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         if ((e = h->nbr.alloc(nb.size())) != cudaSuccess) return cleanup_fail("alloc", e);
         cudaMemcpy(h->nbr.p, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice);
         std::vector<double> edev((size_t)3 * std::max<size_t>(n_edges, 1), 0.0);
-        for (size_t i = 0; i < n_edges; ++i)
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)n_edges; ++i)
             for (int c = 0; c < 3; ++c) edev[c * n_edges + i] = h->tiling.egeo[3 * i + c];
         auto upload_real = [&](void* dst, const std::vector<double>& src) {
             if (h->fp32) {
-                std::vector<float> f(src.begin(), src.end());
+                std::vector<float> f(src.size());
+#pragma omp parallel for schedule(static)
+                for (int64_t i = 0; i < (int64_t)src.size(); ++i) f[i] = (float)src[i];
                 cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
             } else {
                 cudaMemcpy(dst, src.data(), src.size() * sizeof(double), cudaMemcpyHostToDevice);

@@ -9,6 +9,11 @@
 #include <numeric>
 #include <unordered_map>
 
+#ifdef _OPENMP
+#include <omp.h>
+#include <parallel/algorithm>
+#endif
+
 #include "function_sets.h"
 #include "quadrature.h"
 
@@ -86,6 +91,16 @@ static void dubiner_eval(int dof, double z1, double z2, double& phi, double& d1,
         d1 = (p == 1) ? sing_dz1(q) : 0.0;
         d2 = (p == 0) ? 3 * sing_dz2(q) : (p == 1 ? sing_dz2(q + 1) : 0.0);
     }
+}
+
+// sort with a strict total order: the parallel sort (OpenMP builds) gives the sequential result
+template <typename It, typename Cmp>
+static void total_sort(It b, It e, Cmp cmp) {
+#ifdef _OPENMP
+    __gnu_parallel::sort(b, e, cmp);
+#else
+    std::sort(b, e, cmp);
+#endif
 }
 
 static void face_to_master(int f, double z, double& z1, double& z2) {
@@ -183,37 +198,53 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
     }
     T.ne = ne;
     T.nn = m->n_nodes;
-    std::vector<std::pair<uint32_t, int32_t>> ord(ne);
+    bigvec<std::pair<uint32_t, int32_t>> ord(ne);
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < ne; ++i) ord[i] = {m->elem_ids ? m->elem_ids[i] : (uint32_t)i, (int32_t)i};
-    std::sort(ord.begin(), ord.end());
+    if (!std::is_sorted(ord.begin(), ord.end())) total_sort(ord.begin(), ord.end(), std::less<std::pair<uint32_t, int32_t>>());
     T.ids.resize(ne);
     T.src.resize(ne);
     T.enodes.resize(3 * ne);
+    // checked in parallel; the first failing element (in ID order) is reported, as a serial scan would
+    int64_t bad_dup = ne, bad_node = ne, bad_ccw = ne;
+#pragma omp parallel for schedule(static) reduction(min : bad_dup, bad_node, bad_ccw)
     for (int64_t r = 0; r < ne; ++r) {
-        if (r > 0 && ord[r].first == ord[r - 1].first) {
-            err = "Fatal Error: duplicate element ID " + std::to_string(ord[r].first);
-            return DGSW_ERR_MESH;
-        }
+        if (r > 0 && ord[r].first == ord[r - 1].first) bad_dup = std::min(bad_dup, r);
         T.ids[r] = ord[r].first;
         T.src[r] = ord[r].second;
+        bool ok = true;
         for (int v = 0; v < 3; ++v) {
             int32_t n = m->elem_nodes[3 * (int64_t)ord[r].second + v];
             if (n < 0 || n >= m->n_nodes) {
-                err = "Fatal Error: element node index out of range";
-                return DGSW_ERR_MESH;
+                ok = false;
+                n = 0;
             }
             T.enodes[3 * r + v] = n;
+        }
+        if (!ok) {
+            bad_node = std::min(bad_node, r);
+            continue;
         }
         const double* X = m->node_xyz;
         const int32_t* nd = &T.enodes[3 * r];
         double det = (X[3 * nd[1]] - X[3 * nd[0]]) * (X[3 * nd[2] + 1] - X[3 * nd[0] + 1]) -
                      (X[3 * nd[1] + 1] - X[3 * nd[0] + 1]) * (X[3 * nd[2]] - X[3 * nd[0]]);
-        if (!(det > 0)) {
-            err = "element " + std::to_string(T.ids[r]) +
-                  " is not counter-clockwise (or degenerate); reorder its nodes (the reference swaps coordinates "
-                  "but not node IDs for such elements, which this library does not reproduce)";
-            return DGSW_ERR_UNSUPPORTED;
+        if (!(det > 0)) bad_ccw = std::min(bad_ccw, r);
+    }
+    const int64_t first_bad = std::min(bad_dup, std::min(bad_node, bad_ccw));
+    if (first_bad < ne) {
+        if (first_bad == bad_dup) {
+            err = "Fatal Error: duplicate element ID " + std::to_string(ord[first_bad].first);
+            return DGSW_ERR_MESH;
         }
+        if (first_bad == bad_node) {
+            err = "Fatal Error: element node index out of range";
+            return DGSW_ERR_MESH;
+        }
+        err = "element " + std::to_string(T.ids[first_bad]) +
+              " is not counter-clockwise (or degenerate); reorder its nodes (the reference swaps coordinates "
+              "but not node IDs for such elements, which this library does not reproduce)";
+        return DGSW_ERR_UNSUPPORTED;
     }
     // face keys
     struct FK {
@@ -221,13 +252,14 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
         int32_t r;
         int8_t f;
     };
-    std::vector<FK> fk(3 * ne);
+    bigvec<FK> fk(3 * ne);
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < ne; ++r)
         for (int f = 0; f < 3; ++f) {
             uint32_t a = (uint32_t)T.enodes[3 * r + (f + 1) % 3], b = (uint32_t)T.enodes[3 * r + (f + 2) % 3];
             fk[3 * r + f] = {(uint64_t)std::min(a, b) << 32 | std::max(a, b), (int32_t)r, (int8_t)f};
         }
-    std::sort(fk.begin(), fk.end(), [](const FK& x, const FK& y) {
+    total_sort(fk.begin(), fk.end(), [](const FK& x, const FK& y) {
         return x.key != y.key ? x.key < y.key : (x.r != y.r ? x.r < y.r : x.f < y.f);
     });
     T.nbr.assign(3 * ne, -1);
@@ -357,26 +389,41 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
     // interfaces in (in, ex) order, in = smaller reference ID (swe_pre_create_intface.hpp:14-34): the
     // internal ones, then the levee ones (ProblemInterfaceTypes order)
     T.intf.clear();
-    std::vector<int64_t> intf_of_face(3 * ne, -1);
-    for (int kind : {(int)DGSW_BC_INTERNAL, (int)DGSW_BC_LEVEE}) {
-        if (kind == DGSW_BC_LEVEE) T.n_intf_internal = (int64_t)T.intf.size() / 4;
-        for (int64_t r = 0; r < ne; ++r) {
-            // faces of r with a larger neighbour, ordered by the neighbour
-            int fs[3], n = 0;
-            for (int f = 0; f < 3; ++f)
-                if (T.nbr[3 * r + f] > r && T.btype[3 * r + f] == kind) fs[n++] = f;
-            std::sort(fs, fs + n, [&](int a, int b) { return T.nbr[3 * r + a] < T.nbr[3 * r + b]; });
-            for (int k = 0; k < n; ++k) {
-                int f = fs[k];
-                int32_t e = T.nbr[3 * r + f];
-                int fe = T.nbr_face[3 * r + f];
-                int64_t idx = (int64_t)T.intf.size() / 4;
-                T.intf.push_back((int32_t)r);
-                T.intf.push_back(e);
-                T.intf.push_back(f);
-                T.intf.push_back(fe);
-                intf_of_face[3 * r + f] = idx;
-                intf_of_face[3 * (int64_t)e + fe] = idx;
+    std::vector<int32_t> intf_of_face(3 * ne, -1);
+    {
+        // counts per element, prefix sums, then each element writes its own interfaces in place
+        std::vector<int32_t> cnt(2 * ne + 1, 0);
+        const int kinds[2] = {DGSW_BC_INTERNAL, DGSW_BC_LEVEE};
+#pragma omp parallel for schedule(static)
+        for (int64_t r = 0; r < ne; ++r)
+            for (int k = 0; k < 2; ++k) {
+                int n = 0;
+                for (int f = 0; f < 3; ++f) n += (T.nbr[3 * r + f] > r && T.btype[3 * r + f] == kinds[k]) ? 1 : 0;
+                cnt[k * ne + r + 1] = n;
+            }
+        for (int64_t i = 0; i < 2 * ne; ++i) cnt[i + 1] += cnt[i];
+        T.n_intf_internal = cnt[ne];
+        T.intf.resize((size_t)4 * cnt[2 * ne]);
+        for (int k = 0; k < 2; ++k) {
+#pragma omp parallel for schedule(static)
+            for (int64_t r = 0; r < ne; ++r) {
+                // faces of r with a larger neighbour, ordered by the neighbour
+                int fs[3], n = 0;
+                for (int f = 0; f < 3; ++f)
+                    if (T.nbr[3 * r + f] > r && T.btype[3 * r + f] == kinds[k]) fs[n++] = f;
+                std::sort(fs, fs + n, [&](int a, int b) { return T.nbr[3 * r + a] < T.nbr[3 * r + b]; });
+                int32_t idx = cnt[k * ne + r];
+                for (int j = 0; j < n; ++j, ++idx) {
+                    const int f = fs[j];
+                    const int32_t e = T.nbr[3 * r + f];
+                    const int fe = T.nbr_face[3 * r + f];
+                    T.intf[4 * (size_t)idx] = (int32_t)r;
+                    T.intf[4 * (size_t)idx + 1] = e;
+                    T.intf[4 * (size_t)idx + 2] = f;
+                    T.intf[4 * (size_t)idx + 3] = fe;
+                    intf_of_face[3 * r + f] = idx;
+                    intf_of_face[3 * (int64_t)e + fe] = idx;
+                }
             }
         }
     }
@@ -397,6 +444,7 @@ int build_topology(const dgsw_mesh* m, Topology& T, std::string& err) {
     T.order_count.assign(ne, 0);
     T.order_face.assign(3 * ne, 0);
     T.is_in.assign(3 * ne, 0);
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < ne; ++r) {
         std::pair<int64_t, int> items[3];
         int n = 0;
@@ -456,6 +504,34 @@ void face_geometry(const double* X, const int32_t* nd, int f, double& nx, double
     sJ = std::sqrt(std::pow(dx, 2.0) + std::pow(dy, 2.0)) / 2.0;
 }
 
+// open-addressing map from non-negative keys to small ints, for the per-tile edge and halo lookups (a few
+// hundred entries per tile); clear() forgets only the slots in use
+struct FlatMap {
+    static constexpr int CAP = 4096;  // > 2 x the largest tile list (1022 edges, 3 x 256 + halo faces)
+    std::vector<int64_t> keys = std::vector<int64_t>(CAP, -1);
+    std::vector<int32_t> vals = std::vector<int32_t>(CAP, 0);
+    std::vector<int32_t> used;
+    static uint32_t slot(int64_t k) { return (uint32_t)(((uint64_t)k * 0x9E3779B97F4A7C15ull) >> 52) & (CAP - 1); }
+    int find(int64_t k) const {
+        for (uint32_t i = slot(k);; i = (i + 1) & (CAP - 1)) {
+            if (keys[i] == k) return vals[i];
+            if (keys[i] < 0) return -1;
+        }
+    }
+    void insert(int64_t k, int32_t v) {
+        uint32_t i = slot(k);
+        while (keys[i] >= 0) i = (i + 1) & (CAP - 1);
+        keys[i] = k;
+        vals[i] = v;
+        used.push_back((int32_t)i);
+    }
+    int size() const { return (int)used.size(); }
+    void clear() {
+        for (int32_t i : used) keys[i] = -1;
+        used.clear();
+    }
+};
+
 int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tiling& out, std::string& err) {
     const int64_t ne = T.ne;
     if (tile != 64 && tile != 128 && tile != 256) {
@@ -485,6 +561,7 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
             ymax[gi] = std::max(ymax[gi], cy[r]);
         }
         std::vector<uint64_t> key(ne);
+#pragma omp parallel for schedule(static)
         for (int64_t r = 0; r < ne; ++r) {
             const int32_t gi = grouped ? T.group[r] : 0;
             double span = std::max(xmax[gi] - xmin[gi], ymax[gi] - ymin[gi]);
@@ -493,9 +570,10 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
             uint64_t iy = (uint64_t)std::min(2097151.0, std::floor((cy[r] - ymin[gi]) / span * 2097151.0));
             key[r] = spread21(ix) | spread21(iy) << 1;
         }
-        std::stable_sort(out.ref_of_dev.begin(), out.ref_of_dev.end(), [&](int32_t a, int32_t b) {
+        // (member, Morton key, element): the stable order of (member, key)
+        total_sort(out.ref_of_dev.begin(), out.ref_of_dev.end(), [&](int32_t a, int32_t b) {
             const int32_t ga = grouped ? T.group[a] : 0, gb = grouped ? T.group[b] : 0;
-            return ga != gb ? ga < gb : key[a] < key[b];
+            return ga != gb ? ga < gb : (key[a] != key[b] ? key[a] < key[b] : a < b);
         });
     }
     out.dev_of_ref.resize(ne);
@@ -509,104 +587,139 @@ int build_tiling(const Topology& T, const double* X, int tile, bool morton, Tili
     out.eslot.assign(2 * ne, 0);
     out.max_edges = 0;
     out.max_halo = 0;
-    std::vector<int64_t> iface(3 * ne, -1);
-    for (size_t i = 0; i < T.intf.size() / 4; ++i) {
-        iface[3 * (int64_t)T.intf[4 * i] + T.intf[4 * i + 2]] = (int64_t)i;
-        iface[3 * (int64_t)T.intf[4 * i + 1] + T.intf[4 * i + 3]] = (int64_t)i;
+    std::vector<int32_t> iface(3 * ne, -1);
+    const int64_t n_intf = (int64_t)T.intf.size() / 4;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n_intf; ++i) {
+        iface[3 * (int64_t)T.intf[4 * i] + T.intf[4 * i + 2]] = (int32_t)i;
+        iface[3 * (int64_t)T.intf[4 * i + 1] + T.intf[4 * i + 3]] = (int32_t)i;
     }
-    std::vector<int64_t> bface(3 * ne, -1);
-    for (size_t i = 0; i < T.bnd.size() / 3; ++i) bface[3 * (int64_t)T.bnd[3 * i] + T.bnd[3 * i + 1]] = (int64_t)i;
-    std::unordered_map<int64_t, int> local_edge, local_halo;
-    std::vector<int32_t> te;  // this tile's edge records
-    std::vector<double> tg;
-    for (int64_t t = 0; t < out.ntiles; ++t) {
-        local_edge.clear();
-        local_halo.clear();
-        te.clear();
-        tg.clear();
-        const int64_t d0 = t * tile, d1 = std::min(ne, d0 + tile);
-        const int64_t hbase = (int64_t)out.halo.size() / 2;
-        out.tile_edge_off[t] = (int32_t)((int64_t)out.edges.size() / 4);
-        out.tile_halo_off[t] = (int32_t)hbase;
-        // trace slot of (element in reference order, face)
-        auto trace_slot = [&](int32_t r, int f) -> int32_t {
-            const int64_t d = out.dev_of_ref[r];
-            if (d >= d0 && d < d1) return (int32_t)(3 * (d - d0) + f);
-            const int64_t key = 3 * (int64_t)r + f;
-            auto it = local_halo.find(key);
-            if (it != local_halo.end()) return 3 * tile + it->second;
-            const int h = (int)local_halo.size();
-            local_halo[key] = h;
-            out.halo.push_back((int32_t)d);
-            out.halo.push_back(f);
-            return 3 * tile + h;
-        };
-        for (int64_t d = d0; d < d1; ++d) {
-            const int32_t r = out.ref_of_dev[d];
-            uint32_t slots[3] = {1023, 1023, 1023};
-            for (int f = 0; f < 3; ++f) {
-                const int64_t ii = iface[3 * (int64_t)r + f];
-                const int64_t bi = bface[3 * (int64_t)r + f];
-                if (ii >= 0) {
-                    auto it = local_edge.find(ii);
-                    if (it != local_edge.end()) {
-                        slots[f] = (uint32_t)it->second;
-                        continue;
+    std::vector<int32_t> bface(3 * ne, -1);
+    for (size_t i = 0; i < T.bnd.size() / 3; ++i) bface[3 * (int64_t)T.bnd[3 * i] + T.bnd[3 * i + 1]] = (int32_t)i;
+    // tiles are independent: each builds its own edge, geometry and halo lists (in parallel), and the
+    // lists are concatenated in tile order
+    struct TileLists {
+        std::vector<int32_t> te;  // edge records
+        std::vector<double> tg;   // edge geometry
+        std::vector<int32_t> halo;
+    };
+    std::vector<TileLists> lists((size_t)out.ntiles);
+    int overflow = 0;
+#pragma omp parallel
+    {
+        FlatMap local_edge, local_halo;
+#pragma omp for schedule(dynamic, 16) reduction(| : overflow)
+        for (int64_t t = 0; t < out.ntiles; ++t) {
+            local_edge.clear();
+            local_halo.clear();
+            std::vector<int32_t>& te = lists[t].te;
+            te.reserve(4 * (size_t)(3 * tile / 2 + 32));
+            std::vector<double>& tg = lists[t].tg;
+            std::vector<int32_t>& halo = lists[t].halo;
+            const int64_t d0 = t * tile, d1 = std::min(ne, d0 + tile);
+            // trace slot of (element in reference order, face)
+            auto trace_slot = [&](int32_t r, int f) -> int32_t {
+                const int64_t d = out.dev_of_ref[r];
+                if (d >= d0 && d < d1) return (int32_t)(3 * (d - d0) + f);
+                const int64_t key = 3 * (int64_t)r + f;
+                const int found = local_halo.find(key);
+                if (found >= 0) return 3 * tile + found;
+                const int h = local_halo.size();
+                local_halo.insert(key, h);
+                halo.push_back((int32_t)d);
+                halo.push_back(f);
+                return 3 * tile + h;
+            };
+            for (int64_t d = d0; d < d1; ++d) {
+                const int32_t r = out.ref_of_dev[d];
+                uint32_t slots[3] = {1023, 1023, 1023};
+                for (int f = 0; f < 3; ++f) {
+                    const int64_t ii = iface[3 * (int64_t)r + f];
+                    const int64_t bi = bface[3 * (int64_t)r + f];
+                    if (ii >= 0) {
+                        const int found = local_edge.find(ii);
+                        if (found >= 0) {
+                            slots[f] = (uint32_t)found;
+                            continue;
+                        }
+                        const int idx = (int)(te.size() / 4);
+                        local_edge.insert(ii, idx);
+                        slots[f] = (uint32_t)idx;
+                        const int32_t in = T.intf[4 * ii], ex = T.intf[4 * ii + 1];
+                        const int fin = T.intf[4 * ii + 2], fex = T.intf[4 * ii + 3];
+                        te.push_back(trace_slot(in, fin));
+                        te.push_back(trace_slot(ex, fex));
+                        // levee interfaces carry their index among the levee interfaces above bit 8
+                        const bool lev = ii >= T.n_intf_internal;
+                        te.push_back(lev ? (fin | fex << 2 | EK_LEVEE << 4 | (int32_t)(ii - T.n_intf_internal) << 8)
+                                         : (fin | fex << 2 | EK_INTERIOR << 4));
+                        te.push_back(out.dev_of_ref[in]);
+                        double nx, ny, sJ;
+                        face_geometry(X, &T.enodes[3 * (int64_t)in], fin, nx, ny, sJ);
+                        tg.push_back(nx);
+                        tg.push_back(ny);
+                        tg.push_back(sJ);
+                    } else if (bi >= 0) {
+                        const int idx = (int)(te.size() / 4);
+                        slots[f] = (uint32_t)idx;
+                        const int bt = T.bnd[3 * bi + 2];
+                        const int kind = bt == DGSW_BC_LAND   ? EK_LAND
+                                         : bt == DGSW_BC_TIDE ? EK_TIDE
+                                         : bt == DGSW_BC_FLOW ? EK_FLOW
+                                                              : EK_FUNCTION;
+                        // tide / flow faces carry their forcing record as -2 - index in the b slot
+                        const int32_t fidx = (kind == EK_TIDE || kind == EK_FLOW) ? T.bnd_force[bi] : -1;
+                        te.push_back((int32_t)(3 * (d - d0) + f));
+                        te.push_back(fidx >= 0 ? -2 - fidx : -1);
+                        te.push_back(f | kind << 4);
+                        te.push_back((int32_t)d);
+                        double nx, ny, sJ;
+                        face_geometry(X, &T.enodes[3 * (int64_t)r], f, nx, ny, sJ);
+                        tg.push_back(nx);
+                        tg.push_back(ny);
+                        tg.push_back(sJ);
                     }
-                    const int idx = (int)(te.size() / 4);
-                    local_edge[ii] = idx;
-                    slots[f] = (uint32_t)idx;
-                    const int32_t in = T.intf[4 * ii], ex = T.intf[4 * ii + 1];
-                    const int fin = T.intf[4 * ii + 2], fex = T.intf[4 * ii + 3];
-                    te.push_back(trace_slot(in, fin));
-                    te.push_back(trace_slot(ex, fex));
-                    // levee interfaces carry their index among the levee interfaces above bit 8
-                    const bool lev = ii >= T.n_intf_internal;
-                    te.push_back(lev ? (fin | fex << 2 | EK_LEVEE << 4 | (int32_t)(ii - T.n_intf_internal) << 8)
-                                     : (fin | fex << 2 | EK_INTERIOR << 4));
-                    te.push_back(out.dev_of_ref[in]);
-                    double nx, ny, sJ;
-                    face_geometry(X, &T.enodes[3 * (int64_t)in], fin, nx, ny, sJ);
-                    tg.push_back(nx);
-                    tg.push_back(ny);
-                    tg.push_back(sJ);
-                } else if (bi >= 0) {
-                    const int idx = (int)(te.size() / 4);
-                    slots[f] = (uint32_t)idx;
-                    const int bt = T.bnd[3 * bi + 2];
-                    const int kind = bt == DGSW_BC_LAND   ? EK_LAND
-                                     : bt == DGSW_BC_TIDE ? EK_TIDE
-                                     : bt == DGSW_BC_FLOW ? EK_FLOW
-                                                          : EK_FUNCTION;
-                    // tide / flow faces carry their forcing record as -2 - index in the b slot
-                    const int32_t fidx = (kind == EK_TIDE || kind == EK_FLOW) ? T.bnd_force[bi] : -1;
-                    te.push_back((int32_t)(3 * (d - d0) + f));
-                    te.push_back(fidx >= 0 ? -2 - fidx : -1);
-                    te.push_back(f | kind << 4);
-                    te.push_back((int32_t)d);
-                    double nx, ny, sJ;
-                    face_geometry(X, &T.enodes[3 * (int64_t)r], f, nx, ny, sJ);
-                    tg.push_back(nx);
-                    tg.push_back(ny);
-                    tg.push_back(sJ);
                 }
+                int32_t roles = 0;
+                for (int f = 0; f < 3; ++f) roles |= (T.is_in[3 * r + f] ? 1 : 0) << f;
+                int32_t ord = T.order_count[r];
+                for (int k = 0; k < T.order_count[r]; ++k) ord |= T.order_face[3 * r + k] << (2 + 2 * k);
+                out.eslot[2 * d] = (int32_t)(slots[0] | slots[1] << 10 | slots[2] << 20);
+                out.eslot[2 * d + 1] = roles | ord << 3;
             }
-            int32_t roles = 0;
-            for (int f = 0; f < 3; ++f) roles |= (T.is_in[3 * r + f] ? 1 : 0) << f;
-            int32_t ord = T.order_count[r];
-            for (int k = 0; k < T.order_count[r]; ++k) ord |= T.order_face[3 * r + k] << (2 + 2 * k);
-            out.eslot[2 * d] = (int32_t)(slots[0] | slots[1] << 10 | slots[2] << 20);
-            out.eslot[2 * d + 1] = roles | ord << 3;
+            if (te.size() / 4 > 1022) overflow = 1;
         }
-        const int n = (int)(te.size() / 4);
-        if (n > 1022) {
-            err = "tile edge list overflow";
-            return DGSW_ERR_INVALID_ARGUMENT;
-        }
-        out.edges.insert(out.edges.end(), te.begin(), te.end());
-        out.egeo.insert(out.egeo.end(), tg.begin(), tg.end());
-        out.max_edges = std::max(out.max_edges, n);
-        out.max_halo = std::max(out.max_halo, (int)local_halo.size());
+    }
+    if (overflow) {
+        err = "tile edge list overflow";
+        return DGSW_ERR_INVALID_ARGUMENT;
+    }
+    // offsets by a prefix sum over the tiles, then every tile copies its lists into place
+    std::vector<int64_t> eo(out.ntiles + 1, 0), ho(out.ntiles + 1, 0);
+    for (int64_t t = 0; t < out.ntiles; ++t) {
+        eo[t + 1] = eo[t] + (int64_t)lists[t].te.size() / 4;
+        ho[t + 1] = ho[t] + (int64_t)lists[t].halo.size() / 2;
+        out.max_edges = std::max(out.max_edges, (int)(lists[t].te.size() / 4));
+        out.max_halo = std::max(out.max_halo, (int)(lists[t].halo.size() / 2));
+    }
+    if (eo[out.ntiles] >= std::numeric_limits<int32_t>::max() || ho[out.ntiles] >= std::numeric_limits<int32_t>::max()) {
+        err = "too many tile edges";
+        return DGSW_ERR_UNSUPPORTED;
+    }
+    out.edges.resize((size_t)4 * eo[out.ntiles]);
+    out.egeo.resize((size_t)3 * eo[out.ntiles]);
+    out.halo.resize((size_t)2 * ho[out.ntiles]);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t t = 0; t < out.ntiles; ++t) {
+        TileLists& L = lists[t];
+        out.tile_edge_off[t] = (int32_t)eo[t];
+        out.tile_halo_off[t] = (int32_t)ho[t];
+        std::copy(L.te.begin(), L.te.end(), out.edges.begin() + 4 * eo[t]);
+        std::copy(L.tg.begin(), L.tg.end(), out.egeo.begin() + 3 * eo[t]);
+        std::copy(L.halo.begin(), L.halo.end(), out.halo.begin() + 2 * ho[t]);
+        std::vector<int32_t>().swap(L.te);
+        std::vector<double>().swap(L.tg);
+        std::vector<int32_t>().swap(L.halo);
     }
     out.tile_edge_off[out.ntiles] = (int32_t)((int64_t)out.edges.size() / 4);
     out.tile_halo_off[out.ntiles] = (int32_t)((int64_t)out.halo.size() / 2);
@@ -794,6 +907,7 @@ static void l2_node(const Tables& tb, double aJ, const double nodal[3], double* 
 
 void project_bathymetry(const Topology& T, const double* X, const Tables& tb, std::vector<double>& bath) {
     bath.assign(T.ne * tb.nd, 0.0);
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < T.ne; ++r) {
         const int32_t* nd = &T.enodes[3 * r];
         double aJ;
@@ -807,6 +921,7 @@ void project_initial_condition(const Topology& T, const double* X, const Tables&
                                std::vector<double>& q) {
     const int nd = tb.nd;
     q.assign(T.ne * 3 * nd, 0.0);
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < T.ne; ++r) {
         const int32_t* no = &T.enodes[3 * r];
         double aJ;
@@ -859,6 +974,7 @@ void init_wet_dry(const Topology& T, const double* X, const Tables& tb, const dg
     if (!cfg.wetting_drying) return;
     const double thr = 1.0e6 * cfg.h_o * std::numeric_limits<double>::epsilon();
     const int nd = tb.nd;
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < T.ne; ++r) {
         const int32_t* no = &T.enodes[3 * r];
         double* qe = &q[r * 3 * nd];

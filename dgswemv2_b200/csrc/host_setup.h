@@ -5,12 +5,37 @@
 #define DGSW_HOST_SETUP_H
 
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <string>
 #include <vector>
 
 #include "../../include/dgsw_rkdg.h"
 
 namespace dgsw {
+
+// allocator whose value-less construct leaves elements uninitialised: large set-up arrays that are
+// written in full by parallel loops skip the serial zero fill of std::vector::resize
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <typename U>
+    UninitAlloc(const UninitAlloc<U>&) {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U* p, Args&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <typename T>
+using bigvec = std::vector<T, UninitAlloc<T>>;
 
 constexpr int MAX_ND = 6;  // p <= 2
 constexpr int MAX_NQ = 6;
@@ -27,7 +52,7 @@ struct Topology {
     std::vector<int32_t> nbr;       // [3*ne] neighbor element (reference order) or -1
     std::vector<int8_t> nbr_face;   // [3*ne] neighbor's local face or -1
     std::vector<uint8_t> btype;     // [3*ne] DGSW_BC_* (128 interior)
-    std::vector<int32_t> intf;      // [4*n_intf] in, ex, face_in, face_ex in creation order
+    bigvec<int32_t> intf;           // [4*n_intf] in, ex, face_in, face_ex in creation order
     int64_t n_intf_internal = 0;    // the internal interfaces come first, then the levee ones
     std::vector<int32_t> bnd;       // [3*n_bnd] elem, face, type in traversal order
     // per element: faces in accumulation order (interfaces by creation order, then boundaries)
@@ -81,10 +106,10 @@ struct Tiling {
     // [4 * n_edges]: trace slot of the in/owner side a, trace slot of b (-1 for boundaries),
     // meta = face_a | face_b << 2 | kind << 4, device index of a. Trace slots: 3*(element - tile start)
     // + face for tile elements, 3*tile + h for the tile's halo face h.
-    std::vector<int32_t> edges;
-    std::vector<double> egeo;            // [3 * n_edges]: normal x, normal y, half length (of face a)
+    bigvec<int32_t> edges;
+    bigvec<double> egeo;                 // [3 * n_edges]: normal x, normal y, half length (of face a)
     std::vector<int32_t> tile_halo_off;  // [ntiles+1]
-    std::vector<int32_t> halo;           // [2 * n_halo]: device element, face
+    bigvec<int32_t> halo;                // [2 * n_halo]: device element, face
     std::vector<int32_t> eslot;          // [2 * ne] per element (dev order): packed slots, roles + order
     int max_edges = 0;
     int max_halo = 0;

@@ -11,11 +11,13 @@ tidal_p1 / tidal_p2: 100 km x 25 km tidal channel, 524,288 triangles, M2 + K1 ti
   friction, forcing ramp (p = 1 SSP-RK2 dt = 0.5 s / p = 2 SSP-RK3 dt = 0.25 s)
 levee_p1: the same channel cut across by a levee (256 levee interfaces), p = 1, SSP-RK2, dt = 0.5 s
 Prints one JSON line per (configuration, precision): device ms per step after warm-up (CUDA events on
-the handle's stream around graph-replayed steps), element-DOF updates per second per RK stage, and the
-L2 error against the analytic solution at the end.
+the handle's stream around graph-replayed steps), element-DOF updates per second per RK stage, the
+L2 error against the analytic solution at the end, and the host wall time of the handle's creation
+(topology, tiling, projections, uploads, initial state).
 """
 import argparse
 import json
+import time
 
 from . import Problem, configs
 
@@ -43,7 +45,9 @@ def build(name, precision):
 
 def measure(name, precision, steps, warmup=5):
     mesh, cfg = build(name, precision)
+    t0 = time.perf_counter()
     P = Problem(cfg, mesh)
+    create_s = time.perf_counter() - t0
     P.step_serial(warmup)
     P.step_serial(steps)
     ms, launches = P.last_step_timing()
@@ -53,6 +57,7 @@ def measure(name, precision, steps, warmup=5):
         "tile": P.info.tile, "steps": steps, "ms_per_step": per_step,
         "element_dof_per_s_per_stage": P.ne * P.nd * cfg.rk_nstages / (per_step * 1e-3),
         "kernel_launches_per_step": launches / steps, "l2_error": P.compute_residual_L2(),
+        "create_seconds": create_s,
     }
 
 
