@@ -985,6 +985,8 @@ struct Concat {
     std::vector<int64_t> seg_off{0};
     std::vector<std::vector<int32_t>> fnodes;  // forcing block nodes, offset to the joint numbering
     std::vector<dgsw_forcing_block> forcing;
+    std::vector<int32_t> levee_nodes;          // levee pairs, offset to the joint numbering
+    std::vector<double> levee_data;
     dgsw_mesh m{};
 };
 
@@ -1062,6 +1064,21 @@ static int concat_members(int32_t n, const dgsw_mesh* members, Concat& C, std::s
             C.fnodes.push_back(std::move(nodes));
             C.forcing.push_back(B);
         }
+        if (M.n_levee_pairs > 0 && (!M.levee_nodes || !M.levee_data)) {
+            err = "ensemble member " + std::to_string(k) + ": null levee pair list";
+            return DGSW_ERR_INVALID_ARGUMENT;
+        }
+        for (int32_t i = 0; i < M.n_levee_pairs; ++i) {
+            for (int j = 0; j < 2; ++j) {
+                const int32_t n = M.levee_nodes[2 * i + j];
+                if (n < 0 || n >= M.n_nodes) {
+                    err = "ensemble member " + std::to_string(k) + ": levee node index out of range";
+                    return DGSW_ERR_MESH;
+                }
+                C.levee_nodes.push_back((int32_t)(n + node_base));
+            }
+            for (int j = 0; j < 3; ++j) C.levee_data.push_back(M.levee_data[3 * i + j]);
+        }
         node_base += M.n_nodes;
         id_base += M.n_elems;
     }
@@ -1081,6 +1098,9 @@ static int concat_members(int32_t n, const dgsw_mesh* members, Concat& C, std::s
     for (size_t b = 0; b < C.forcing.size(); ++b) C.forcing[b].nodes = C.fnodes[b].data();
     C.m.n_forcing = (int32_t)C.forcing.size();
     C.m.forcing = C.forcing.empty() ? nullptr : C.forcing.data();
+    C.m.n_levee_pairs = (int32_t)(C.levee_nodes.size() / 2);
+    C.m.levee_nodes = C.levee_nodes.empty() ? nullptr : C.levee_nodes.data();
+    C.m.levee_data = C.levee_data.empty() ? nullptr : C.levee_data.data();
     return DGSW_OK;
 }
 
