@@ -338,7 +338,7 @@ def run_ours(args):
     for _ in range(ke):
         P.set_state(hq)
         P.step_serial(1)
-        hq[:] = P.get_state()
+        P.get_state(out=hq)
     torch.cuda.synchronize()
     e2e_s = dist_max(time.perf_counter() - t0, world)
     barrier(world)

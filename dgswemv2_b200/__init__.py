@@ -192,10 +192,15 @@ class Problem:
         return out.value
 
     # state access ----------------------------------------------------------------------------
-    def get_state(self):
-        q = np.empty((self.ne, 3, self.nd), np.float64)
-        _lib.check(_lib.load().dgsw_rkdg_get_state(self._h, _lib.ptr(q, C.c_double)))
-        return q
+    def get_state(self, out=None):
+        """Modal state [ne][3][nd] in ascending element-ID order; `out`: a C-contiguous float64 array of that
+        shape (for example pinned host memory) to write into instead of a new array."""
+        if out is None:
+            out = np.empty((self.ne, 3, self.nd), np.float64)
+        elif out.dtype != np.float64 or out.shape != (self.ne, 3, self.nd) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (ne, 3, nd)")
+        _lib.check(_lib.load().dgsw_rkdg_get_state(self._h, _lib.ptr(out, C.c_double)))
+        return out
 
     def set_state(self, q):
         q = np.ascontiguousarray(q, np.float64)
