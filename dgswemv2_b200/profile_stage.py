@@ -1,8 +1,12 @@
-"""Small driver for profiling the RK stage kernel: config 2 (p = 2 manufactured solution on 512 x 512
-jittered quads, 524,288 triangles, SSP-RK3) in one precision, two steps without CUDA graphs (each stage
-is a separate launch, so `ncu -k regex:rkdg_stage_kernel -s 3 -c 1` selects the first stage of step 2).
+"""Small driver for profiling the RK stage kernel, two steps without CUDA graphs (each stage is a
+separate launch, so `ncu -k regex:rkdg_stage_kernel -s <n> -c <m>` selects stages of step 2):
 
-    python -m dgswemv2_b200.profile_stage fp32 [nq]
+    python -m dgswemv2_b200.profile_stage fp32 [nq] [workload]
+
+workload "manufactured" (default): config 2, p = 2 manufactured solution on nq x nq jittered quads
+(nq = 512: 524,288 triangles), SSP-RK3; "bowl": config 3, Thacker bowl on nq x nq quads (nq = 256:
+131,072 triangles), p = 1, SSP-RK2, wetting/drying and the slope limiter (stage kernel, then limiter
+kernel, per stage).
 """
 import sys
 
@@ -11,12 +15,17 @@ from . import Problem, configs
 
 def main():
     prec = sys.argv[1] if len(sys.argv) > 1 else "fp32"
-    nq = int(sys.argv[2]) if len(sys.argv) > 2 else 512
-    mesh, cfg = configs.config2(nq=nq, precision=prec)
+    workload = sys.argv[3] if len(sys.argv) > 3 else "manufactured"
+    if workload == "bowl":
+        nq = int(sys.argv[2]) if len(sys.argv) > 2 else 256
+        mesh, cfg = configs.config3(nq=nq, precision=prec)
+    else:
+        nq = int(sys.argv[2]) if len(sys.argv) > 2 else 512
+        mesh, cfg = configs.config2(nq=nq, precision=prec)
     P = Problem(cfg, mesh, use_graphs=False)
     P.step_serial(2)
     P.synchronize()
-    print("ok", prec, P.ne)
+    print("ok", prec, workload, P.ne)
 
 
 if __name__ == "__main__":
