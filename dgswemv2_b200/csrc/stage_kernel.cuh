@@ -474,16 +474,27 @@ __device__ __forceinline__ void cp_async_commit_and_wait() {
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
-// resident CTAs per SM the register budget is sized for
+// resident CTAs per SM the register budget is sized for (p = 1 and p = 2 separately; measured at tile
+// 128 on 524,288 triangles: p = 2 FP32 4 (5 spills 592 B and runs 40 % slower), p = 1 FP32 5 (3-9 %
+// faster than 4 on the bowl, tidal, levee and manufactured workloads; 6 spills and is slower), FP64 3
+// at both orders (4 is 14 % slower at p = 1))
 #ifndef DGSW_F32_MB128
 #define DGSW_F32_MB128 4
 #endif
 #ifndef DGSW_F64_MB128
 #define DGSW_F64_MB128 3
 #endif
+#ifndef DGSW_F32_P1_MB128
+#define DGSW_F32_P1_MB128 5
+#endif
+#ifndef DGSW_F64_P1_MB128
+#define DGSW_F64_P1_MB128 DGSW_F64_MB128
+#endif
 template <int P, typename Real, int TILE>
 struct MinBlocks {
-    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? DGSW_F32_MB128 : 2) : (TILE == 128 ? DGSW_F64_MB128 : 1);
+    static constexpr int f32 = P == 1 ? DGSW_F32_P1_MB128 : DGSW_F32_MB128;
+    static constexpr int f64 = P == 1 ? DGSW_F64_P1_MB128 : DGSW_F64_MB128;
+    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? f32 : 2) : (TILE == 128 ? f64 : 1);
 };
 
 // shared-memory capacities a tile almost always fits (measured: about 0.27 TILE halo faces and 1.65 TILE
