@@ -235,8 +235,13 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
 }
 
 // One thread per visited element (every element, or the indicator's work list with a grid-stride loop).
+// three resident 256-thread blocks per SM (80 registers, a few hundred bytes of spills): measured 13 %
+// faster than two blocks at 128 registers, and faster than four, on 524,288 bowl triangles
+#ifndef DGSW_LIM_MB
+#define DGSW_LIM_MB 3
+#endif
 template <int ND, typename Real>
-__global__ void __launch_bounds__(256) cs_limiter_kernel(const LimiterArgs<Real> L) {
+__global__ void __launch_bounds__(256, DGSW_LIM_MB) cs_limiter_kernel(const LimiterArgs<Real> L) {
     const int n = L.list ? *L.list_count : L.ne;
     const int stride = gridDim.x * blockDim.x;
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {  // block-uniform trip count
