@@ -235,13 +235,10 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
 }
 
 // One thread per visited element (every element, or the indicator's work list with a grid-stride loop).
-// three resident 256-thread blocks per SM (80 registers, a few hundred bytes of spills): measured 13 %
-// faster than two blocks at 128 registers, and faster than four, on 524,288 bowl triangles
-#ifndef DGSW_LIM_MB
-#define DGSW_LIM_MB 3
-#endif
-template <int ND, typename Real>
-__global__ void __launch_bounds__(256, DGSW_LIM_MB) cs_limiter_kernel(const LimiterArgs<Real> L) {
+// MB resident 256-thread blocks per SM: 2 (128 registers) or 3 (80 registers and a few hundred bytes of
+// spills); measured on the bowl, 3 is 13 % faster at 524,288 triangles and 2 is faster at 131,072
+template <int ND, typename Real, int MB>
+__global__ void __launch_bounds__(256, MB) cs_limiter_kernel(const LimiterArgs<Real> L) {
     const int n = L.list ? *L.list_count : L.ne;
     const int stride = gridDim.x * blockDim.x;
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {  // block-uniform trip count
@@ -270,10 +267,18 @@ template <typename Real>
 cudaError_t launch_limiter_kernel(const LimiterArgs<Real>& L, int p, cudaStream_t s, int list_blocks = 0) {
     const int blocks = L.list ? list_blocks : (L.ne + 255) / 256;
     if (blocks <= 0) return cudaSuccess;
-    if (p == 1)
-        cs_limiter_kernel<3, Real><<<blocks, 256, 0, s>>>(L);
-    else
-        cs_limiter_kernel<6, Real><<<blocks, 256, 0, s>>>(L);
+    const bool big = L.ne >= (1 << 18);
+    if (p == 1) {
+        if (big)
+            cs_limiter_kernel<3, Real, 3><<<blocks, 256, 0, s>>>(L);
+        else
+            cs_limiter_kernel<3, Real, 2><<<blocks, 256, 0, s>>>(L);
+    } else {
+        if (big)
+            cs_limiter_kernel<6, Real, 3><<<blocks, 256, 0, s>>>(L);
+        else
+            cs_limiter_kernel<6, Real, 2><<<blocks, 256, 0, s>>>(L);
+    }
     return cudaGetLastError();
 }
 
