@@ -10,6 +10,8 @@
 5. ensemble of p=1 members with random smooth bathymetry and wet/dry
 6. tidal channel: two-constituent tide on the open (x = 0) end, a steady + periodic river flow on the
    other, land sides, sloping bathymetry, Chezy or Manning bottom friction, forcing ramp
+7. levee channel: the tidal channel cut across by an internal barrier that the tide overtops (optionally
+   onto dry land, with wetting/drying and the slope limiter)
 """
 import math
 
@@ -162,12 +164,12 @@ def tidal_channel(nx=24, ny=6, p=1, rk=(2, 2), dt=2.0, friction="chezy", cf=0.00
 
 def levee_channel(nx=24, ny=6, p=1, rk=(2, 2), dt=1.0, crest=0.1, c_sub=0.8, c_super=0.6, dry_right=False,
                   friction="chezy", cf=0.0025, ramp_days=0.005, precision="fp64", jitter=0.1, seed=4,
-                  length=10000.0, width=2000.0, depth=10.0):
+                  length=10000.0, width=2000.0, depth=10.0, limiter=False):
     """The tidal channel cut across its middle by a levee (an internal barrier of coincident but distinct
     nodes) with crest elevation `crest` and discharge coefficients c_sub / c_super: the tide (M2 + K1) on
     x = 0 overtops it into the right half. dry_right: the right half is land 0.05 m above datum (with
     wetting/drying, h_o = 0.01 m) that the overtopping floods; else it is 0.6 `depth` deep with a
-    river flow on x = length."""
+    river flow on x = length. limiter: the Cockburn-Shu limiter (M = 1e-8, nu = 1.5)."""
     def bath(x, y):
         b = depth - 0.4 * depth * x / length
         return np.where(x > length / 2 + 1e-9, -0.05, b) if dry_right else b
@@ -193,5 +195,5 @@ def levee_channel(nx=24, ny=6, p=1, rk=(2, 2), dt=1.0, crest=0.1, c_sub=0.8, c_s
         mesh.node_manning_n = 0.02 + 0.01 * x / length
     cfg = ProblemConfig(p=p, rk_nstages=rk[0], rk_order=rk[1], dt=dt, g=9.81, ic_type=0, ic_const=(0.0, 0.0, 0.0),
                         bottom_friction=kind, friction_cf=cf, ramp_duration=ramp_days, precision=precision,
-                        wetting_drying=dry_right, h_o=0.01)
+                        wetting_drying=dry_right, h_o=0.01, slope_limiting=limiter, sl_M=1.0e-8, sl_nu=1.5)
     return mesh, cfg
