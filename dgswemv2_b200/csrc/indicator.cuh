@@ -76,7 +76,8 @@ __device__ __forceinline__ bool element_features(const FeatureArgs<Real>& F, int
             for (int v = 0; v < 3; ++v) d[f][v] = __dsub_rn((double)F.q[(size_t)(v * ND) * P + m], a[v]);
         } else {
             const int bt = -2 - m;
-            ok = ok && (bt == 0 || bt == 3);
+            // land, tide, flow and function boundaries: wet_neigh is the element's own flag
+            ok = ok && (bt >= 0 && bt <= 3);
 #pragma unroll
             for (int v = 0; v < 3; ++v) d[f][v] = 0.0;
         }

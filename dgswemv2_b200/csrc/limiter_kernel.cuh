@@ -116,9 +116,10 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
             ok = ok && (L.wet[nb[f]] != 0);
         } else {
             const int bt = -2 - nb[f];
-            // land / function boundaries set wet_neigh to the element's own flag; faces without a
-            // boundary object (outflow) never set it and keep its initial false
-            ok = ok && (bt == 0 || bt == 3);
+            // land, tide, flow and function boundaries set wet_neigh to the element's own flag; faces
+            // without a boundary object (outflow, an unpaired levee face) never set it and keep its
+            // initial false
+            ok = ok && (bt >= 0 && bt <= 3);  // DGSW_BC_LAND .. DGSW_BC_FUNCTION
         }
     }
     if (!ok) return 0;

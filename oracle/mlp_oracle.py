@@ -81,7 +81,7 @@ def features(q, wet, nbr, btype, node_xyz, elem_nodes, g, M):
         for f in range(3):
             F[:, 5 + 5 * v + f] = d[:, f, v] * inv
     w = np.asarray(wet) != 0
-    nbr_wet = np.where(has, w[np.where(has, nbr, 0)], (btype == 0) | (btype == 3))
+    nbr_wet = np.where(has, w[np.where(has, nbr, 0)], btype <= 3)  # land, tide, flow, function objects
     ok = w & nbr_wet.all(axis=1)
     return F.astype(np.float32), ok
 
