@@ -106,6 +106,28 @@ def test_features_match_oracle_bit_exact(precision):
     assert np.array_equal(feat.cpu().numpy(), F)
 
 
+@pytest.mark.gpu
+def test_features_with_tide_flow_and_levee_faces():
+    """Features on a mesh with tide and land boundaries and levee interfaces (the element across a levee
+    is a neighbour; tide faces are boundary objects like land faces), bit-exact against the oracle."""
+    import torch
+
+    from dgswemv2_b200 import configs
+
+    mesh, cfg = configs.levee_channel(p=1, dt=2.0, dry_right=True, limiter=True, precision="fp32")
+    P = Problem(cfg, mesh)
+    P.step_serial(500)
+    feat = torch.empty((P.ne, 18), dtype=torch.float32, device="cuda")
+    ok = torch.empty(P.ne, dtype=torch.uint8, device="cuda")
+    P.indicator_features(feat.data_ptr(), ok.data_ptr())
+    nbr, bt, _, _ = mesh_topology(mesh)
+    F, okr = mo.features(P.get_state(), P.get_wet(), nbr, bt, mesh.node_xyz, mesh.elem_nodes, cfg.g, cfg.sl_M)
+    tide_elems = np.any(bt == 1, axis=1)
+    assert okr[tide_elems].any()  # cells on the tide boundary are eligible
+    assert np.array_equal(ok.cpu().numpy() != 0, okr)
+    assert np.array_equal(feat.cpu().numpy(), F)
+
+
 def _random_batch(n, seed):
     rng = np.random.default_rng(seed)
     X = rng.uniform(-1, 1, (n, 18)).astype(np.float32)
