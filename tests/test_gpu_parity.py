@@ -337,3 +337,24 @@ def test_manning_friction_in_drying_cells(oracle):
     assert int(wo.sum()) > mesh.n_elems // 2 + 10
     assert abs(int(wg.sum()) - int(wo.sum())) <= max(2, 0.005 * mesh.n_elems)
     assert rel_err(P.get_state(), O.get_state()) <= 1e-9
+
+
+def test_forcing_block_with_a_repeated_node_is_rejected():
+    """A node listed twice in one block would shift its constituents in the reference's per-node lists;
+    the library rejects it with DGSW_ERR_MESH instead."""
+    from dgswemv2_b200._lib import DgswError
+
+    mesh, cfg = configs.tidal_channel(nx=6, ny=3, flow=False)
+    b = mesh.forcing[0]
+    b.nodes = np.concatenate([b.nodes, b.nodes[:1]])
+    b.amplitude = np.concatenate([b.amplitude, b.amplitude[:, :1]], 1)
+    b.phase = np.concatenate([b.phase, b.phase[:, :1]], 1)
+    with pytest.raises(DgswError, match="twice") as ei:
+        Problem(cfg, mesh)
+    assert ei.value.status == 2
+    mesh2, cfg2 = configs.levee_channel(nx=6, ny=3)
+    mesh2.levee_pairs = mesh2.levee_pairs[1:]
+    mesh2.levee_data = mesh2.levee_data[1:]
+    with pytest.raises(DgswError, match="unable to find levee data") as ei:
+        Problem(cfg2, mesh2)
+    assert ei.value.status == 2
