@@ -358,3 +358,25 @@ def test_forcing_block_with_a_repeated_node_is_rejected():
     with pytest.raises(DgswError, match="unable to find levee data") as ei:
         Problem(cfg2, mesh2)
     assert ei.value.status == 2
+
+
+def test_p2_limiter_matches_where_decisions_are_clear(oracle):
+    """p = 2 with the Cockburn-Shu limiter on a steep hump (many elements limited from the first stage,
+    far from the 1e-12 write-back threshold): state within 1e-12 and identical limiter decisions over
+    the first step. Over long runs with small states the 1e-12 relative-change test can flip on
+    last-bit differences, and a flip zeroes that element's p = 2 modes, so long p = 2 limiter runs agree
+    only statistically (the reference itself would differ between compilers the same way)."""
+    mesh = meshgen.quad_mesh(16, 16, corners=((0, 0), (1000, 0), (1000, 1000), (0, 1000)), bc=(LAND,) * 4,
+                             jitter=0.15, seed=6, bathymetry=meshgen.bath_flat(5.0))
+    cfg = configs.ProblemConfig(p=2, rk_nstages=3, rk_order=3, dt=0.5, ic_type=1,
+                                function_set=configs.FN_GAUSSIAN_HUMPS, slope_limiting=True, sl_M=1e-8, sl_nu=1.5,
+                                fn_params=configs.humps_params([(1.0, 500.0, 500.0, 60.0)]))
+    P = Problem(cfg, mesh, use_graphs=False)
+    O = oracle.problem(cfg, mesh, n_threads=8)
+    for _ in range(3):
+        P.stage_serial()
+        O.stage()
+        lg, lo = P.get_limited(), O.limited_flags()
+        assert np.array_equal(lg, lo)
+        assert rel_err(P.get_state(), O.get_state()) <= 1e-12
+    assert lo.sum() > 10
