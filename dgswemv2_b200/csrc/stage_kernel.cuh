@@ -181,11 +181,20 @@ __device__ __noinline__ void wd_fixup(Real g, const Real* qi, const Real* qe, Re
     }
 }
 
-// analytic function sets evaluated out of line (one copy per kernel)
+// three values returned by value from the out-of-line helpers below: an output array passed by
+// address would live in local memory at every call site
 template <typename Real>
-__device__ __noinline__ void fn_eval_dev(int id, const double* P, const dgsw_fn_time* T, int source, Real x, Real y,
-                                         Real* out) {
+struct Val3 {
+    Real v0, v1, v2;
+};
+
+// analytic function sets evaluated out of line (one copy per kernel); T points to the CTA's shared copy
+template <typename Real>
+__device__ __noinline__ Val3<Real> fn_eval_dev(int id, const double* P, const dgsw_fn_time* T, int source, Real x,
+                                               Real y) {
+    Real out[3];
     dgsw_fn_eval<Real>(id, P, *T, source, x, y, out);
+    return Val3<Real>{out[0], out[1], out[2]};
 }
 
 // Ghost states of the boundaries with data, out of line (one call site per Gauss point):
@@ -198,13 +207,14 @@ __device__ __noinline__ void fn_eval_dev(int id, const double* P, const dgsw_fn_
 // ghost surface elevation to it and keeps the interior momentum; a flow keeps the interior elevation
 // and sets the ghost momentum to it times the outward normal. fi is the face's forcing record.
 template <typename Real>
-__device__ __noinline__ void boundary_ghost(const StageArgs<Real>* Ap, const dgsw_fn_time* T, int kind, int fi,
-                                            int gp, double t, Real x, Real y, Real qi0, Real qi1, Real qi2, Real nx,
-                                            Real ny, Real* qe) {
+__device__ __noinline__ Val3<Real> boundary_ghost(const StageArgs<Real>* Ap, const dgsw_fn_time* T, int kind,
+                                                  int fi, int gp, double t, Real x, Real y, Real qi0, Real qi1,
+                                                  Real qi2, Real nx, Real ny) {
     const StageArgs<Real>& A = *Ap;
     if (kind == 2) {
+        Real qe[3];
         dgsw_fn_eval<Real>(A.fn_set, A.fn_params, *T, 0, x, y, qe);
-        return;
+        return Val3<Real>{qe[0], qe[1], qe[2]};
     }
     constexpr double REF_PI = 3.14159265359;
     const double ramp = A.ramp_on ? tanh(2.0 * (t / 86400.0) / A.ramp_duration) : 1.0;
@@ -214,15 +224,8 @@ __device__ __noinline__ void boundary_ghost(const StageArgs<Real>* Ap, const dgs
         const double* r = A.fcon + (size_t)(fc.x + c) * FORCE_STRIDE_DEV;
         acc += ramp * r[1] * r[3 + gp] * cos(r[0] * t + (r[2] - r[6 + gp]) * REF_PI / 180.0);
     }
-    if (kind == 4) {
-        qe[0] = qi0;
-        qe[1] = (Real)acc * nx;
-        qe[2] = (Real)acc * ny;
-    } else {
-        qe[0] = (Real)acc;
-        qe[1] = qi1;
-        qe[2] = qi2;
-    }
+    if (kind == 4) return Val3<Real>{qi0, (Real)acc * nx, (Real)acc * ny};
+    return Val3<Real>{(Real)acc, qi1, qi2};
 }
 
 // the Manning friction factor g n^2 / h^(1/3), bounded below by the Chezy coefficient (swe_source.hpp:37-42)
@@ -533,7 +536,11 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     const double t_stage = A.clock->t + A.drk_s;  // ESSPRKStepper::GetTimeAtCurrentStage
     const Real g = (Real)A.g;
     const double* __restrict__ qs = A.qk[A.nterms - 1];  // this stage's state
-    const dgsw_fn_time FT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
+    // the stage's time factors, once per CTA in shared memory (the out-of-line helpers read them there)
+    __shared__ dgsw_fn_time sFT;
+    if (threadIdx.x == 0) sFT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
+    __syncthreads();
+    const dgsw_fn_time& FT = sFT;
     // FP32 only: in FP64 the inlined double sine/cosine raise register pressure more than the call costs
     const bool sine_set = FSRC && sizeof(Real) == 4 && A.fn_set == DGSW_FN_MANUFACTURED_SINE;
     SineSrc<Real> SS;
@@ -670,10 +677,12 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                     const Real xg = xr0 * (Real)s0 + xr1 * (Real)s1 + xr2 * (Real)s2;
                     const Real yg = yr0 * (Real)s0 + yr1 * (Real)s1 + yr2 * (Real)s2;
                     Real fs[3];
-                    if (sine_set)
+                    if (sine_set) {
                         sine_src_eval<Real>(SS, xg, yg, fs);
-                    else
-                        fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, xg, yg, fs);
+                    } else {
+                        const Val3<Real> r = fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, xg, yg);
+                        fs[0] = r.v0, fs[1] = r.v1, fs[2] = r.v2;
+                    }
                     sfor<0, 3>([&](auto V) {
                         constexpr int v = decltype(V)::value;
                         sfor<0, ND>([&](auto K) {
@@ -828,8 +837,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                 } else {
                     // function, tide and flow boundaries (a tide / flow face's b slot holds -2 - its
                     // forcing record)
-                    boundary_ghost<Real>(&A, &FT, kind, -2 - sb, gp, t_stage, (Real)(xa * wa_ + xb * wb_),
-                                         (Real)(ya * wa_ + yb * wb_), qi[0], qi[1], qi[2], nx, ny, qe);
+                    const Val3<Real> r =
+                        boundary_ghost<Real>(&A, &FT, kind, -2 - sb, gp, t_stage, (Real)(xa * wa_ + xb * wb_),
+                                             (Real)(ya * wa_ + yb * wb_), qi[0], qi[1], qi[2], nx, ny);
+                    qe[0] = r.v0, qe[1] = r.v1, qe[2] = r.v2;
                 }
                 Real Fi[3];
                 llf_flux<Real>(g, qi, qe, bi, sp, nx, ny, Fi);
