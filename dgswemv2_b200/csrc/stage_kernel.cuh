@@ -157,11 +157,22 @@ __device__ __forceinline__ void land_flux(Real g, Real nx, Real ny, const Real q
     llf_flux<Real>(g, qin, qex, bath, sp, nx, ny, F);
 }
 
-// Wet/dry fix-ups of ISP::Internal (rkdg_swe_is_internal.hpp:47-90) for an interface whose LLF
-// ze-flux exceeds 1e-12 in magnitude with one side dry. Out of line: taken on few edges only.
+// both sides' fluxes of an interface Gauss point, returned by value from wd_fixup
 template <typename Real>
-__device__ __noinline__ void wd_fixup(Real g, const Real* qi, const Real* qe, Real bi, Real be, Real sp, Real nx, Real ny,
-                                      bool wa, bool wb, Real* Fi, Real* Fe) {
+struct Flux2 {
+    Real i0, i1, i2, e0, e1, e2;
+};
+
+// Wet/dry fix-ups of ISP::Internal (rkdg_swe_is_internal.hpp:47-90) for an interface whose LLF
+// ze-flux exceeds 1e-12 in magnitude with one side dry; the ex-side flux starts as -F. Out of line
+// (taken on few edges only), with its arguments and results passed by value so that the call site
+// keeps them in registers.
+template <typename Real>
+__device__ __noinline__ Flux2<Real> wd_fixup(Real g, Real qi0, Real qi1, Real qi2, Real qe0, Real qe1, Real qe2,
+                                             Real bi, Real be, Real sp, Real nx, Real ny, bool wa, bool wb, Real F0,
+                                             Real F1, Real F2) {
+    const Real qi[3] = {qi0, qi1, qi2}, qe[3] = {qe0, qe1, qe2};
+    Real Fi[3] = {F0, F1, F2}, Fe[3] = {-F0, -F1, -F2};
     if (Fi[0] > Real(1e-12)) {
         if (!wa) {  // water flowing from the dry in-side: zero flux there, reflective wall on the ex side
             Fi[0] = Fi[1] = Fi[2] = Real(0);
@@ -179,6 +190,7 @@ __device__ __noinline__ void wd_fixup(Real g, const Real* qi, const Real* qe, Re
             Fi[0] = -Fe[0];
         }
     }
+    return Flux2<Real>{Fi[0], Fi[1], Fi[2], Fe[0], Fe[1], Fe[2]};
 }
 
 // three values returned by value from the out-of-line helpers below: an output array passed by
@@ -236,9 +248,8 @@ __device__ __noinline__ Real manning_cf(Real gn2, Real h, Real cf0) {
     return cf;
 }
 
-// The manufactured sine set's source terms inline (FP32 path), with its constants hoisted out of the
-// quadrature loops (the same formulas as dgsw_fn_eval, function_sets.h); every other set, and the FP64
-// path, goes through fn_eval_dev.
+// The manufactured sine set's source terms inline, with its constants hoisted out of the quadrature
+// loops (the same formulas as dgsw_fn_eval, function_sets.h); every other set goes through fn_eval_dev.
 template <typename Real>
 struct SineSrc {
     // ze = c1 P, qx = -c2 Q, qy = c2 R, zex = c3 Q, zey = -c3 R, zet = -c4 P, qxx = qyy = c5 P,
@@ -335,18 +346,23 @@ __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double b
                 qy[v] = 0.0;
             }
         } else {
-            // first minimum / first maximum, like std::min_element / std::max_element
+            // first minimum / first maximum, like std::min_element / std::max_element (the values
+            // are tracked beside the indices: an array indexed at run time would live in local memory;
+            // here some vertices are dry and some are not, so hmin != hmax)
             int hmin = 0, hmax = 0;
+            double hminv = h[0], hmaxv = h[0];
+#pragma unroll
             for (int v = 1; v < 3; ++v) {
-                if (h[v] < h[hmin]) hmin = v;
-                if (h[v] > h[hmax]) hmax = v;
+                if (h[v] < hminv) hmin = v, hminv = h[v];
+                if (h[v] > hmaxv) hmax = v, hmaxv = h[v];
             }
             const int hmid = 3 - hmax - hmin;
-            double ht[3];
-            ht[hmin] = h_o;
-            ht[hmid] = fmax(h_o, h[hmid] - (ht[hmin] - h[hmin]) / 2);
-            ht[hmax] = h[hmax] - (ht[hmin] - h[hmin]) - (ht[hmid] - h[hmid]);
-            for (int v = 0; v < 3; ++v) h[v] = ht[v];
+            const double hmidv = hmid == 0 ? h[0] : (hmid == 1 ? h[1] : h[2]);
+            const double tmin = h_o;
+            const double tmid = fmax(h_o, hmidv - (tmin - hminv) / 2);
+            const double tmax = hmaxv - (tmin - hminv) - (tmid - hmidv);
+#pragma unroll
+            for (int v = 0; v < 3; ++v) h[v] = v == hmin ? tmin : (v == hmax ? tmax : tmid);
             double dqx = 0, dqy = 0;
             int ndv = 0;
             for (int v = 0; v < 3; ++v)
@@ -369,10 +385,12 @@ __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double b
         check = true;
     }
     if (check) {
-        int hmax = 0;
+        // z at the first maximum of h
+        double hmaxv = h[0], zmax = z[0];
+#pragma unroll
         for (int v = 1; v < 3; ++v)
-            if (h[v] > h[hmax]) hmax = v;
-        if (z[hmax] > h_o - bath_min) {
+            if (h[v] > hmaxv) hmaxv = h[v], zmax = z[v];
+        if (zmax > h_o - bath_min) {
             wet = true;
         } else {
             wet = false;
@@ -385,15 +403,16 @@ __device__ __forceinline__ bool wetting_drying(Real (&qv)[3][ND], const double b
     }
     if (reproject) {
         // ProjectLinearToBasis through T_linear_basis (:236-257)
-        const double* src[3] = {z, qx, qy};
-        for (int var = 0; var < 3; ++var) {
-            const double* s = src[var];
+        auto project = [&](const double (&s)[3], int var) {
             qv[var][0] = (Real)(s[0] * (1.0 / 3.0) + s[1] * (1.0 / 3.0) + s[2] * (1.0 / 3.0));
             qv[var][1] = (Real)(s[0] * (-1.0 / 6.0) + s[1] * (-1.0 / 6.0) + s[2] * (1.0 / 3.0));
             qv[var][2] = (Real)(s[0] * (-1.0 / 2.0) + s[1] * (1.0 / 2.0));
 #pragma unroll
             for (int k = 3; k < ND; ++k) qv[var][k] = Real(0);
-        }
+        };
+        project(z, 0);
+        project(qx, 1);
+        project(qy, 2);
     }
     return wet;
 }
@@ -541,8 +560,8 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
     if (threadIdx.x == 0) sFT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
     __syncthreads();
     const dgsw_fn_time& FT = sFT;
-    // FP32 only: in FP64 the inlined double sine/cosine raise register pressure more than the call costs
-    const bool sine_set = FSRC && sizeof(Real) == 4 && A.fn_set == DGSW_FN_MANUFACTURED_SINE;
+    // the manufactured sine set's source inline, in both precisions; other sets go through fn_eval_dev
+    const bool sine_set = FSRC && A.fn_set == DGSW_FN_MANUFACTURED_SINE;
     SineSrc<Real> SS;
     if (sine_set) SS = sine_src_prepare<Real>(A.fn_params, FT);
 
@@ -846,7 +865,12 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
                 llf_flux<Real>(g, qi, qe, bi, sp, nx, ny, Fi);
                 if (WD && kind == 0) {
                     Real Fe[3] = {-Fi[0], -Fi[1], -Fi[2]};
-                    if (!(wa && wb)) wd_fixup<Real>(g, qi, qe, bi, be, sp, nx, ny, wa, wb, Fi, Fe);
+                    if (!(wa && wb)) {
+                        const Flux2<Real> r = wd_fixup<Real>(g, qi[0], qi[1], qi[2], qe[0], qe[1], qe[2], bi, be, sp,
+                                                             nx, ny, wa, wb, Fi[0], Fi[1], Fi[2]);
+                        Fi[0] = r.i0, Fi[1] = r.i1, Fi[2] = r.i2;
+                        Fe[0] = r.e0, Fe[1] = r.e1, Fe[2] = r.e2;
+                    }
 #pragma unroll
                     for (int v = 0; v < 3; ++v) sF[((3 + v) * NG + gp) * max_edges + le] = Fe[v];
                 }
