@@ -255,6 +255,7 @@ struct SineSrc {
     // ze = c1 P, qx = -c2 Q, qy = c2 R, zex = c3 Q, zey = -c3 R, zet = -c4 P, qxx = qyy = c5 P,
     // qxy = qyx = c5 S, qxt = -c6 Q, qyt = c6 R with P = sx cy, Q = cx cy, R = sx sy, S = cx sy
     Real k, c1, c2, c3, c5, c6, c0, g, H;  // c0 = 2 c5 - c4 (the continuity source)
+    Real kpi;                              // k / pi = 2 / L
 };
 
 template <typename Real>
@@ -263,6 +264,7 @@ __device__ __forceinline__ SineSrc<Real> sine_src_prepare(const double* P, const
     const double st = T.s[0], ct = T.s[1];
     SineSrc<Real> S;
     S.k = (Real)k;
+    S.kpi = (Real)(2.0 / P[0]);
     S.c1 = (Real)(A * ct);
     S.c2 = (Real)(B * st);
     S.c3 = (Real)(A * k * ct);
@@ -277,8 +279,16 @@ __device__ __forceinline__ SineSrc<Real> sine_src_prepare(const double* P, const
 template <typename Real>
 __device__ __forceinline__ void sine_src_eval(const SineSrc<Real>& S, Real x, Real y, Real (&out)[3]) {
     Real sx, cx, sy, cy;
-    dgsw_sincos(S.k * x, &sx, &cx);
-    dgsw_sincos(S.k * y, &sy, &cy);
+    if constexpr (sizeof(Real) == 8) {
+        // FP64: sin and cos of k x = pi (2 x / L) through sincospi, whose argument reduction is an exact
+        // rounding to an integer (sincos reduces by pi in several parts); the two differ by the
+        // rounding of 2 pi / L, a few 1e-16 relative
+        sincospi(S.kpi * x, &sx, &cx);
+        sincospi(S.kpi * y, &sy, &cy);
+    } else {
+        dgsw_sincos(S.k * x, &sx, &cx);
+        dgsw_sincos(S.k * y, &sy, &cy);
+    }
     const Real Pp = sx * cy, Q = cx * cy, R = sx * sy, Sq = cx * sy;
     const Real qx = -S.c2 * Q, qy = S.c2 * R;
     const Real zex = S.c3 * Q, zey = -S.c3 * R;
