@@ -508,8 +508,9 @@ __device__ __forceinline__ void cp_async_commit_and_wait() {
 
 // resident CTAs per SM the register budget is sized for (p = 1 and p = 2 separately; measured at tile
 // 128 on 524,288 triangles: p = 2 FP32 4 (5 spills 592 B and runs 40 % slower), p = 1 FP32 5 (3-9 %
-// faster than 4 on the bowl, tidal, levee and manufactured workloads; 6 spills and is slower), FP64 3
-// at both orders (4 is 14 % slower at p = 1))
+// faster than 4 on the bowl, tidal, levee and manufactured workloads; 6 spills and is slower), p = 2
+// FP64 3, p = 1 FP64 4 without wetting/drying (14-15 % faster than 3 on the tidal, levee and
+// manufactured workloads) and 3 with it (4 spills in the wet/dry pass and is 6 % slower on the bowl))
 #ifndef DGSW_F32_MB128
 #define DGSW_F32_MB128 4
 #endif
@@ -520,12 +521,15 @@ __device__ __forceinline__ void cp_async_commit_and_wait() {
 #define DGSW_F32_P1_MB128 5
 #endif
 #ifndef DGSW_F64_P1_MB128
-#define DGSW_F64_P1_MB128 DGSW_F64_MB128
+#define DGSW_F64_P1_MB128 4
 #endif
-template <int P, typename Real, int TILE>
+#ifndef DGSW_F64_P1_WD_MB128
+#define DGSW_F64_P1_WD_MB128 3
+#endif
+template <int P, typename Real, int TILE, bool WD>
 struct MinBlocks {
     static constexpr int f32 = P == 1 ? DGSW_F32_P1_MB128 : DGSW_F32_MB128;
-    static constexpr int f64 = P == 1 ? DGSW_F64_P1_MB128 : DGSW_F64_MB128;
+    static constexpr int f64 = P == 1 ? (WD ? DGSW_F64_P1_WD_MB128 : DGSW_F64_P1_MB128) : DGSW_F64_MB128;
     static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? f32 : 2) : (TILE == 128 ? f64 : 1);
 };
 
@@ -539,7 +543,7 @@ struct TileCap {
 };
 
 template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, bool CAPPED>
-__global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE>::value))
+__global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD>::value))
     rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_halo_rt, int max_edges_rt) {
     const int max_halo = CAPPED ? TileCap<TILE>::halo : max_halo_rt;
     const int max_edges = CAPPED ? TileCap<TILE>::edges : max_edges_rt;
