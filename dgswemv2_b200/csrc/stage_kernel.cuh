@@ -240,10 +240,12 @@ __device__ __noinline__ Val3<Real> boundary_ghost(const StageArgs<Real>* Ap, con
     return Val3<Real>{(Real)acc, qi1, qi2};
 }
 
-// the Manning friction factor g n^2 / h^(1/3), bounded below by the Chezy coefficient (swe_source.hpp:37-42)
+// the Manning friction factor g n^2 / h^(1/3), bounded below by the Chezy coefficient (swe_source.hpp:37-42);
+// h^(-1/3) through the reciprocal cube root (the reference's pow(h, 1/3) differs from cbrt by the
+// rounding of 1/3, a few ulps)
 template <typename Real>
-__device__ __noinline__ Real manning_cf(Real gn2, Real h, Real cf0) {
-    Real cf = gn2 / pow(h, Real(1.0 / 3.0));
+__device__ __forceinline__ Real manning_cf(Real gn2, Real h, Real cf0) {
+    Real cf = gn2 * rcbrt(h);
     if (cf < cf0) cf = cf0;
     return cf;
 }
