@@ -673,11 +673,13 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD>::value))
                 // bathymetry-slope source, swe_source.hpp:15-21 (the analytic source follows in its own loop)
                 Real S[3] = {Real(0), g * (dbx * qg[0]), g * (dby * qg[0])};
                 // bottom friction, swe_source.hpp:29-51: S(qx, qy) -= Cf |u| / h (qx, qy), Cf the Chezy
-                // coefficient or, for Manning, max(g n^2 / h^(1/3), Cf)
+                // coefficient or, for Manning, max(g n^2 / h^(1/3), Cf); |u| as sqrt(u^2 + v^2) and / h as
+                // * (1 / h) where the reference has hypot and a division (each within an ulp; velocities
+                // are far from hypot's overflow range)
                 if (FRIC) {
                     const Real cf = A.friction == DGSW_FRICTION_MANNING ? manning_cf<Real>(A.manning[d], h, (Real)A.friction_cf)
                                                                         : (Real)A.friction_cf;
-                    const Real tau = cf * hypot(u, vv) / h;
+                    const Real tau = cf * sqrt(u * u + vv * vv) * ih;
                     S[1] -= tau * qg[1];
                     S[2] -= tau * qg[2];
                 }
