@@ -107,6 +107,7 @@ struct StageArgs {
     // levee interface fluxes of this stage, [n_levee][2][3][NG] (levee.cu): in side, then ex side
     const double* levF;
     unsigned char* went_dry;  // [ne] wet_dry_state.went_completely_dry of the last wet/dry pass, or null
+    int reverse;              // visit the tiles in reverse order (grid = one CTA per tile)
 };
 
 constexpr int FORCE_STRIDE_DEV = 9;
@@ -561,7 +562,9 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD>::value))
     double* shq = reinterpret_cast<double*>(smem_raw + SM::off_halo(TILE, max_halo, max_edges));  // [3*ND][max_halo]
     Real* shb = reinterpret_cast<Real*>(smem_raw + SM::off_hbath(TILE, max_halo, max_edges));      // [3][max_halo]
 
-    const int tile = blockIdx.x;
+    // odd stages walk the tiles backwards: they start on the tiles the previous stage wrote last,
+    // whose states are still in L2 (tiles are independent, so the results do not change)
+    const int tile = A.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
     const int e0 = tile * TILE;
     const int nloc = min(TILE, A.ne - e0);
     const int tid = threadIdx.x;
