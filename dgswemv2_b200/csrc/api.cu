@@ -235,7 +235,9 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.ramp_on = std::fabs(h->cfg.ramp_duration) < std::numeric_limits<double>::epsilon() * 100 ? 0 : 1;
     A.ramp_duration = h->cfg.ramp_duration;
     A.went_dry = h->went_dry.p;
-    A.reverse = s & 1;
+    // tile order alternates from stage to stage, across steps too (qswap flips once per step and keys
+    // the step graphs), so that each stage starts where the previous one ended
+    A.reverse = (s + h->qswap * h->ns) & 1;
 }
 
 cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, int mode) {
