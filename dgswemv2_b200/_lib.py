@@ -209,6 +209,12 @@ SIGNATURES = {
                                   C.c_int64, C.c_void_p, C.c_void_p]),
     "dgsw_mlp_adam": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_float,
                                   C.c_float, C.c_float, C.c_void_p]),
+    "dgsw_check_llf_flux": (C.c_int32, [C.c_int32, C.c_int64, C.c_double] + [C.POINTER(C.c_double)] * 6),
+    "dgsw_check_internal_flux": (C.c_int32, [C.c_int32, C.c_int64, C.c_double] + [C.POINTER(C.c_double)] * 6 +
+                                 [C.POINTER(C.c_uint8)] * 2 + [C.POINTER(C.c_double)] * 2),
+    "dgsw_check_wetting_drying": (C.c_int32, [C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                              C.POINTER(C.c_uint8), C.POINTER(C.c_double), C.POINTER(C.c_uint8),
+                                              C.POINTER(C.c_uint8)]),
     "dgsw_rkdg_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_synchronize": (C.c_int32, [C.c_void_p]),
     "dgsw_rkdg_last_step_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

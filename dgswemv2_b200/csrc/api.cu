@@ -216,6 +216,8 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.status = h->status.p;
     A.clock = h->clock.p;
     A.drk_s = h->cfg.dt * h->rk.drk[s];
+    A.stage_index = s;
+    A.nstages = h->ns;
     A.ne = (int)h->ne;
     A.ne_pad = (int)h->ne_pad;
     A.g = h->cfg.g;
@@ -452,12 +454,19 @@ int check_status(dgsw_rkdg_s* h) {
     CUDA_TRY(cudaMemcpyAsync(&st, h->status.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (st.nan_flag) {
-        uint32_t id = st.nan_ref_elem < h->topo.ids.size() ? h->topo.ids[st.nan_ref_elem] : 0;
+        // the first stage with a NaN and its smallest element, as the reference's per-stage scrutiny
+        // reports it before aborting
+        const uint32_t ref = (uint32_t)(st.nan_key & 0xffffffffull);
+        const unsigned long long counter = st.nan_key >> 32;
+        uint32_t id = ref < h->topo.ids.size() ? h->topo.ids[ref] : 0;
         DevStatus z;
         std::memset(&z, 0, sizeof(z));
-        z.nan_ref_elem = 0xffffffffu;
+        z.nan_key = ~0ull;
         cudaMemcpyAsync(h->status.p, &z, sizeof(z), cudaMemcpyHostToDevice, h->stream);
-        return fail(DGSW_ERR_NAN, "Fatal Error: NaN found at element " + std::to_string(id));
+        cudaStreamSynchronize(h->stream);
+        return fail(DGSW_ERR_NAN, "Fatal Error: NaN found at element " + std::to_string(id) + " (step " +
+                                      std::to_string(counter / (unsigned long long)h->ns) + ", stage " +
+                                      std::to_string(counter % (unsigned long long)h->ns) + ")");
     }
     return DGSW_OK;
 }
@@ -838,7 +847,7 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         if ((e = h->status.alloc(1)) != cudaSuccess) return cleanup_fail("alloc", e);
         DevStatus z;
         std::memset(&z, 0, sizeof(z));
-        z.nan_ref_elem = 0xffffffffu;
+        z.nan_key = ~0ull;
         cudaMemcpy(h->status.p, &z, sizeof(z), cudaMemcpyHostToDevice);
         if ((e = h->clock.alloc(1)) != cudaSuccess) return cleanup_fail("alloc", e);
         cudaMemset(h->clock.p, 0, sizeof(DevClock));

@@ -44,10 +44,14 @@ __device__ __forceinline__ void sfor(F&& f) {
     }
 }
 
+// NaN scrutiny (scrutinize_solution after every stage, rkdg_swe_proc_serial_step.hpp:59-65): the reference
+// stops at the first stage whose state holds a NaN and reports the first element (ascending ID) there.
+// nan_key = (stage counter << 32) | reference element index, stage counter = step * stages + stage, kept
+// as the minimum over all stages and elements of a batch: the first bad stage, then its smallest element.
 struct DevStatus {
+    unsigned long long nan_key;  // ~0 while no NaN has been seen
     unsigned int nan_flag;
-    unsigned int nan_ref_elem;  // smallest reference element index with a NaN
-    unsigned int pad[2];
+    unsigned int pad;
 };
 
 struct DevClock {
@@ -85,6 +89,7 @@ struct StageArgs {
     DevStatus* status;
     const DevClock* clock;
     double drk_s;  // stage-time offset of this stage (t + dt*drk[s])
+    int stage_index, nstages;  // this stage and the stages per step (the NaN report's stage counter)
     int ne;
     int ne_pad;
     int n_edges;  // total edge records (stride of egeo)
@@ -1034,8 +1039,9 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD>::value))
         }
     }
     if (has_nan) {
+        const unsigned long long counter = (unsigned long long)A.clock->step * A.nstages + A.stage_index;
         atomicOr(&A.status->nan_flag, 1u);
-        atomicMin(&A.status->nan_ref_elem, (unsigned int)A.ref_of_dev[d]);
+        atomicMin(&A.status->nan_key, (counter << 32) | (unsigned int)A.ref_of_dev[d]);
     }
 }
 

@@ -286,6 +286,25 @@ int32_t dgsw_mlp_grad(const float* d_x, const uint8_t* d_y, int64_t n, const flo
 int32_t dgsw_mlp_adam(float* d_params, float* d_m, float* d_v, const float* d_grad, int32_t step, float lr,
                       float beta1, float beta2, float eps, void* stream);
 
+/* ---- kernel self-checks: the stage kernel's device functions on caller data ----------------------
+ * Host arrays in and out (device scratch is allocated per call); no handle. They run the same device
+ * code the stage kernel inlines, so known-answer vectors can be checked against the CUDA path itself.
+ * precision: DGSW_FP64 or DGSW_FP32 (inputs are rounded to FP32 and the flux evaluated in FP32). */
+/* LLF_flux (rkdg_swe_LLF_flux.hpp:7-60) as test/test_llf_flux.cpp calls it: q_in, q_ex [n][3], bath and
+ * the spherical factor sp [n] (applied to the in side), unit normal [n][2] -> F [n][3] */
+int32_t dgsw_check_llf_flux(int32_t precision, int64_t n, double g, const double* q_in, const double* q_ex,
+                            const double* bath, const double* sp, const double* normal, double* F);
+/* ISP::Internal::ComputeFlux at one Gauss point (rkdg_swe_is_internal.hpp:26-95): LLF, F_ex = -F_in, and
+ * the wet/dry fix-ups for a dry side (wet flags [n] of each side, bathymetry of each side) */
+int32_t dgsw_check_internal_flux(int32_t precision, int64_t n, double g, const double* q_in, const double* q_ex,
+                                 const double* bath_in, const double* bath_ex, const double* sp, const double* normal,
+                                 const uint8_t* wet_in, const uint8_t* wet_ex, double* F_in, double* F_ex);
+/* wetting_drying_kernel (swe_post_wet_dry.hpp:6-145) on p = 1 elements as test/test_wetting_drying.cpp
+ * drives it: modal q [n][3 var][3 dof], bathymetry at the vertices [n][3], h_o (threshold
+ * 1e6 h_o eps as swe_pre_init_prob_params.hpp:36), wet flags in -> q_out, wet_out, went_dry (may be NULL) */
+int32_t dgsw_check_wetting_drying(int64_t n, const double* q, const double* bath_vrtx, double h_o,
+                                  const uint8_t* wet_in, double* q_out, uint8_t* wet_out, uint8_t* went_dry);
+
 /* execution control */
 int32_t dgsw_rkdg_set_stream(dgsw_handle h, void* cuda_stream);
 int32_t dgsw_rkdg_synchronize(dgsw_handle h);

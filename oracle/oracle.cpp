@@ -1805,6 +1805,50 @@ void orc_llf_flux(double g, const double* q_in, const double* q_ex, double bath,
     LLF_flux(g, q_in, q_ex, bath, sp, n, F);
 }
 
+// ISP::Internal::ComputeFlux at one Gauss point (rkdg_swe_is_internal.hpp:26-95), the per-point body of
+// interface_flux above: LLF with the in side's sp, F_ex = -F_in, the wet/dry fix-ups when a side is dry
+void orc_internal_flux(double g, const double* qi, const double* qe, double bath_in, double bath_ex, double sp_in,
+                       double sp_ex, const double* n, int wet_in, int wet_ex, double* Fi, double* Fe) {
+    const double n_in[2] = {n[0], n[1]};
+    const double n_ex[2] = {-n[0], -n[1]};
+    LLF_flux(g, qi, qe, bath_in, sp_in, n_in, Fi);
+    for (int v = 0; v < 3; ++v) Fe[v] = -Fi[v];
+    if (Fi[0] > 1e-12) {
+        if (!wet_in) {
+            for (int v = 0; v < 3; ++v) Fi[v] = 0.0;
+            land_flux(g, n_ex, qe, bath_ex, sp_ex, Fe);
+        } else if (!wet_ex) {
+            LLF_flux(0.0, qe, qi, bath_ex, sp_ex, n_ex, Fe);
+            Fe[0] = -Fi[0];
+        }
+    } else if (Fi[0] < -1e-12) {
+        if (!wet_ex) {
+            for (int v = 0; v < 3; ++v) Fe[v] = 0.0;
+            land_flux(g, n_in, qi, bath_in, sp_in, Fi);
+        } else if (!wet_in) {
+            LLF_flux(0.0, qi, qe, bath_in, sp_in, n_in, Fi);
+            Fi[0] = -Fe[0];
+        }
+    }
+}
+
+// the analytic function sets (true solution / source, bathymetry of Thacker's bowl) at n points, for
+// tests that check them against an independent evaluation
+int orc_fn_eval(int id, const double* params, double t, int what, int n, const double* x, const double* y,
+                double* out) {
+    for (int i = 0; i < n; ++i) {
+        if (what == 2) {
+            out[i] = fn_thacker_bath(params, x[i], y[i]);
+            continue;
+        }
+        const dgsw_fn3 f = what == 1 ? dgsw_fn_source(id, params, t, x[i], y[i]) : dgsw_fn_true(id, params, t, x[i], y[i]);
+        out[3 * i] = f.ze;
+        out[3 * i + 1] = f.qx;
+        out[3 * i + 2] = f.qy;
+    }
+    return 0;
+}
+
 int orc_dubiner(int p, int npt, const double* z1, const double* z2, double* phi, double* dphi1, double* dphi2) {
     vector<double> a(z1, z1 + npt), b(z2, z2 + npt);
     vector<double> ph = get_phi(p, a, b), d1, d2;

@@ -106,6 +106,12 @@ int orc_trouble(orc_handle h, double* I, uint8_t* troubled);
 // unit-level entry points used to pin the oracle against the reference's unit-test vectors
 void orc_llf_flux(double g, const double* q_in, const double* q_ex, double bath, double sp, const double* n,
                   double* F);
+// ISP::Internal::ComputeFlux at one Gauss point (LLF, F_ex = -F_in, wet/dry fix-ups for a dry side)
+void orc_internal_flux(double g, const double* qi, const double* qe, double bath_in, double bath_ex, double sp_in,
+                       double sp_ex, const double* n, int wet_in, int wet_ex, double* Fi, double* Fe);
+// function set `id` at n points: what 0 = true solution, 1 = source (out [n][3]), 2 = Thacker bathymetry (out [n])
+int orc_fn_eval(int id, const double* params, double t, int what, int n, const double* x, const double* y,
+                double* out);
 int orc_dubiner(int p, int npt, const double* z1, const double* z2, double* phi, double* dphi1, double* dphi2);
 int orc_triangle_rule(int degree, double* w, double* z1, double* z2, int cap);
 int orc_gl_rule(int degree, double* w, double* z, int cap);

@@ -1,8 +1,11 @@
 // Test driver for the C++ host side (include/dgsw_rkdg_problem.hpp): parses a `.15` input file and its
 // ADCIRC mesh without a GPU and prints what it read, one "key value" per line, then the host-only
 // topology of the mesh (dgsw_mesh_topology) as counts and checksums. Errors print "error <status>
-// <message>" and exit 3.
+// <message>" and exit 3. With a second argument (a directory), the mesh arrays the reader produced are
+// also written there as raw little-endian files (<name>.bin) plus an index (arrays.txt: name, type,
+// element count), so that a test can hand exactly these arrays to the library and to the oracle.
 #include <cstdint>
+#include <fstream>
 #include <iostream>
 
 #include "../../include/dgsw_rkdg_problem.hpp"
@@ -13,8 +16,20 @@ static uint64_t fnv(const void* p, size_t n, uint64_t h = 1469598103934665603ull
     return h;
 }
 
+struct Dump {
+    std::string dir;
+    std::ofstream index;
+    explicit Dump(const std::string& d) : dir(d), index(d + "/arrays.txt") {}
+    template <typename T>
+    void put(const std::string& name, const char* type, const std::vector<T>& v) {
+        std::ofstream f(dir + "/" + name + ".bin", std::ios::binary);
+        if (!v.empty()) f.write((const char*)v.data(), (std::streamsize)(v.size() * sizeof(T)));
+        index << name << " " << type << " " << v.size() << "\n";
+    }
+};
+
 int main(int argc, char** argv) {
-    if (argc != 2) return 1;
+    if (argc != 2 && argc != 3) return 1;
     try {
         dgsw::InputParameters in(argv[1]);
         const auto& pi = in.problem_input;
@@ -82,6 +97,29 @@ int main(int argc, char** argv) {
                   << "elem_ids_hash " << fnv(M.elem_names.data(), M.elem_names.size() * 4) << "\n"
                   << "seg_type_hash " << fnv(M.seg_type.data(), M.seg_type.size() * 4) << "\n"
                   << "seg_nodes_hash " << fnv(M.seg_nodes.data(), M.seg_nodes.size() * 4) << "\n";
+        if (argc == 3) {
+            Dump D(argv[2]);
+            D.put("node_xyz", "f64", M.node_xyz);
+            D.put("elem_nodes", "i32", M.elem_nodes);
+            D.put("elem_ids", "u32", M.elem_names);
+            D.put("seg_type", "i32", M.seg_type);
+            D.put("seg_offsets", "i64", M.seg_offsets);
+            D.put("seg_nodes", "i32", M.seg_nodes);
+            D.put("node_manning_n", "f64", M.node_manning_n);
+            D.put("levee_nodes", "i32", M.levee_nodes);
+            D.put("levee_data", "f64", M.levee_data);
+            for (size_t b = 0; b < M.forcing.size(); ++b) {
+                const auto& F = M.forcing[b];
+                const std::string k = "forcing" + std::to_string(b) + "_";
+                D.put(k + "type", "i32", std::vector<int32_t>{F.type});
+                D.put(k + "nodes", "i32", F.nodes);
+                D.put(k + "frequency", "f64", F.frequency);
+                D.put(k + "forcing_fact", "f64", F.forcing_fact);
+                D.put(k + "equilib_arg", "f64", F.equilib_arg);
+                D.put(k + "amplitude", "f64", F.amplitude);
+                D.put(k + "phase", "f64", F.phase);
+            }
+        }
         const dgsw_mesh m = M.view();
         int64_t ni = 0, nb = 0;
         dgsw::check(dgsw_mesh_topology(&m, nullptr, nullptr, &ni, nullptr, &nb, nullptr), "dgsw_mesh_topology");

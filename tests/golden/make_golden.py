@@ -1,9 +1,9 @@
 """Extract the known-answer vectors of the reference's unit tests into JSON fixtures.
 
-Run in a container where the reference checkout is mounted (default path below); the fixtures are
-committed so the tests never read the reference at run time.
+Run where a checkout of the reference is available, giving its path; the fixtures are committed so
+the tests never read the reference at run time.
 
-    python tests/golden/make_golden.py [/path/to/dgswemv2]
+    python tests/golden/make_golden.py /path/to/dgswemv2
 
 Sources (paths inside the reference project):
   test/test_llf_flux.cpp:66-171            three LLF configurations and their expected fluxes
@@ -12,6 +12,13 @@ Sources (paths inside the reference project):
   test/test_element_triangle.cpp:1-48      the triangle and the integrand (x+1)^2 + (y-1)^2
   test/test_wetting_drying.cpp:15-380      five single-element wetting/drying cases
 The numbers are read from the files; nothing here re-types them.
+
+Input files the reference's tests and correctness scripts run, copied byte for byte into
+tests/golden/reference_inputs/:
+  test/files_for_testing/sample_fort.14              the mesh of test/test_mesh_metadata.cpp:26-45
+  test/files_for_testing/weir/{dgswemv2_input.15, weir.14, weir.bcis}
+                                                     the RKDG levee / flow / limiter case of
+                                                     scripts/correctness/test_rkdg_parallel_weirs.sh
 """
 import json
 import math
@@ -19,7 +26,7 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = None  # the reference checkout, from the command line
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 NUM = r"[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?"
@@ -174,13 +181,35 @@ def wet_dry():
             "vertices": verts[:3], "cases": cases}
 
 
+INPUT_FILES = [
+    ("test/files_for_testing/sample_fort.14", "sample_fort.14"),
+    ("test/files_for_testing/weir/dgswemv2_input.15", "weir/dgswemv2_input.15"),
+    ("test/files_for_testing/weir/weir.14", "weir/weir.14"),
+    ("test/files_for_testing/weir/weir.bcis", "weir/weir.bcis"),
+]
+
+
+def copy_inputs():
+    for src, dst in INPUT_FILES:
+        out = os.path.join(OUT, "reference_inputs", dst)
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        with open(os.path.join(REF, src), "rb") as f, open(out, "wb") as g:
+            g.write(f.read())
+        print("copied", dst)
+
+
 def main():
+    global REF
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/dgswemv2")
+    REF = sys.argv[1]
     fixtures = {"llf_flux.json": llf(), "dubiner_2d.json": dubiner(), "element_triangle.json": element(),
                 "wetting_drying.json": wet_dry()}
     for name, data in fixtures.items():
         with open(os.path.join(OUT, name), "w") as f:
             json.dump(data, f, indent=1)
         print("wrote", name)
+    copy_inputs()
 
 
 if __name__ == "__main__":

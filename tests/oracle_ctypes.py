@@ -220,6 +220,9 @@ class Oracle:
         lib.orc_ndof.argtypes = [C.c_void_p]
         lib.orc_llf_flux.argtypes = [C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double, C.c_double,
                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        D = C.POINTER(C.c_double)
+        lib.orc_internal_flux.argtypes = [C.c_double, D, D, C.c_double, C.c_double, C.c_double, C.c_double, D, C.c_int,
+                                          C.c_int, D, D]
         self.lib = lib
 
     def problem(self, cfg, mesh, n_threads=1):
@@ -234,6 +237,27 @@ class Oracle:
         self.lib.orc_llf_flux(g, _ptr(a, C.c_double), _ptr(b, C.c_double), bath, sp, _ptr(nn, C.c_double),
                               _ptr(F, C.c_double))
         return F
+
+    def internal_flux(self, g, q_in, q_ex, bath_in, bath_ex, sp, n, wet_in, wet_ex):
+        a = np.ascontiguousarray(q_in, np.float64)
+        b = np.ascontiguousarray(q_ex, np.float64)
+        nn = np.ascontiguousarray(n, np.float64)
+        Fi, Fe = np.zeros(3), np.zeros(3)
+        self.lib.orc_internal_flux(g, _ptr(a, C.c_double), _ptr(b, C.c_double), bath_in, bath_ex, sp, sp,
+                                   _ptr(nn, C.c_double), int(wet_in), int(wet_ex), _ptr(Fi, C.c_double),
+                                   _ptr(Fe, C.c_double))
+        return Fi, Fe
+
+    def fn_eval(self, fn_set, params, t, what, x, y):
+        """function_sets.h as the oracle compiles it: what 0 true solution, 1 source ([n][3]), 2 bowl bathymetry."""
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        P = np.zeros(16)
+        P[:len(params)] = params
+        out = np.zeros((len(x), 3)) if what != 2 else np.zeros(len(x))
+        self.lib.orc_fn_eval(int(fn_set), _ptr(P, C.c_double), C.c_double(t), int(what), len(x), _ptr(x, C.c_double),
+                             _ptr(y, C.c_double), _ptr(out, C.c_double))
+        return out
 
     def dubiner(self, p, pts):
         pts = np.asarray(pts, np.float64)

@@ -131,6 +131,41 @@ def test_nan_is_reported_not_aborted(oracle):
     assert "element" in str(ei.value)
 
 
+def test_nan_mid_batch_reports_the_first_stage_and_element(oracle):
+    """A NaN that enters in the middle of a batch of steps is reported as the reference's per-stage
+    scrutiny reports it (rkdg_swe_proc_serial_step.hpp:59-65): at the first stage whose new state holds a
+    NaN, the smallest element ID there - not the smallest ID carrying a NaN when the batch ends, by which
+    time the NaN has spread. The NaN goes into one element's stage-1 state; the oracle, stepped stage by
+    stage, gives the expected stage and element."""
+    from dgswemv2_b200._lib import DgswError
+
+    mesh, cfg = configs.manufactured(10, p=1, rk=(3, 3), dt=5.0)
+    P = Problem(cfg, mesh)
+    O = oracle.problem(cfg, mesh)
+    P.stage_serial()
+    O.stage()
+    q = P.get_state()
+    bad = 117
+    q[bad, 2, 1] = np.nan
+    P.set_state(q)
+    O.set_state(q)
+    expected = None
+    for k in range(1, 9):  # stages 1, 2 of step 0, then step 1, ...
+        try:
+            O.stage()
+        except RuntimeError as e:  # the oracle's scrutiny stops at the first stage with a NaN
+            rows = np.nonzero(np.isnan(O.get_state()).any(axis=(1, 2)))[0]
+            expected = (k // 3, k % 3, int(rows.min()))
+            assert "NaN found at element %d" % expected[2] in str(e)
+            break
+    assert expected is not None and expected[:2] == (0, 1)
+    assert expected[2] < bad  # a neighbour with a smaller ID is hit at the same stage
+    with pytest.raises(DgswError) as ei:
+        P.step_serial(4)
+    assert ei.value.status == 4
+    assert "NaN found at element %d (step %d, stage %d)" % (expected[2], expected[0], expected[1]) in str(ei.value)
+
+
 def test_fp32_bowl_keeps_the_fp64_wet_set():
     """Bowl with Gaussian humps at 131,072 triangles, FP32 bulk arithmetic: a flattened dry cell sits at
     depth h_o, which the FP64 threshold 1e6 h_o eps separates from wet only if the stage states carry
