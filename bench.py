@@ -27,12 +27,15 @@ sys.path.insert(0, ROOT)
 
 METRIC = "element-DOF updates/s per RK stage, FP32+MLP vs FP64 plain on B200 at equal L2"
 UNIT = "element-DOF/s"
-# compulsory HBM bytes per element-DOF and RK stage for p=2 SSP-RK3 (state in, q0 on 2 of 3 stages,
-# state out, per-element geometry and per-edge data, each array touched once): FP32 45 B, FP64 87 B
 # compulsory HBM bytes per element-DOF per RK stage (each array touched once): stage states read
 # (1 + the fraction of stages that also read q_0) and written, FP64 in both precisions; element
 # geometry and bathymetry (FP32 in the FP32 path) and the edge records. p = 2 SSP-RK3, p = 1 SSP-RK2.
 ALG_BYTES_PER_UNIT = {("fp32", 2): 77.0, ("fp64", 2): 87.0, ("fp32", 1): 82.0, ("fp64", 1): 99.0}
+
+
+def workload_name(nq, ne):
+    return ("manufactured solution p=2 at scale: %dx%d quads -> %d jittered triangles, Dunavant deg 4 / "
+            "3-pt Gauss-Legendre, LLF, SSP-RK3" % (nq, nq, ne))
 
 
 def parse():
@@ -49,34 +52,94 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+    """SM clock, power and throttle reasons sampled while the timed region runs: NVML polled every 2 ms
+    from a thread (a short timed region still gets samples), else nvidia-smi at its 100 ms minimum."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML_REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+                    ("sw_power_cap", 0x4))
+    SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
+        self.samples = []  # (sm_mhz, max_mhz, power_w, set of reasons)
         self.proc = None
-        self.lines = []
+        self.nv = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.device)
+        try:
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _sample_nvml(self):
+        nv, h = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+        try:
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.samples.append((float(sm), float(smax), pw, {n for n, bit in self.NVML_REASONS if r & bit}))
+
+    def _poll(self):
+        while not self._stop.is_set():
+            try:
+                self._sample_nvml()
+            except Exception:
+                return
+            time.sleep(0.002)
+
+    def _read_smi(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm, smax, pw = float(parts[1]), float(parts[2]), float(parts[3])
+            except ValueError:
+                continue
+            self.samples.append((sm, smax, pw, {n for n, v in zip(names, parts[5:9]) if v.lower().startswith("active")}))
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
+            self.nv = self._nvml_handle()
+            self._sample_nvml()
+            self._t = threading.Thread(target=self._poll, daemon=True)
         except Exception:
-            self.proc = None
+            self.nv = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.SMI_FIELDS,
+                     "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE,
+                    stderr=subprocess.DEVNULL, text=True)
+                self._t = threading.Thread(target=self._read_smi, daemon=True)
+            except Exception:
+                self.proc = None
+        if self._t:
+            self._t.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc:
+        self._stop.set()
+        if self.nv:
+            self._t.join(timeout=2)
+            try:
+                self._sample_nvml()
+            except Exception:
+                pass
+        elif self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -85,22 +148,14 @@ class ClockSampler:
             self._t.join(timeout=2)
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [x[0] for x in self.samples]
+        reasons = set()
+        for x in self.samples:
+            reasons |= x[3]
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": self.samples[-1][1] if self.samples else None, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max((x[2] for x in self.samples), default=None),
+                "source": "nvml 2 ms" if self.nv else "nvidia-smi 100 ms"}
 
 
 def dist_setup(n, backend=None):
@@ -175,18 +230,15 @@ def load_traffic(precision):
         return None
 
 
-def cpu_baseline(nq, seconds, precision_note):
-    """The oracle (FP64 CPU restatement) on the host cores, on a bounded sample of the workload."""
-    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+def oracle_rate(nq, seconds, threads):
+    """FP64 oracle steps of the config-2 discretisation on an nq x nq mesh for about `seconds`:
+    (element-DOF/s, steps, elapsed s, triangles)."""
     from dgswemv2_b200 import configs
     from tests.oracle_ctypes import Oracle
 
-    cores = os.cpu_count() or 1
     O = Oracle(os.path.join(ROOT, "oracle", "build", "liboracle.so"))
-    # size the sample so one RK step takes well under the budget: start from a quarter-size mesh
-    sub = max(32, nq // 4)
-    mesh, cfg = configs.config2(nq=sub)
-    P = O.problem(cfg, mesh, n_threads=cores)
+    mesh, cfg = configs.config2(nq=nq)
+    P = O.problem(cfg, mesh, n_threads=threads)
     P.step(1)  # warm-up
     n, t0 = 0, time.perf_counter()
     while True:
@@ -195,11 +247,25 @@ def cpu_baseline(nq, seconds, precision_note):
         el = time.perf_counter() - t0
         if el >= seconds or n >= 1000:
             break
-    units = mesh.n_elems * 6 * 3 * n
-    return {"value": units / el, "unit": UNIT, "cores": cores, "kind": "port",
+    return mesh.n_elems * 6 * 3 * n / el, n, el, mesh.n_elems
+
+
+def cpu_baseline(nq, seconds):
+    """The oracle (FP64 C++ restatement of the reference step) on the host cores, on bounded samples of the
+    workload: all host threads (OpenMP) on a quarter-size mesh, and one thread (the reference's serial
+    driver) on an eighth-size mesh."""
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    cores = os.cpu_count() or 1
+    sub = max(32, nq // 4)
+    v, n, el, ne = oracle_rate(sub, seconds, cores)
+    sub1 = max(16, nq // 8)
+    v1, n1, el1, ne1 = oracle_rate(sub1, seconds / 2, 1)
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": "oracle (FP64 C++ restatement of the reference step) on the same discretisation at %dx%d quads "
-                      "(%d triangles), %d SSP-RK3 steps in %.1f s, %d OpenMP threads" % (sub, sub, mesh.n_elems, n, el,
-                                                                                        cores)}
+                      "(%d triangles), %d SSP-RK3 steps in %.1f s, %d OpenMP threads" % (sub, sub, ne, n, el, cores),
+            "serial": {"value": v1, "unit": UNIT, "cores": 1,
+                       "sample": "the same oracle on one thread (as the reference's serial driver runs), %dx%d quads "
+                                 "(%d triangles), %d steps in %.1f s" % (sub1, sub1, ne1, n1, el1)}}
 
 
 def run_reference(args):
@@ -212,8 +278,8 @@ def run_reference(args):
 
     cores = os.cpu_count() or 1
     O = Oracle(os.path.join(ROOT, "oracle", "build", "liboracle.so"))
-    # each step is one SSP-RK3 step on a bounded sample of the workload: the mesh is scaled so that
-    # warm-up + timed steps take about two minutes on this host
+    # each step is one SSP-RK3 step of the workload; when warm-up + timed steps would take more than
+    # about two minutes on this host, the mesh is scaled down and the line says so
     budget = 120.0
     nq = args.nq
     while True:
@@ -231,15 +297,17 @@ def run_reference(args):
     el = time.perf_counter() - t0
     units = mesh.n_elems * 6 * 3 * args.steps
     v = units / el
+    sample = ("oracle FP64 C++ restatement of the reference step (the reference needs Eigen, yaml-cpp and METIS, "
+              "absent here), %dx%d quads, %d OpenMP threads" % (nq, nq, cores))
+    if nq != args.nq:
+        sample += "; mesh scaled down from %dx%d to keep %d steps within %d s" % (args.nq, args.nq,
+                                                                                  args.steps + args.warmup, budget)
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "manufactured solution p=2, SSP-RK3, jittered triangles (%dx%d quads, %d triangles)" % (
-            nq, nq, mesh.n_elems), "p": 2, "rk": "SSP(3,3)", "precision": "fp64"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": "oracle FP64 C++ restatement of the reference step (the reference needs Eigen, "
-                                   "yaml-cpp and METIS, absent here), %dx%d quads, %d OpenMP threads" % (nq, nq, cores)},
+        "config": {"workload": workload_name(nq, mesh.n_elems), "elements": mesh.n_elems, "p": 2, "rk": "SSP(3,3)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -256,37 +324,75 @@ def time_steps(P, K):
     return ms, launches, wall
 
 
-def limiter_workload(dev, steps=400, warmup=5):
-    """The metric's "FP32 + MLP vs FP64 plain" on the limited workload it concerns: config 3 (Thacker bowl,
-    131,072 triangles, p = 1, wetting/drying + Cockburn-Shu limiter). FP32 bulk with the learned
-    indicator gating the limiter (confidence 0.9, committed weights) against the FP64 path with the
-    plain limiter, plus FP32 with the plain limiter; device time of graph-replayed steps, L2 error
-    against the analytic solution after the same number of steps."""
+def e2e_leg(P, steps, world):
+    """The metric through the host API every step: set_state from pinned host memory, one RK step,
+    get_state back into the same pinned buffer (wall clock, max over ranks)."""
+    import torch
+
+    ne, nd, ns = P.ne, P.nd, P.cfg.rk_nstages
+    host = torch.empty((ne, 3, nd), dtype=torch.float64).pin_memory()
+    hq = host.numpy()
+    hq[:] = P.get_state()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        P.set_state(hq)
+        P.step_serial(1)
+        P.get_state(out=hq)
+    torch.cuda.synchronize()
+    el = dist_max(time.perf_counter() - t0, world)
+    barrier(world)
+    return {"value": ne * nd * ns * steps * world / el, "unit": UNIT, "h2d_bytes_per_step": int(hq.nbytes),
+            "d2h_bytes_per_step": int(hq.nbytes), "steps": steps}
+
+
+def limiter_workload(dev, steps=400, warmup=5, nq=256, dt=0.25, name="config 3: Thacker bowl, 131072 triangles"):
+    """The metric's "FP32 + MLP vs FP64 plain" on the limited workloads it concerns: the Thacker bowl (p = 1,
+    wetting/drying + Cockburn-Shu limiter). FP32 bulk with the learned indicator gating the limiter
+    (confidence 0.9, committed weights) against the FP64 path with the plain limiter, plus FP32 with the
+    plain limiter; device time of graph-replayed steps, L2 error against the analytic solution after the
+    same number of steps."""
     from dgswemv2_b200 import Problem, configs, indicator
 
     W = indicator.load_weights()
-    out = {"workload": "config 3: Thacker bowl, 131072 triangles, p=1, SSP-RK2, wetting/drying + limiter",
-           "steps": steps + warmup}
-    for name, prec, mode in (("fp32_mlp", "fp32", 1), ("fp32_plain", "fp32", 0), ("fp64_plain", "fp64", 0)):
-        mesh, cfg = configs.config3(precision=prec)
+    out = {"workload": name + ", p=1, SSP-RK2, wetting/drying + limiter", "steps": steps + warmup}
+    for key, prec, mode in (("fp32_mlp", "fp32", 1), ("fp32_plain", "fp32", 0), ("fp64_plain", "fp64", 0)):
+        mesh, cfg = configs.config3(nq=nq, dt=dt, precision=prec)
         P = Problem(cfg, mesh, device=dev)
         if mode:
             P.set_indicator(W, confidence=0.9, mode=mode)
         P.step_serial(warmup)
         ms, _, _ = time_steps(P, steps)
         units = P.ne * P.nd * cfg.rk_nstages * steps
-        out[name] = {"value": units / (ms / 1e3), "ms_per_step": ms / steps, "l2_error": P.compute_residual_L2()}
+        out[key] = {"value": units / (ms / 1e3), "ms_per_step": ms / steps, "l2_error": P.compute_residual_L2()}
         if mode:
             c = P.indicator_stats()
-            out[name]["sent_fraction"] = c[1] / max(1, c[0])
+            out[key]["sent_fraction"] = c[1] / max(1, c[0])
         del P
     out["speedup_fp32_mlp_over_fp64_plain"] = out["fp32_mlp"]["value"] / out["fp64_plain"]["value"]
     out["l2_ratio_fp32_mlp_over_fp64_plain"] = out["fp32_mlp"]["l2_error"] / out["fp64_plain"]["l2_error"]
     return out
 
 
+def ensemble_workload(dev, steps=20, warmup=3):
+    """Config 5: 256 p = 1 members of 64^2 to 200^2 quads with wetting/drying, FP32 bulk, one autotuned
+    stage-kernel launch per RK stage for all members, graph-replayed steps."""
+    from dgswemv2_b200 import configs, ensemble
+
+    meshes, cfgs = configs.config5(precision="fp32")
+    t0 = time.perf_counter()
+    E = ensemble(cfgs[0], meshes, [c.fn_params for c in cfgs], device=dev)
+    create_s = time.perf_counter() - t0
+    E.step_serial(warmup)
+    ms, launches, _ = time_steps(E, steps)
+    m0 = E.mass()
+    return {"workload": "config 5: ensemble of 256 p=1 members (64^2-200^2 quads, %d triangles), wetting/drying, "
+                        "FP32 bulk" % E.ne, "steps": steps, "value": E.ne * E.nd * E.cfg.rk_nstages * steps / (ms / 1e3),
+            "ms_per_step": ms / steps, "tile_autotuned": E.info.tile, "tuning": E.tuning(),
+            "kernel_launches_per_step": launches / steps, "create_seconds": create_s, "mass": m0}
+
+
 def run_ours(args):
-    import numpy as np
     import torch
 
     world, rank, local = dist_setup(args.gpus)
@@ -308,6 +414,11 @@ def run_ours(args):
         barrier(world)
     ms = dist_max(ms, world)
     value = job_value(units_per_step, args.steps, world, ms)
+    # the stage kernel's own duration: the same number of steps again, each stage-kernel launch bracketed
+    # by CUDA events on the handle's stream (stages launched one by one)
+    kms, klaunches = P.step_timed(args.steps)
+    stage_ms = dist_max(kms / max(1, klaunches), world)
+    e2e = e2e_leg(P, max(3, min(args.steps, 40)), world)
 
     # the FP64 plain path on the same workload (the comparator of the FP32 path)
     fp64 = None
@@ -319,52 +430,37 @@ def run_ours(args):
         ms64, _, _ = time_steps(P64, args.steps)
         barrier(world)
         ms64 = dist_max(ms64, world)
+        k64, n64 = P64.step_timed(args.steps)
         fp64 = {"value": job_value(units_per_step, args.steps, world, ms64), "ms_per_step": ms64 / args.steps,
-                "tile_autotuned": P64.info.tile}
+                "tile_autotuned": P64.info.tile, "stage_kernel_ms": dist_max(k64 / max(1, n64), world)}
+        fp64["stage_kernel_frac_of_hbm"] = (ALG_BYTES_PER_UNIT[("fp64", cfg.p)] * ne * nd /
+                                            (fp64["stage_kernel_ms"] / 1e3) / 1e9 / load_peaks()[0])
+        fp64["e2e"] = e2e_leg(P64, max(3, min(args.steps, 40)), world)
+        # both paths advanced the same steps: warm-up, timed, kernel-timed and e2e
         l2_32, l2_64 = P.compute_residual_L2(), P64.compute_residual_L2()
         fp64["l2_error_fp64"] = l2_64
         fp64["l2_error_fp32"] = l2_32
         fp64["l2_ratio_fp32_over_fp64"] = l2_32 / l2_64
         del P64
 
-    # end to end through the C ABI host API: H2D of the state from pinned memory, one RK step,
-    # D2H of the new state, every step
-    ke = max(3, min(args.steps, 40))
-    host = torch.empty((ne, 3, nd), dtype=torch.float64).pin_memory()
-    host.numpy()[:] = P.get_state()
-    hq = host.numpy()
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(ke):
-        P.set_state(hq)
-        P.step_serial(1)
-        P.get_state(out=hq)
-    torch.cuda.synchronize()
-    e2e_s = dist_max(time.perf_counter() - t0, world)
-    barrier(world)
-    e2e = {"value": units_per_step * ke * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(hq.nbytes),
-           "d2h_bytes_per_step": int(hq.nbytes), "steps": ke}
-
     peak, peak_kind = load_peaks()
-    stage_ms = ms / (args.steps * ns)
     alg = ALG_BYTES_PER_UNIT[(args.precision, cfg.p)] * ne * nd
     achieved = alg / (stage_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": load_traffic(args.precision), "peak_kind": peak_kind,
                 "kernel": "rkdg_stage_kernel<2,%s,...>" % ("float" if args.precision == "fp32" else "double"),
-                "stage_kernel_ms": stage_ms, "algorithmic_bytes_per_launch": alg}
+                "stage_kernel_ms": stage_ms, "stage_kernel_launches_timed": int(klaunches),
+                "step_ms_over_stages": ms / (args.steps * ns), "algorithmic_bytes_per_launch": alg}
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": "manufactured solution p=2 at scale: %dx%d quads -> %d jittered triangles, Dunavant "
-                               "deg 4 / 3-pt Gauss-Legendre, LLF, SSP-RK3" % (args.nq, args.nq, ne),
-                   "elements": ne, "p": 2, "rk": "SSP(3,3)", "precision": args.precision,
-                   "parallelism": "replicas" if world > 1 else "single GPU",
-                   "tile_fp32_autotuned": P.info.tile,
+        "config": {"workload": workload_name(args.nq, ne), "elements": ne, "p": 2, "rk": "SSP(3,3)",
                    "l2_cache": "no flush: the per-step working set (%d MB of stage states, bathymetry and mesh "
                                "arrays) exceeds the 126 MB L2" % int(P.info.device_bytes / 2 ** 20)},
+        "precision": args.precision, "parallelism": "replicas" if world > 1 else "single GPU",
+        "tile_autotuned": P.info.tile,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "e2e": e2e,
@@ -376,9 +472,14 @@ def run_ours(args):
     if args.precision == "fp32":
         out["limiter_workload"] = limiter_workload(dev)
         barrier(world)
+        out["limiter_workload_config4"] = limiter_workload(dev, steps=50, nq=1024, dt=0.06,
+                                                           name="config 4: Thacker bowl, 2097152 triangles")
+        barrier(world)
+        out["ensemble_workload"] = ensemble_workload(dev)
+        barrier(world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            out["cpu_baseline"] = cpu_baseline(args.nq, args.cpu_seconds, args.precision)
+            out["cpu_baseline"] = cpu_baseline(args.nq, args.cpu_seconds)
         except Exception as e:  # the CPU leg must not hide the GPU number
             out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                    "sample": "failed: %s" % e}

@@ -272,6 +272,13 @@ class Problem:
     def get_state_device(self, dptr):
         _lib.check(_lib.load().dgsw_rkdg_get_state_device(self._h, C.c_void_p(dptr)))
 
+    def step_timed(self, nsteps):
+        """nsteps steps with every stage-kernel launch timed by its own CUDA events (no step graphs):
+        (summed stage-kernel milliseconds, number of stage-kernel launches)."""
+        ms, n = C.c_double(), C.c_int64()
+        _lib.check(_lib.load().dgsw_rkdg_step_timed(self._h, int(nsteps), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def time(self):
         t = C.c_double()
         st = C.c_int64()

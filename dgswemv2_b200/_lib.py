@@ -218,6 +218,7 @@ SIGNATURES = {
     "dgsw_rkdg_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_synchronize": (C.c_int32, [C.c_void_p]),
     "dgsw_rkdg_last_step_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "dgsw_rkdg_step_timed": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
 }
 
 _lib = None

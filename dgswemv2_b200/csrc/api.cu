@@ -149,6 +149,10 @@ struct dgsw_rkdg_s {
     cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
     int qswap = 0;  // parity of the q_0 <-> q_ns swaps so far
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // per-launch timing of the stage kernel (dgsw_rkdg_step_timed): event pairs, recorded while kt_on
+    std::vector<cudaEvent_t> kt_ev;
+    bool kt_on = false;
+    size_t kt_used = 0;
     DBuf<L2Rule> l2rule;
     DBuf<double> staging;  // FP64 host-layout state for the host API (allocated on first use)
     double last_ms = 0.0;
@@ -365,8 +369,18 @@ __global__ void record_labels_kernel(const unsigned char* limited, const int* re
 
 // one RK stage: stage kernel, (clock on the last stage), indicator, limiter, wet flag buffer flip
 cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageRecord* rec = nullptr) {
+    const bool timed = h->kt_on && h->kt_used + 2 <= h->kt_ev.size();
+    if (timed) {
+        cudaError_t e = cudaEventRecord(h->kt_ev[h->kt_used], h->stream);
+        if (e != cudaSuccess) return e;
+    }
     cudaError_t e = h->fp32 ? launch_stage<float>(h, s) : launch_stage<double>(h, s);
     if (e != cudaSuccess) return e;
+    if (timed) {
+        e = cudaEventRecord(h->kt_ev[h->kt_used + 1], h->stream);
+        if (e != cudaSuccess) return e;
+        h->kt_used += 2;
+    }
     launches += h->n_levee ? 2 : 1;
     h->wet_cur = 1 - h->wet_cur;
     int s_out = s + 1;
@@ -1219,6 +1233,7 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     h->ind_gate.release();
     h->ind_counters.release();
     h->ind_error.release();
+    for (cudaEvent_t ev : h->kt_ev) cudaEventDestroy(ev);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1567,6 +1582,37 @@ int32_t dgsw_rkdg_step(dgsw_handle h, int32_t nsteps) {
     h->last_ms = ms;
     h->last_launches = launches;
     return rc;
+}
+
+int32_t dgsw_rkdg_step_timed(dgsw_handle h, int32_t nsteps, double* stage_ms, int64_t* stage_launches) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (nsteps < 0 || nsteps > 100000) return fail(DGSW_ERR_INVALID_ARGUMENT, "step count out of range");
+    cudaSetDevice(h->device);
+    // one event pair per stage of the batch, created once and kept for later calls
+    const size_t need = 2 * (size_t)(nsteps + 1) * (size_t)h->ns;
+    while (h->kt_ev.size() < need) {
+        cudaEvent_t ev;
+        CUDA_TRY(cudaEventCreate(&ev));
+        h->kt_ev.push_back(ev);
+    }
+    // the stages run as separate launches (no step graphs), each bracketed by its own events
+    const int32_t graphs = h->cfg.use_graphs;
+    h->cfg.use_graphs = 0;
+    h->kt_on = true;
+    h->kt_used = 0;
+    const int32_t rc = dgsw_rkdg_step(h, nsteps);
+    h->kt_on = false;
+    h->cfg.use_graphs = graphs;
+    if (rc != DGSW_OK) return rc;
+    double total = 0.0;
+    for (size_t i = 0; i + 1 < h->kt_used; i += 2) {
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, h->kt_ev[i], h->kt_ev[i + 1]));
+        total += ms;
+    }
+    if (stage_ms) *stage_ms = total;
+    if (stage_launches) *stage_launches = (int64_t)(h->kt_used / 2);
+    return DGSW_OK;
 }
 
 int32_t dgsw_rkdg_get_time(dgsw_handle h, double* t, int64_t* step, int32_t* stage) {

@@ -311,6 +311,11 @@ int32_t dgsw_rkdg_synchronize(dgsw_handle h);
 /* device time of the most recent dgsw_rkdg_step call's stage kernels, from CUDA events recorded on the
  * handle's stream around it: total milliseconds and number of stage-kernel launches */
 int32_t dgsw_rkdg_last_step_timing(dgsw_handle h, double* ms, int64_t* kernel_launches);
+/* dgsw_rkdg_step(h, nsteps) with the stages launched one by one (no step graph) and a CUDA event pair
+ * recorded on the handle's stream around every stage-kernel launch (with its levee pass on meshes with
+ * levees): the summed device time of those launches and their number (a measurement aid; the same
+ * states result as from dgsw_rkdg_step) */
+int32_t dgsw_rkdg_step_timed(dgsw_handle h, int32_t nsteps, double* stage_ms, int64_t* stage_launches);
 
 #ifdef __cplusplus
 }
