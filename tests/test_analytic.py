@@ -126,14 +126,18 @@ def l2_pair(P, mesh, true, order):
 @pytest.mark.gpu
 @pytest.mark.parametrize("p,rk", [(1, (2, 2)), (2, (3, 3))])
 def test_manufactured_h_convergence(p, rk):
-    """nq x nq quads (nq = 8, 16, 32, 64; jitter 0.1) on the config-1 square, to t = 2000 s with dt = 4 s."""
+    """nq x nq quads (nq = 8, 16, 32, 64; jitter 0.1) on the config-1 square, to t = 200 s with dt = 0.05 s.
+    The time step is small because the reference's SSP-RK stage times all equal the step's start time
+    (the crk/drk recurrence of explicit_ssp_rk_stepper.cpp:262-277 gives zero offsets for these tables),
+    so a time-dependent source enters at first order in dt: at dt = 4 s to t = 2000 s that error, about
+    8 in this L2 norm, hides the p = 2 spatial error from 32^2 quads on."""
     M = analytic.Manufactured()
     errs = []
     for nq in (8, 16, 32, 64):
-        mesh, cfg = configs.manufactured(nq, p=p, rk=rk, dt=4.0, jitter=0.1, seed=5)
+        mesh, cfg = configs.manufactured(nq, p=p, rk=rk, dt=0.05, jitter=0.1, seed=5)
         P = Problem(cfg, mesh)
-        P.step_serial(500)
-        assert P.time()[0] == 2000.0
+        P.step_serial(4000)
+        assert abs(P.time()[0] - 200.0) <= 1e-9
         e_np, e_lib = l2_pair(P, mesh, M, p)
         assert abs(e_np - e_lib) <= 1e-6 * e_lib, (nq, e_np, e_lib)
         errs.append(e_np)

@@ -92,6 +92,18 @@ def test_fp32_bulk_l2_within_5_percent(oracle):
     assert rel_err(P.get_state(), O.get_state()) < 1e-4
 
 
+def test_fp32_l2_stays_within_5_percent_over_2000_steps():
+    """Config-2 discretisation (p = 2, SSP-RK3, jittered) at 64 x 64 quads for 2,000 steps of dt = 2 s: the
+    FP32 path's L2 error against the analytic solution within 1.05x of the FP64 path's."""
+    l2 = {}
+    for prec in ("fp32", "fp64"):
+        mesh, cfg = configs.manufactured(64, p=2, rk=(3, 3), dt=2.0, jitter=0.2, precision=prec)
+        P = Problem(cfg, mesh)
+        P.step_serial(2000)
+        l2[prec] = P.compute_residual_L2()
+    assert l2["fp32"] <= 1.05 * l2["fp64"], l2
+
+
 def test_land_boundaries_conserve_mass(oracle):
     """Closed basin with land boundaries: FP64 mass is conserved to rounding."""
     mesh = meshgen.quad_mesh(16, 16, corners=((0, 0), (1000, 0), (1000, 1000), (0, 1000)), bc=(LAND,) * 4,

@@ -130,7 +130,8 @@ def test_internal_flux_with_wet_dry_fixups_against_the_oracle(oracle):
         scale = max(1e-300, np.abs(ri).max(), np.abs(re_).max())
         assert np.abs(Fi[k] - ri).max() <= 1e-13 * scale, (k, Fi[k], ri)
         assert np.abs(Fe[k] - re_).max() <= 1e-13 * scale, (k, Fe[k], re_)
-        if not (wet_in[k] and wet_ex[k]) and abs(ri[0]) > 1e-12:
-            kinds.add((int(wet_in[k]), int(wet_ex[k]), ri[0] > 0))
+        F = oracle.llf_flux(g, qi[k], qe[k], bath_in[k], 1.0, nrm[k])  # the flux before any fix-up
+        if not (wet_in[k] and wet_ex[k]) and abs(F[0]) > 1e-12:
+            kinds.add((int(wet_in[k]), int(wet_ex[k]), bool(F[0] > 0)))
     # every branch of the fix-up ran
     assert len(kinds) >= 6, kinds
