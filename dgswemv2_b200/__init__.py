@@ -15,7 +15,7 @@ from .types import MeshArrays, ProblemConfig  # noqa: F401
 __all__ = ["Problem", "ProblemConfig", "MeshArrays", "DgswError", "mesh_topology", "ensemble"]
 
 
-def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True):
+def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True, fp64_limiter=False):
     lib = _lib.load()
     c = _lib.Config()
     lib.dgsw_config_default(C.byref(c))
@@ -47,6 +47,7 @@ def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True):
     c.tile = tile
     c.renumber = int(renumber)
     c.use_graphs = int(use_graphs)
+    c.fp64_limiter = int(fp64_limiter)
     return c
 
 
@@ -142,10 +143,10 @@ class Problem:
     """One RKDG problem on one GPU (SWE::RKDG::Problem + Serial::Simulation, rkdg_swe_problem.hpp:34-194,
     simulation.hpp:14-93)."""
 
-    def __init__(self, cfg, mesh, device=0, tile=0, renumber=True, use_graphs=True, init=True):
+    def __init__(self, cfg, mesh, device=0, tile=0, renumber=True, use_graphs=True, init=True, fp64_limiter=False):
         lib = _lib.load()
         self.cfg = cfg
-        self._c = _make_config(cfg, device, tile, renumber, use_graphs)
+        self._c = _make_config(cfg, device, tile, renumber, use_graphs, fp64_limiter)
         m, self._keep = _mesh_struct(mesh)
         h = C.c_void_p()
         _lib.check(lib.dgsw_rkdg_create(C.byref(self._c), C.byref(m), C.byref(h)))

@@ -63,7 +63,8 @@ class Config(C.Structure):
         ("tile", C.c_int32),
         ("renumber", C.c_int32),
         ("use_graphs", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("fp64_limiter", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 

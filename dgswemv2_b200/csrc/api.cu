@@ -304,17 +304,19 @@ cudaError_t launch_limiter(dgsw_rkdg_s* h, int s_out) {
     L.status = h->status.p;
     L.ref_of_dev = h->ref_of_dev.p;
     L.lgeo = h->lgeo.p;
+    // the FP32 path limits in FP32 arithmetic (FP64 differences, decisions free of rounding noise)
+    const bool f32 = h->fp32 && !h->cfg.fp64_limiter;
     if (h->ind_mode == 1) {
         L.list = h->ind_list.p;
         L.list_count = h->ind_count.p;
         L.counters = h->ind_counters.p;
-        return launch_limiter_kernel<Real>(L, h->cfg.p, h->stream, 8 * h->sm_count);
+        return launch_limiter_kernel<Real>(L, h->cfg.p, h->stream, 8 * h->sm_count, f32);
     }
     if (h->ind_mode == 2) {
         L.gate = h->ind_gate.p;
         L.counters = h->ind_counters.p;
     }
-    return launch_limiter_kernel<Real>(L, h->cfg.p, h->stream);
+    return launch_limiter_kernel<Real>(L, h->cfg.p, h->stream, 0, f32);
 }
 
 template <typename Real>

@@ -4,9 +4,10 @@
 // limiter geometry from problem_preprocessor/swe_pre_init_data.hpp:252-326).
 //
 // One thread per element, after the stage kernel has written the new state, the new wet flags and
-// the barycentre values of every element. The limiter arithmetic runs in FP64 in both precisions:
-// its write-back test compares a relative change against 1e-12. The geometry (centroids, medians,
-// alpha = A^-1 b, r^2) is rebuilt from the FP64 node coordinates instead of being stored.
+// the barycentre values of every element. The FP64 path limits in FP64 (cs_limit_element); the FP32 path
+// in FP32 arithmetic on FP64 differences (cs_limit_element_f32), arranged so that FP32 rounding cannot
+// reach the write-back test, a relative change against 1e-12. The geometry (centroids, medians,
+// alpha = A^-1 b, r^2) is precomputed once per handle from the FP64 node coordinates.
 // The KXRCF trouble indicator the reference evaluates in the same pass (swe_trouble_check.hpp) does
 // not feed the limiter there and is not evaluated here.
 #ifndef DGSW_LIMITER_KERNEL_CUH
@@ -235,10 +236,130 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
     return lim;
 }
 
+// The same limiter with its characteristic arithmetic in FP32, for the FP32 path. Rounding noise must not
+// reach the write-back test (relative change of the vertex values above 1e-12), so the pass works on
+// deviations from the unlimited reconstruction: the differences it transforms (midpoint minus barycentre,
+// neighbour minus own barycentre) are formed in FP64 before rounding to FP32; each characteristic slope's
+// change dch - wt is exactly zero where the minmod keeps wt; the positivity rebalance acts on the sum of
+// those changes (the unlimited deltas sum to zero); and the vertex change R (dch - wt) T, free of rounding
+// where nothing was limited, is compared with 1e-12 of the vertex values. A changed element keeps its FP64
+// mean (mode 0, which the rebalanced deltas leave unchanged) and gets its slope modes as FP64 plus the FP32
+// correction; higher modes are zeroed as ProjectLinearToBasis does.
+template <int ND, typename Real>
+__device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<Real>& L, int e, bool write) {
+    const size_t P = (size_t)L.ne_pad;
+    bool ok = L.wet[e] != 0;
+    int nb[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        nb[f] = L.nbr[f * P + e];
+        if (nb[f] >= 0)
+            ok = ok && (L.wet[nb[f]] != 0);
+        else
+            ok = ok && (-2 - nb[f] >= 0 && -2 - nb[f] <= 3);  // boundary objects: land .. function
+    }
+    if (!ok) return 0;
+    double md[3][3];  // modes 0..2 per variable
+    float du[3][3], dn[3][3], nq[3];  // [bound][var] midpoint - barycentre, [face][var] neighbour - own, |ql|
+    double qb[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const double a = (double)L.q[(v * ND + 0) * P + e], b = (double)L.q[(v * ND + 1) * P + e],
+                     c = (double)L.q[(v * ND + 2) * P + e];
+        md[v][0] = a, md[v][1] = b, md[v][2] = c;
+        const double l0 = a - b - c, l1 = a - b + c, l2 = a + 2.0 * b;
+        qb[v] = L.baryctr[v * P + e];
+        du[0][v] = (float)((l1 * 0.5 + l2 * 0.5) - qb[v]);
+        du[1][v] = (float)((l0 * 0.5 + l2 * 0.5) - qb[v]);
+        du[2][v] = (float)((l0 * 0.5 + l1 * 0.5) - qb[v]);
+        nq[v] = (float)sqrt(l0 * l0 + l1 * l1 + l2 * l2);
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int v = 0; v < 3; ++v) dn[f][v] = nb[f] >= 0 ? (float)(L.baryctr[v * P + nb[f]] - qb[v]) : 0.0f;
+    double G[LIM_GEO];
+    if (L.lgeo) {
+#pragma unroll
+        for (int i = 0; i < LIM_GEO; ++i) G[i] = L.lgeo[i * P + e];
+    } else {
+        limiter_geometry(L, e, nb, G);
+    }
+    const float h = (float)(qb[0] + G[15]);
+    const float ih = 1.0f / h;
+    const float u = (float)qb[1] * ih, vv = (float)qb[2] * ih;
+    const float c = sqrtf((float)L.g * h), i2c = 0.5f / c;
+    const float M = (float)L.M, nu = (float)L.nu;
+    float dd[3][3];  // [bound][var] change of the limited delta from the unlimited one
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const int e1 = b, e2 = (b + 1) % 3;
+        const float al0 = (float)G[5 * b], al1 = (float)G[5 * b + 1], nx = (float)G[5 * b + 2], ny = (float)G[5 * b + 3],
+                    rsq = (float)G[5 * b + 4];
+        const float un = u * nx + vv * ny;
+        const float iR[3][3] = {{(c + un) * i2c, -nx * i2c, -ny * i2c},
+                                {u * ny - vv * nx, -ny, nx},
+                                {(c - un) * i2c, nx * i2c, ny * i2c}};
+        const float R[3][3] = {{1.0f, 0.0f, 1.0f}, {u - c * nx, -ny, u + c * nx}, {vv - c * ny, nx, vv + c * ny}};
+        float ch[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float wt = 0.0f, w1 = 0.0f, w2 = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                wt += iR[i][j] * du[b][j];
+                w1 += iR[i][j] * dn[e1][j];
+                w2 += iR[i][j] * dn[e2][j];
+            }
+            const float wd = al0 * w1 + al1 * w2;
+            float dch;
+            if (fabsf(wt) <= M * rsq)
+                dch = wt;
+            else if (signbit(wt) == signbit(wd))
+                dch = copysignf(1.0f, wt) * fminf(fabsf(wt), fabsf(nu * wd));
+            else
+                dch = 0.0f;
+            ch[i] = dch - wt;
+        }
+#pragma unroll
+        for (int v = 0; v < 3; ++v) dd[b][v] = R[v][0] * ch[0] + R[v][1] * ch[1] + R[v][2] * ch[2];
+    }
+    unsigned char lim = 0;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        // positivity rebalance of the deltas du + dd (the unlimited deltas sum to zero)
+        const float dsum = dd[0][v] + dd[1][v] + dd[2][v];
+        if (dsum != 0.0f) {
+            float d[3], pos = 0.0f, neg = 0.0f;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                d[b] = du[b][v] + dd[b][v];
+                pos += fmaxf(0.0f, d[b]);
+                neg += fmaxf(0.0f, -d[b]);
+            }
+            const float tp = fminf(1.0f, neg / pos), tn = fminf(1.0f, pos / neg);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) dd[b][v] = (tp * fmaxf(0.0f, d[b]) - tn * fmaxf(0.0f, -d[b])) - du[b][v];
+        }
+        // change of the vertex values, (dd T)_k with T = ones - 2 I
+        const float s = dd[0][v] + dd[1][v] + dd[2][v];
+        const float x0 = s - 2.0f * dd[0][v], x1 = s - 2.0f * dd[1][v], x2 = s - 2.0f * dd[2][v];
+        if (sqrtf(x0 * x0 + x1 * x1 + x2 * x2) > 1.0e-12f * nq[v]) {
+            lim = 1;
+            if (!write) continue;
+            L.q[(v * ND + 1) * P + e] = (Real)(md[v][1] + (double)((-x0 - x1 + 2.0f * x2) * (1.0f / 6.0f)));
+            L.q[(v * ND + 2) * P + e] = (Real)(md[v][2] + (double)((-x0 + x1) * 0.5f));
+#pragma unroll
+            for (int k = 3; k < ND; ++k) L.q[(v * ND + k) * P + e] = Real(0);
+        }
+    }
+    return lim;
+}
+
 // One thread per visited element (every element, or the indicator's work list with a grid-stride loop).
 // MB resident 256-thread blocks per SM: 2 (128 registers) or 3 (80 registers and a few hundred bytes of
 // spills); measured on the bowl, 3 is 13 % faster at 524,288 triangles and 2 is faster at 131,072
-template <int ND, typename Real, int MB>
+template <int ND, typename Real, int MB, bool F32 = false>
 __global__ void __launch_bounds__(256, MB) cs_limiter_kernel(const LimiterArgs<Real> L) {
     const int n = L.list ? *L.list_count : L.ne;
     const int stride = gridDim.x * blockDim.x;
@@ -248,7 +369,7 @@ __global__ void __launch_bounds__(256, MB) cs_limiter_kernel(const LimiterArgs<R
         if (i < n) {
             const int e = L.list ? L.list[i] : i;
             const bool write = !L.gate || L.gate[e];
-            const bool lim = cs_limit_element<ND, Real>(L, e, write) != 0;
+            const bool lim = (F32 ? cs_limit_element_f32<ND, Real>(L, e, write) : cs_limit_element<ND, Real>(L, e, write)) != 0;
             applied = lim && write;
             missed = lim && !write;
             L.limited[e] = applied ? 1 : 0;
@@ -263,23 +384,33 @@ __global__ void __launch_bounds__(256, MB) cs_limiter_kernel(const LimiterArgs<R
     }
 }
 
-// grid: one block per 256 elements, or a persistent grid of `list_blocks` blocks over a work list
-template <typename Real>
-cudaError_t launch_limiter_kernel(const LimiterArgs<Real>& L, int p, cudaStream_t s, int list_blocks = 0) {
-    const int blocks = L.list ? list_blocks : (L.ne + 255) / 256;
-    if (blocks <= 0) return cudaSuccess;
+// grid: one block per 256 elements, or a persistent grid of `list_blocks` blocks over a work list;
+// f32: the FP32-arithmetic form (the FP32 path)
+template <typename Real, bool F32>
+void launch_limiter_kernel_t(const LimiterArgs<Real>& L, int p, cudaStream_t s, int blocks) {
     const bool big = L.ne >= (1 << 18);
     if (p == 1) {
         if (big)
-            cs_limiter_kernel<3, Real, 3><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<3, Real, 3, F32><<<blocks, 256, 0, s>>>(L);
         else
-            cs_limiter_kernel<3, Real, 2><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<3, Real, 2, F32><<<blocks, 256, 0, s>>>(L);
     } else {
         if (big)
-            cs_limiter_kernel<6, Real, 3><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<6, Real, 3, F32><<<blocks, 256, 0, s>>>(L);
         else
-            cs_limiter_kernel<6, Real, 2><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<6, Real, 2, F32><<<blocks, 256, 0, s>>>(L);
     }
+}
+
+template <typename Real>
+cudaError_t launch_limiter_kernel(const LimiterArgs<Real>& L, int p, cudaStream_t s, int list_blocks = 0,
+                                  bool f32 = false) {
+    const int blocks = L.list ? list_blocks : (L.ne + 255) / 256;
+    if (blocks <= 0) return cudaSuccess;
+    if (f32)
+        launch_limiter_kernel_t<Real, true>(L, p, s, blocks);
+    else
+        launch_limiter_kernel_t<Real, false>(L, p, s, blocks);
     return cudaGetLastError();
 }
 

@@ -76,7 +76,10 @@ typedef struct {
                                   (dgsw_rkdg_tuning reports the timings) */
     int32_t renumber;          /* 0 keep input order, 1 Morton order of element centroids (default 1) */
     int32_t use_graphs;        /* capture each RK step in a CUDA graph (default 1) */
-    int32_t reserved[8];
+    int32_t fp64_limiter;      /* FP32 precision only: 1 runs the slope limiter's characteristic arithmetic in
+                                  FP64; 0 (default) in FP32 on FP64 differences, with the write-back test
+                                  free of FP32 rounding (limiter_kernel.cuh) */
+    int32_t reserved[7];
 } dgsw_config;
 
 /* One tide or flow block of the `.bcis` file (SWE::Inputs::read_bcis, problem_input/swe_inputs.cpp:211-

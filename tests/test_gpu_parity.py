@@ -104,6 +104,29 @@ def test_fp32_l2_stays_within_5_percent_over_2000_steps():
     assert l2["fp32"] <= 1.05 * l2["fp64"], l2
 
 
+def test_fp32_limiter_against_the_fp64_limiter():
+    """The FP32 path limits in FP32 arithmetic on FP64 differences (limiter_kernel.cuh). On the config-3 bowl
+    (wetting/drying, limiter, p = 1) at 128 x 128 quads for 400 steps, against the same FP32 path with the
+    FP64 limiter: limiter decisions agree on >= 99.5 % of the cells, wet counts within 0.5 %, states
+    within 1e-3 of each variable's scale, mass to 1e-7 relative (the FP32 bulk arithmetic's bound; the
+    limiter keeps each element's FP64 mean), and the L2 error against Thacker's solution within 1.05x of
+    the FP64 path's."""
+    mesh, cfg = configs.config3(nq=128, dt=0.5, precision="fp32")
+    A = Problem(cfg, mesh)
+    B = Problem(cfg, mesh, fp64_limiter=True)
+    m64, c64 = configs.config3(nq=128, dt=0.5)
+    C = Problem(c64, m64)
+    m0 = A.mass()
+    for P in (A, B, C):
+        P.step_serial(400)
+    assert np.mean(A.get_limited() != B.get_limited()) <= 0.005
+    assert A.get_limited().sum() > 100  # the limiter acts
+    assert abs(int(A.get_wet().sum()) - int(B.get_wet().sum())) <= 0.005 * mesh.n_elems
+    assert rel_err(A.get_state(), B.get_state()) <= 1e-3
+    assert abs(A.mass() / m0 - 1) <= 1e-7
+    assert A.compute_residual_L2() <= 1.05 * C.compute_residual_L2()
+
+
 def test_land_boundaries_conserve_mass(oracle):
     """Closed basin with land boundaries: FP64 mass is conserved to rounding."""
     mesh = meshgen.quad_mesh(16, 16, corners=((0, 0), (1000, 0), (1000, 1000), (0, 1000)), bc=(LAND,) * 4,
