@@ -313,6 +313,12 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def autotuned(P):
+    """The autotuner's choice and its timed candidates (tile, occupancy, tile order, ms per step)."""
+    return {"tile": P.info.tile, "occupancy": P.info.occupancy, "tile_order": P.info.tile_order,
+            "candidates": [list(c) for c in P.tuning()]}
+
+
 def time_steps(P, K):
     import torch
 
@@ -388,7 +394,7 @@ def ensemble_workload(dev, steps=20, warmup=3):
     m0 = E.mass()
     return {"workload": "config 5: ensemble of 256 p=1 members (64^2-200^2 quads, %d triangles), wetting/drying, "
                         "FP32 bulk" % E.ne, "steps": steps, "value": E.ne * E.nd * E.cfg.rk_nstages * steps / (ms / 1e3),
-            "ms_per_step": ms / steps, "tile_autotuned": E.info.tile, "tuning": E.tuning(),
+            "ms_per_step": ms / steps, "autotuned": autotuned(E),
             "kernel_launches_per_step": launches / steps, "create_seconds": create_s, "mass": m0}
 
 
@@ -401,7 +407,7 @@ def run_ours(args):
     dev = local
     torch.cuda.set_device(dev)
     mesh, cfg = configs.config2(nq=args.nq, precision=args.precision)
-    # tile size chosen by the library's autotuner (both sizes timed on this workload at create)
+    # tile size, register budget and tile order chosen by the library's autotuner (all timed at create)
     P = Problem(cfg, mesh, device=dev, tile=-1)
     ne, nd, ns = P.ne, P.nd, cfg.rk_nstages
     units_per_step = ne * nd * ns
@@ -432,7 +438,7 @@ def run_ours(args):
         ms64 = dist_max(ms64, world)
         k64, n64 = P64.step_timed(args.steps)
         fp64 = {"value": job_value(units_per_step, args.steps, world, ms64), "ms_per_step": ms64 / args.steps,
-                "tile_autotuned": P64.info.tile, "stage_kernel_ms": dist_max(k64 / max(1, n64), world)}
+                "autotuned": autotuned(P64), "stage_kernel_ms": dist_max(k64 / max(1, n64), world)}
         fp64["stage_kernel_frac_of_hbm"] = (ALG_BYTES_PER_UNIT[("fp64", cfg.p)] * ne * nd /
                                             (fp64["stage_kernel_ms"] / 1e3) / 1e9 / load_peaks()[0])
         fp64["e2e"] = e2e_leg(P64, max(3, min(args.steps, 40)), world)
@@ -460,7 +466,7 @@ def run_ours(args):
                    "l2_cache": "no flush: the per-step working set (%d MB of stage states, bathymetry and mesh "
                                "arrays) exceeds the 126 MB L2" % int(P.info.device_bytes / 2 ** 20)},
         "precision": args.precision, "parallelism": "replicas" if world > 1 else "single GPU",
-        "tile_autotuned": P.info.tile,
+        "autotuned": autotuned(P),
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "e2e": e2e,

@@ -15,7 +15,8 @@ from .types import MeshArrays, ProblemConfig  # noqa: F401
 __all__ = ["Problem", "ProblemConfig", "MeshArrays", "DgswError", "mesh_topology", "ensemble"]
 
 
-def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True, fp64_limiter=False):
+def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True, fp64_limiter=False, occupancy=0,
+                 tile_order=0):
     lib = _lib.load()
     c = _lib.Config()
     lib.dgsw_config_default(C.byref(c))
@@ -48,6 +49,8 @@ def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True, fp64_lim
     c.renumber = int(renumber)
     c.use_graphs = int(use_graphs)
     c.fp64_limiter = int(fp64_limiter)
+    c.occupancy = int(occupancy)
+    c.tile_order = int(tile_order)
     return c
 
 
@@ -108,14 +111,14 @@ def mesh_topology(mesh):
 
 
 def ensemble(cfg, meshes, member_params=None, device=0, tile=_lib.DGSW_TILE_AUTOTUNE, renumber=True,
-             use_graphs=True, init=True):
+             use_graphs=True, init=True, occupancy=0, tile_order=0):
     """Ensemble batching (dgsw_ensemble_create): the members share `cfg` except their function-set
     parameters (member_params: one 16-value list per member, or None for cfg.fn_params). Returns a
     Problem whose state holds the members one after another (Problem.member_range)."""
     lib = _lib.load()
     P = Problem.__new__(Problem)
     P.cfg = cfg
-    P._c = _make_config(cfg, device, tile, renumber, use_graphs)
+    P._c = _make_config(cfg, device, tile, renumber, use_graphs, occupancy=occupancy, tile_order=tile_order)
     arr = (_lib.Mesh * len(meshes))()
     P._keep = []
     for k, m in enumerate(meshes):
@@ -143,10 +146,11 @@ class Problem:
     """One RKDG problem on one GPU (SWE::RKDG::Problem + Serial::Simulation, rkdg_swe_problem.hpp:34-194,
     simulation.hpp:14-93)."""
 
-    def __init__(self, cfg, mesh, device=0, tile=0, renumber=True, use_graphs=True, init=True, fp64_limiter=False):
+    def __init__(self, cfg, mesh, device=0, tile=0, renumber=True, use_graphs=True, init=True, fp64_limiter=False,
+                 occupancy=0, tile_order=0):
         lib = _lib.load()
         self.cfg = cfg
-        self._c = _make_config(cfg, device, tile, renumber, use_graphs, fp64_limiter)
+        self._c = _make_config(cfg, device, tile, renumber, use_graphs, fp64_limiter, occupancy, tile_order)
         m, self._keep = _mesh_struct(mesh)
         h = C.c_void_p()
         _lib.check(lib.dgsw_rkdg_create(C.byref(self._c), C.byref(m), C.byref(h)))
@@ -311,12 +315,13 @@ class Problem:
         return f.value, n.value
 
     def tuning(self):
-        """The autotuner's record: [(tile, device ms per step), ...] (empty if not tuned)."""
-        t = (C.c_int32 * 4)()
-        ms = (C.c_double * 4)()
+        """The autotuner's record: [(tile, occupancy, tile_order, device ms per step), ...] (empty if not tuned)."""
+        cap = 8
+        t, o, r = (C.c_int32 * cap)(), (C.c_int32 * cap)(), (C.c_int32 * cap)()
+        ms = (C.c_double * cap)()
         n = C.c_int32()
-        _lib.check(_lib.load().dgsw_rkdg_tuning(self._h, t, ms, C.byref(n)))
-        return [(t[i], ms[i]) for i in range(n.value)]
+        _lib.check(_lib.load().dgsw_rkdg_tuning(self._h, t, o, r, ms, C.byref(n)))
+        return [(t[i], o[i], r[i], ms[i]) for i in range(n.value)]
 
     def synchronize(self):
         _lib.check(_lib.load().dgsw_rkdg_synchronize(self._h))

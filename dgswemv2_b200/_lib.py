@@ -64,7 +64,9 @@ class Config(C.Structure):
         ("renumber", C.c_int32),
         ("use_graphs", C.c_int32),
         ("fp64_limiter", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("occupancy", C.c_int32),
+        ("tile_order", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -159,6 +161,8 @@ class Info(C.Structure):
         ("tile", C.c_int32),
         ("device_bytes", C.c_int64),
         ("state_bytes", C.c_int64),
+        ("occupancy", C.c_int32),
+        ("tile_order", C.c_int32),
     ]
 
 
@@ -173,7 +177,8 @@ SIGNATURES = {
     "dgsw_ensemble_create": (C.c_int32, [C.POINTER(Config), C.c_int32, C.POINTER(Mesh), C.POINTER(C.c_double),
                                          C.POINTER(C.c_void_p)]),
     "dgsw_ensemble_member_range": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
-    "dgsw_rkdg_tuning": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "dgsw_rkdg_tuning": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "dgsw_rkdg_info": (C.c_int32, [C.c_void_p, C.POINTER(Info)]),
     "dgsw_rkdg_init_state": (C.c_int32, [C.c_void_p]),
     "dgsw_rkdg_set_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),

@@ -165,8 +165,12 @@ struct dgsw_rkdg_s {
     std::vector<int64_t> member_first;
     // autotuner record: candidate tile sizes and their measured device time per step
     int32_t n_tuned = 0;
-    int32_t tuned_tile[4] = {0, 0, 0, 0};
-    double tuned_ms[4] = {0, 0, 0, 0};
+    int32_t tuned_tile[DGSW_TUNE_MAX_CANDIDATES] = {0};
+    int32_t tuned_occ[DGSW_TUNE_MAX_CANDIDATES] = {0};
+    int32_t tuned_order[DGSW_TUNE_MAX_CANDIDATES] = {0};
+    double tuned_ms[DGSW_TUNE_MAX_CANDIDATES] = {0};
+    // stage-kernel register budget (0 default, 1 the alternative) and tile order (0 alternating, 1 ascending)
+    int occ = 0, order = 0;
     // troubled-cell indicator (mode 0 off, 1 gate the limiter, 2 shadow: plain limiter, misses counted)
     int ind_mode = 0;
     float ind_skip_below = 0.1f;
@@ -243,16 +247,22 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.went_dry = h->went_dry.p;
     // tile order alternates from stage to stage, across steps too (qswap flips once per step and keys
     // the step graphs), so that each stage starts where the previous one ended
-    A.reverse = (s + h->qswap * h->ns) & 1;
+    A.reverse = h->order == 0 ? ((s + h->qswap * h->ns) & 1) : 0;
 }
 
 cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, int mode) {
     const int nt = (int)h->tiling.ntiles, mh = h->tiling.max_halo, me = h->tiling.max_edges;
+    if (h->occ)
+        return h->cfg.p == 1 ? launch_stage_p1_f64_occ(A, h->tile, nt, mh, me, mode, h->stream)
+                             : launch_stage_p2_f64_occ(A, h->tile, nt, mh, me, mode, h->stream);
     return h->cfg.p == 1 ? launch_stage_p1_f64(A, h->tile, nt, mh, me, mode, h->stream)
                          : launch_stage_p2_f64(A, h->tile, nt, mh, me, mode, h->stream);
 }
 cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<float>& A, int mode) {
     const int nt = (int)h->tiling.ntiles, mh = h->tiling.max_halo, me = h->tiling.max_edges;
+    if (h->occ)
+        return h->cfg.p == 1 ? launch_stage_p1_f32_occ(A, h->tile, nt, mh, me, mode, h->stream)
+                             : launch_stage_p2_f32_occ(A, h->tile, nt, mh, me, mode, h->stream);
     return h->cfg.p == 1 ? launch_stage_p1_f32(A, h->tile, nt, mh, me, mode, h->stream)
                          : launch_stage_p2_f32(A, h->tile, nt, mh, me, mode, h->stream);
 }
@@ -681,6 +691,12 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         return fail(DGSW_ERR_INVALID_ARGUMENT, "tile must be 0 (automatic), 128 or 256");
     }
     h->tile = tile;
+    if ((cfg->occupancy != 0 && cfg->occupancy != 1) || (cfg->tile_order != 0 && cfg->tile_order != 1)) {
+        delete h;
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "occupancy and tile_order must be 0 or 1");
+    }
+    h->occ = cfg->occupancy;
+    h->order = cfg->tile_order;
     rc = build_tiling(h->topo, h->node_xyz.data(), tile, cfg->renumber != 0, h->tiling, err);
     if (rc) {
         delete h;
@@ -905,24 +921,40 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
 // describe the problem the timing runs on (a subset of an ensemble's members, or the problem itself);
 // the winner is then built for the full problem unless the tuning problem is the full problem.
 // Decisions are cached per (elements, order, precision, stages, options, device) for the process.
+// an autotuner candidate and its device time per step; the decisions are cached per problem shape
+struct TuneRecord {
+    int tile, occ, order;
+    double ms;
+};
 static std::mutex g_tune_mutex;
-static std::map<std::string, int> g_tune_cache;
+static std::map<std::string, TuneRecord> g_tune_cache;
 
-static int32_t time_candidate(const dgsw_config* cfg, const dgsw_mesh* mesh, const int32_t* group, int32_t ng,
-                              const double* gp, int tile, double* ms, dgsw_handle* keep) {
+// One tile size of the autotuner: a handle built with that tile, then each (occupancy, tile order) pair
+// timed on it, 4 graph-replayed steps after 2 warm-up steps, from the initial state each time. Returns
+// the handle (in *keep, left at the last variant) or destroys it.
+
+static int32_t time_tile(const dgsw_config* cfg, const dgsw_mesh* mesh, const int32_t* group, int32_t ng,
+                         const double* gp, int tile, std::vector<TuneRecord>& rec, dgsw_handle* keep) {
     dgsw_config c = *cfg;
     c.tile = tile;
     dgsw_handle h = nullptr;
     int32_t rc = create_impl(&c, mesh, group, ng, gp, &h);
     if (rc) return rc;
     const int warm = 2, timed = 4;
-    if ((rc = dgsw_rkdg_init_state(h)) || (rc = dgsw_rkdg_step(h, warm)) || (rc = dgsw_rkdg_step(h, timed))) {
-        dgsw_rkdg_destroy(h);
-        return rc;
-    }
-    int64_t nl = 0;
-    dgsw_rkdg_last_step_timing(h, ms, &nl);
-    *ms /= timed;
+    for (int occ = 0; occ < 2; ++occ)
+        for (int order = 0; order < 2; ++order) {
+            destroy_graphs(h);  // the step graphs hold the kernel and its arguments
+            h->occ = occ;
+            h->order = order;
+            if ((rc = dgsw_rkdg_init_state(h)) || (rc = dgsw_rkdg_step(h, warm)) || (rc = dgsw_rkdg_step(h, timed))) {
+                dgsw_rkdg_destroy(h);
+                return rc;
+            }
+            double ms = 0;
+            int64_t nl = 0;
+            dgsw_rkdg_last_step_timing(h, &ms, &nl);
+            rec.push_back({tile, occ, order, ms / timed});
+        }
     if (keep) {
         *keep = h;
     } else {
@@ -935,64 +967,67 @@ static int32_t create_tuned(const dgsw_config* cfg, const dgsw_mesh* mesh, const
                             const double* gp, const dgsw_mesh* tune_mesh, const int32_t* tune_group, int32_t tune_ng,
                             const double* tune_gp, dgsw_handle* out) {
     const bool same = tune_mesh == mesh;
-    const int cands[2] = {128, 256};
+    const int tiles[2] = {128, 256};
     cudaDeviceProp prop;
     std::memset(&prop, 0, sizeof(prop));
     cudaGetDeviceProperties(&prop, cfg->device);
     char key[512];
-    std::snprintf(key, sizeof(key), "%lld/%lld/%d/%d/%d/%d/%d/%d/%d/%s", (long long)mesh->n_elems,
+    std::snprintf(key, sizeof(key), "%lld/%lld/%d/%d/%d/%d/%d/%d/%d/%d/%d/%s", (long long)mesh->n_elems,
                   (long long)tune_mesh->n_elems, cfg->p, cfg->precision, cfg->rk_nstages, cfg->wetting_drying,
-                  cfg->slope_limiting, cfg->function_source, ng, prop.name);
-    int chosen = 0;
+                  cfg->slope_limiting, cfg->function_source, cfg->bottom_friction, cfg->fp64_limiter, ng, prop.name);
+    TuneRecord chosen = {0, 0, 0, 0.0};
     {
         std::lock_guard<std::mutex> lk(g_tune_mutex);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) chosen = it->second;
     }
-    double ms[2] = {0, 0};
-    dgsw_handle best = nullptr;
-    int ntimed = 0;
-    if (!chosen) {
-        double best_ms = 1e300;
+    std::vector<TuneRecord> rec;
+    dgsw_handle kept[2] = {nullptr, nullptr};
+    if (!chosen.tile) {
         for (int i = 0; i < 2; ++i) {
-            dgsw_handle h = nullptr;
-            int32_t rc = time_candidate(cfg, tune_mesh, tune_group, tune_ng, tune_gp, cands[i], &ms[i],
-                                        same ? &h : nullptr);
+            int32_t rc = time_tile(cfg, tune_mesh, tune_group, tune_ng, tune_gp, tiles[i], rec, same ? &kept[i] : nullptr);
             if (rc) {
-                if (best) dgsw_rkdg_destroy(best);
+                for (dgsw_handle k : kept)
+                    if (k) dgsw_rkdg_destroy(k);
                 return rc;
             }
-            ++ntimed;
-            if (ms[i] < best_ms) {
-                best_ms = ms[i];
-                chosen = cands[i];
-                if (same) {
-                    if (best) dgsw_rkdg_destroy(best);
-                    best = h;
-                }
-            } else if (same) {
-                dgsw_rkdg_destroy(h);
-            }
         }
+        chosen = rec[0];
+        for (const TuneRecord& r : rec)
+            if (r.ms < chosen.ms) chosen = r;
         std::lock_guard<std::mutex> lk(g_tune_mutex);
         g_tune_cache[key] = chosen;
     }
+    dgsw_handle best = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        if (kept[i] && tiles[i] == chosen.tile)
+            best = kept[i];
+        else if (kept[i])
+            dgsw_rkdg_destroy(kept[i]);
+    }
     if (!best) {
         dgsw_config c = *cfg;
-        c.tile = chosen;
+        c.tile = chosen.tile;
+        c.occupancy = chosen.occ;
+        c.tile_order = chosen.order;
         int32_t rc = create_impl(&c, mesh, group, ng, gp, &best);
         if (rc) return rc;
     } else {
+        destroy_graphs(best);
+        best->occ = chosen.occ;
+        best->order = chosen.order;
         int32_t rc = dgsw_rkdg_init_state(best);  // back to t = 0 after the timing steps
         if (rc) {
             dgsw_rkdg_destroy(best);
             return rc;
         }
     }
-    best->n_tuned = ntimed;
-    for (int i = 0; i < ntimed; ++i) {
-        best->tuned_tile[i] = cands[i];
-        best->tuned_ms[i] = ms[i];
+    best->n_tuned = (int32_t)std::min<size_t>(rec.size(), DGSW_TUNE_MAX_CANDIDATES);
+    for (int i = 0; i < best->n_tuned; ++i) {
+        best->tuned_tile[i] = rec[i].tile;
+        best->tuned_occ[i] = rec[i].occ;
+        best->tuned_order[i] = rec[i].order;
+        best->tuned_ms[i] = rec[i].ms;
     }
     *out = best;
     return DGSW_OK;
@@ -1173,11 +1208,14 @@ int32_t dgsw_ensemble_member_range(dgsw_handle h, int32_t member, int64_t* first
     return DGSW_OK;
 }
 
-int32_t dgsw_rkdg_tuning(dgsw_handle h, int32_t* tiles, double* ms_per_step, int32_t* n) {
+int32_t dgsw_rkdg_tuning(dgsw_handle h, int32_t* tiles, int32_t* occupancy, int32_t* tile_order, double* ms_per_step,
+                         int32_t* n) {
     if (!h || !n) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     *n = h->n_tuned;
     for (int i = 0; i < h->n_tuned; ++i) {
         if (tiles) tiles[i] = h->tuned_tile[i];
+        if (occupancy) occupancy[i] = h->tuned_occ[i];
+        if (tile_order) tile_order[i] = h->tuned_order[i];
         if (ms_per_step) ms_per_step[i] = h->tuned_ms[i];
     }
     return DGSW_OK;
@@ -1261,6 +1299,8 @@ int32_t dgsw_rkdg_info(dgsw_handle h, dgsw_info* o) {
     o->tile = h->tile;
     o->device_bytes = h->device_bytes;
     o->state_bytes = (int64_t)3 * h->nd * h->ne_pad * (int64_t)sizeof(double);
+    o->occupancy = h->occ;
+    o->tile_order = h->order;
     return DGSW_OK;
 }
 

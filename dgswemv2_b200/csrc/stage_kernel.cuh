@@ -556,11 +556,14 @@ __device__ __forceinline__ void cp_async_commit_and_wait() {
 #ifndef DGSW_F64_P1_WD_MB128
 #define DGSW_F64_P1_WD_MB128 3
 #endif
-template <int P, typename Real, int TILE, bool WD>
+// OCC = 1 selects the autotuner's alternative budget: one resident CTA fewer where the default holds
+// several (more registers per thread), one more where it holds one (tile 256 in FP64)
+template <int P, typename Real, int TILE, bool WD, int OCC = 0>
 struct MinBlocks {
     static constexpr int f32 = P == 1 ? DGSW_F32_P1_MB128 : DGSW_F32_MB128;
     static constexpr int f64 = P == 1 ? (WD ? DGSW_F64_P1_WD_MB128 : DGSW_F64_P1_MB128) : DGSW_F64_MB128;
-    static constexpr int value = sizeof(Real) == 4 ? (TILE == 128 ? f32 : 2) : (TILE == 128 ? f64 : 1);
+    static constexpr int base = sizeof(Real) == 4 ? (TILE == 128 ? f32 : 2) : (TILE == 128 ? f64 : 1);
+    static constexpr int value = OCC == 0 ? base : (base > 1 ? base - 1 : base + 1);
 };
 
 // shared-memory capacities a tile almost always fits (measured: about 0.27 TILE halo faces and 1.65 TILE
@@ -572,8 +575,8 @@ struct TileCap {
     static constexpr int edges = TILE + TILE / 2 + TILE / 4 + 16;  // 240 for 128, 464 for 256
 };
 
-template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, bool CAPPED>
-__global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD>::value))
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, bool CAPPED, int OCC = 0>
+__global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::value))
     rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_halo_rt, int max_edges_rt) {
     const int max_halo = CAPPED ? TileCap<TILE>::halo : max_halo_rt;
     const int max_edges = CAPPED ? TileCap<TILE>::edges : max_edges_rt;
@@ -1129,7 +1132,9 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD>::value))
     }
 }
 
-// launchers, one translation unit per (order, precision)
+// launchers, one translation unit per (order, precision, register budget); bit 3 of `mode` selects the
+// alternative budget (OCC = 1)
+constexpr int STAGE_MODE_OCC = 8;
 cudaError_t launch_stage_p1_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
                                 int mode, cudaStream_t s);
 cudaError_t launch_stage_p1_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
@@ -1138,12 +1143,20 @@ cudaError_t launch_stage_p2_f64(const StageArgs<double>& A, int tile, int ntiles
                                 int mode, cudaStream_t s);
 cudaError_t launch_stage_p2_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
                                 int mode, cudaStream_t s);
+cudaError_t launch_stage_p1_f64_occ(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                    int mode, cudaStream_t s);
+cudaError_t launch_stage_p1_f32_occ(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                    int mode, cudaStream_t s);
+cudaError_t launch_stage_p2_f64_occ(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                    int mode, cudaStream_t s);
+cudaError_t launch_stage_p2_f32_occ(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                    int mode, cudaStream_t s);
 
-template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE>
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, int OCC>
 cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo, int max_edges, cudaStream_t s) {
     const bool capped = max_halo <= TileCap<TILE>::halo && max_edges <= TileCap<TILE>::edges;
-    auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, true>
-                       : rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, false>;
+    auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, true, OCC>
+                       : rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, false, OCC>;
     const size_t smem = capped ? Smem<P, Real, WD>::bytes(TILE, TileCap<TILE>::halo, TileCap<TILE>::edges)
                                : Smem<P, Real, WD>::bytes(TILE, max_halo, max_edges);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1152,32 +1165,32 @@ cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo
     return cudaGetLastError();
 }
 
-template <int P, typename Real, bool WD, bool FSRC, bool FRIC>
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int OCC>
 cudaError_t launch_stage_tile(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges,
                               cudaStream_t s) {
     switch (tile) {
         case 128:
-            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 128>(A, ntiles, max_halo, max_edges, s);
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 128, OCC>(A, ntiles, max_halo, max_edges, s);
         case 256:
-            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 256>(A, ntiles, max_halo, max_edges, s);
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 256, OCC>(A, ntiles, max_halo, max_edges, s);
         default:
             return cudaErrorInvalidValue;
     }
 }
 
 // wetting/drying, function source and bottom friction select the instantiation (bit 0, 1, 2 of `mode`)
-template <int P, typename Real>
+template <int P, typename Real, int OCC>
 cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges,
                                   int mode, cudaStream_t s) {
     switch (mode & 7) {
-        case 0: return launch_stage_tile<P, Real, false, false, false>(A, tile, ntiles, max_halo, max_edges, s);
-        case 1: return launch_stage_tile<P, Real, true, false, false>(A, tile, ntiles, max_halo, max_edges, s);
-        case 2: return launch_stage_tile<P, Real, false, true, false>(A, tile, ntiles, max_halo, max_edges, s);
-        case 3: return launch_stage_tile<P, Real, true, true, false>(A, tile, ntiles, max_halo, max_edges, s);
-        case 4: return launch_stage_tile<P, Real, false, false, true>(A, tile, ntiles, max_halo, max_edges, s);
-        case 5: return launch_stage_tile<P, Real, true, false, true>(A, tile, ntiles, max_halo, max_edges, s);
-        case 6: return launch_stage_tile<P, Real, false, true, true>(A, tile, ntiles, max_halo, max_edges, s);
-        default: return launch_stage_tile<P, Real, true, true, true>(A, tile, ntiles, max_halo, max_edges, s);
+        case 0: return launch_stage_tile<P, Real, false, false, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        case 1: return launch_stage_tile<P, Real, true, false, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        case 2: return launch_stage_tile<P, Real, false, true, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        case 3: return launch_stage_tile<P, Real, true, true, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        case 4: return launch_stage_tile<P, Real, false, false, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        case 5: return launch_stage_tile<P, Real, true, false, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        case 6: return launch_stage_tile<P, Real, false, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        default: return launch_stage_tile<P, Real, true, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
     }
 }
 

@@ -1,0 +1,10 @@
+// Stage-kernel instantiations for polynomial order 1, FP64 arithmetic, the autotuner's alternative register
+// budget (compiled as a separate unit).
+#include "stage_kernel.cuh"
+
+namespace dgsw {
+cudaError_t launch_stage_p1_f64_occ(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                    int mode, cudaStream_t s) {
+    return launch_stage_dispatch<1, double, 1>(A, tile, ntiles, max_halo, max_edges, mode, s);
+}
+}  // namespace dgsw

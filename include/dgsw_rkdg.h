@@ -72,14 +72,19 @@ typedef struct {
                                   integrals) with FP64 stage states, wet/dry tests, limiter and reductions */
     int32_t device;            /* CUDA device ordinal */
     int32_t tile;              /* elements per stage-kernel tile: 128 or 256; 0 = 128; DGSW_TILE_AUTOTUNE =
-                                  measure both on the device at create and keep the faster
-                                  (dgsw_rkdg_tuning reports the timings) */
+                                  time every (tile, occupancy, tile_order) candidate on the device at create
+                                  and keep the fastest (dgsw_rkdg_tuning reports the timings) */
     int32_t renumber;          /* 0 keep input order, 1 Morton order of element centroids (default 1) */
     int32_t use_graphs;        /* capture each RK step in a CUDA graph (default 1) */
     int32_t fp64_limiter;      /* FP32 precision only: 1 runs the slope limiter's characteristic arithmetic in
                                   FP64; 0 (default) in FP32 on FP64 differences, with the write-back test
                                   free of FP32 rounding (limiter_kernel.cuh) */
-    int32_t reserved[7];
+    int32_t occupancy;         /* stage-kernel register budget: 0 the default resident CTAs per SM, 1 the
+                                  alternative (one CTA fewer, or one more where the default is one); set by
+                                  the autotuner when tile = DGSW_TILE_AUTOTUNE */
+    int32_t tile_order;        /* 0 alternate the tile order from stage to stage (each stage starts where
+                                  the previous one ended), 1 always ascending; set by the autotuner too */
+    int32_t reserved[5];
 } dgsw_config;
 
 /* One tide or flow block of the `.bcis` file (SWE::Inputs::read_bcis, problem_input/swe_inputs.cpp:211-
@@ -132,6 +137,7 @@ typedef struct {
     int32_t p, ndof, ngp_volume, ngp_edge, nstages, precision, tile;
     int64_t device_bytes;      /* bytes of device memory held by the handle */
     int64_t state_bytes;       /* bytes of one stage state array */
+    int32_t occupancy, tile_order;  /* the stage kernel's register budget and tile order in use */
 } dgsw_info;
 
 typedef struct dgsw_rkdg_s* dgsw_handle;
@@ -162,9 +168,12 @@ int32_t dgsw_ensemble_create(const dgsw_config* cfg, int32_t n_members, const dg
                              const double* member_params, dgsw_handle* out);
 /* element range of one member in the handle's state order (a single problem is member 0) */
 int32_t dgsw_ensemble_member_range(dgsw_handle h, int32_t member, int64_t* first, int64_t* n_elems);
-/* the autotuner's record: candidate tile sizes and device milliseconds per step (n = 0 when the handle
- * was not tuned, or reused a cached decision); arrays of 4 */
-int32_t dgsw_rkdg_tuning(dgsw_handle h, int32_t* tiles, double* ms_per_step, int32_t* n);
+/* the autotuner's record, one entry per timed candidate: tile size, occupancy, tile order and device
+ * milliseconds per step (*n = 0 when the handle was not tuned, or reused a cached decision). Pass NULL
+ * arrays to query *n; otherwise the arrays hold at least DGSW_TUNE_MAX_CANDIDATES entries. */
+#define DGSW_TUNE_MAX_CANDIDATES 8
+int32_t dgsw_rkdg_tuning(dgsw_handle h, int32_t* tiles, int32_t* occupancy, int32_t* tile_order, double* ms_per_step,
+                         int32_t* n);
 int32_t dgsw_rkdg_info(dgsw_handle h, dgsw_info* out);
 
 /* Problem::preprocessor_serial -> initialize_data_serial (swe_pre_init_data.hpp:9-327): bathymetry and

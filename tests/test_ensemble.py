@@ -36,15 +36,19 @@ def test_members_match_individual_runs_fp64():
     assert E.member_range(4)[0] + E.member_range(4)[1] == E.ne
 
 
-def test_autotuner_times_both_tiles_and_keeps_the_faster():
+def test_autotuner_times_every_candidate_and_keeps_the_fastest():
+    """Tile size x register budget x tile order: eight candidates timed, the fastest kept."""
     meshes, cfgs = configs.config5(n_members=6, seed=1, nmin=32, nmax=64, precision="fp32")
     E = ensemble(cfgs[0], meshes, [c.fn_params for c in cfgs])  # tile = DGSW_TILE_AUTOTUNE
     rec = E.tuning()
-    assert sorted(t for t, _ in rec) == [128, 256] and all(ms > 0 for _, ms in rec)
-    assert E.info.tile == min(rec, key=lambda r: r[1])[0]
+    assert len(rec) == 8 and all(r[3] > 0 for r in rec)
+    assert {(t, o, r) for t, o, r, _ in rec} == {(t, o, r) for t in (128, 256) for o in (0, 1) for r in (0, 1)}
+    best = min(rec, key=lambda r: r[3])
+    assert (E.info.tile, E.info.occupancy, E.info.tile_order) == best[:3]
     # the tuned handle starts from t = 0 like an untuned one
     assert E.time()[1] == 0
-    F = ensemble(cfgs[0], meshes, [c.fn_params for c in cfgs], tile=E.info.tile)
+    F = ensemble(cfgs[0], meshes, [c.fn_params for c in cfgs], tile=E.info.tile, occupancy=E.info.occupancy,
+                 tile_order=E.info.tile_order)
     E.step_serial(20)
     F.step_serial(20)
     assert np.array_equal(E.get_state(), F.get_state())
