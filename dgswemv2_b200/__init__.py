@@ -254,6 +254,10 @@ class Problem:
         assert prm.size == _lib.DGSW_MLP_NPARAM
         _lib.check(_lib.load().dgsw_rkdg_set_indicator(self._h, _lib.ptr(prm, C.c_float), float(confidence), int(mode)))
 
+    def set_indicator_features(self, feature_set):
+        """0: the characteristic feature set (default); 1: raw modal coefficients and neighbour means."""
+        _lib.check(_lib.load().dgsw_rkdg_set_indicator_features(self._h, int(feature_set)))
+
     def indicator_stats(self, reset=False):
         """(considered, sent to the limiter, limited, missed) cell counts since the last reset."""
         c = (C.c_int64 * 4)()

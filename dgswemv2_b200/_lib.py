@@ -209,6 +209,7 @@ SIGNATURES = {
     "dgsw_rkdg_stage_record": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "dgsw_rkdg_set_indicator": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.c_double, C.c_int32]),
     "dgsw_rkdg_indicator_stats": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64), C.c_int32]),
+    "dgsw_rkdg_set_indicator_features": (C.c_int32, [C.c_void_p, C.c_int32]),
     "dgsw_mlp_forward": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "dgsw_mlp_grad_work_floats": (C.c_int64, [C.c_int64]),
     "dgsw_mlp_grad": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,

@@ -173,6 +173,7 @@ struct dgsw_rkdg_s {
     int occ = 0, order = 0;
     // troubled-cell indicator (mode 0 off, 1 gate the limiter, 2 shadow: plain limiter, misses counted)
     int ind_mode = 0;
+    int ind_fset = 0;  // indicator feature set (IND_FEATURES_*)
     float ind_skip_below = 0.1f;
     DBuf<float> ind_params;
     DBuf<int> ind_list;
@@ -343,6 +344,7 @@ FeatureArgs<Real> feature_args(dgsw_rkdg_s* h, int s_out) {
     F.nd = h->nd;
     F.g = h->cfg.g;
     F.M = h->cfg.sl_M;
+    F.fset = h->ind_fset;
     return F;
 }
 
@@ -1469,6 +1471,15 @@ int32_t dgsw_rkdg_set_indicator(dgsw_handle h, const float* params, double confi
     if (h->ind_mode != mode) destroy_graphs(h);
     h->ind_mode = mode;
     h->ind_skip_below = (float)(1.0 - confidence);
+    return DGSW_OK;
+}
+
+int32_t dgsw_rkdg_set_indicator_features(dgsw_handle h, int32_t feature_set) {
+    if (!h) return fail(DGSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (feature_set != IND_FEATURES_CHARACTERISTIC && feature_set != IND_FEATURES_RAW)
+        return fail(DGSW_ERR_INVALID_ARGUMENT, "feature set must be 0 (characteristic) or 1 (raw)");
+    h->ind_fset = feature_set;
+    destroy_graphs(h);  // a gated step graph holds the feature arguments
     return DGSW_OK;
 }
 

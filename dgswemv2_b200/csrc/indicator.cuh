@@ -49,12 +49,18 @@ struct FeatureArgs {
     const double* nz;          // node depths
     int ne, ne_pad, nd;
     double g, M;               // gravity, TVB constant of the limiter
+    int fset;                  // feature set: 0 characteristic (below), 1 the raw modal coefficients and
+                               // neighbour cell means
 };
 
-// The 18 features of element e (definition in oracle/mlp_oracle.py: fields in characteristic units,
-// one common scale, TVB ratio, Froude numbers) and whether the limiter looks at the cell (it and its
-// neighbours wet, boundary faces land or function). FP64 arithmetic with explicit roundings (no
-// contraction), so the host oracle reproduces the values bit for bit.
+constexpr int IND_FEATURES_CHARACTERISTIC = 0, IND_FEATURES_RAW = 1;
+
+// The 18 features of element e and whether the limiter looks at the cell (it and its neighbours wet,
+// boundary faces land or function). Feature set 0 (definition in oracle/mlp_oracle.py): fields in
+// characteristic units, one common scale, TVB ratio, Froude numbers. Feature set 1, the literal input list
+// of the learned-indicator workload: the p = 1 modal coefficients of ze, qx, qy (3 x 3) and the cell means
+// of the three neighbours of each field (9; a boundary face repeats the cell's own mean). FP64 arithmetic
+// with explicit roundings (no contraction), so the host oracle reproduces the values bit for bit.
 template <typename Real>
 __device__ __forceinline__ bool element_features(const FeatureArgs<Real>& F, int e, float* out) {
     const size_t P = (size_t)F.ne_pad;
@@ -74,13 +80,30 @@ __device__ __forceinline__ bool element_features(const FeatureArgs<Real>& F, int
             ok = ok && (F.wet[m] != 0);
 #pragma unroll
             for (int v = 0; v < 3; ++v) d[f][v] = __dsub_rn((double)F.q[(size_t)(v * ND) * P + m], a[v]);
+            if (F.fset == IND_FEATURES_RAW) {
+#pragma unroll
+                for (int v = 0; v < 3; ++v) out[9 + 3 * f + v] = __double2float_rn((double)F.q[(size_t)(v * ND) * P + m]);
+            }
         } else {
             const int bt = -2 - m;
             // land, tide, flow and function boundaries: wet_neigh is the element's own flag
             ok = ok && (bt >= 0 && bt <= 3);
 #pragma unroll
             for (int v = 0; v < 3; ++v) d[f][v] = 0.0;
+            if (F.fset == IND_FEATURES_RAW) {
+#pragma unroll
+                for (int v = 0; v < 3; ++v) out[9 + 3 * f + v] = __double2float_rn(a[v]);
+            }
         }
+    }
+    if (F.fset == IND_FEATURES_RAW) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            out[3 * v] = __double2float_rn(a[v]);
+            out[3 * v + 1] = __double2float_rn(b[v]);
+            out[3 * v + 2] = __double2float_rn(c[v]);
+        }
+        return ok;
     }
     const int n[3] = {F.enodes[e], F.enodes[P + e], F.enodes[2 * P + e]};
     const double third = 1.0 / 3.0;

@@ -8,7 +8,7 @@ config-3-style bowls with seeded Gaussian humps; training runs the library's FP3
 kernels (dgsw_mlp_grad, dgsw_mlp_adam); inference inside the step runs on the tensor cores. torch is
 used only to hold device buffers and to shuffle/gather minibatches.
 
-    python -m dgswemv2_b200.indicator train --out weights.f32      # data + training on cuda:0
+    python -m dgswemv2_b200.indicator train --compare-raw --report record.json   # data + training on cuda:0
 """
 import argparse
 import ctypes as C
@@ -104,27 +104,62 @@ class Trainer:
         return self.P.cpu().numpy().copy()
 
 
-def record(nq=256, seeds=range(8), steps=400, every=4, keep=0.035, dt=0.25, precision="fp32", seed=0):
+def record(nq=256, seeds=range(8), steps=400, every=4, keep=0.035, dt=0.25, precision="fp32", seed=0,
+           feature_sets=(0,)):
     """Features and labels of the cells the limiter looks at, from bowl runs with random Gaussian humps:
-    every `every`-th stage of `steps` SSP-RK2 steps, a random `keep` fraction of those cells."""
+    every `every`-th stage of `steps` SSP-RK2 steps, a random `keep` fraction of those cells. With several
+    feature sets, one run per set steps in lockstep (the runs are deterministic: identical states and
+    labels) and each gives its features for the same cells. Returns ([X per feature set], y)."""
     torch = _torch()
     g = torch.Generator(device="cuda")
     g.manual_seed(seed)
-    Xs, ys = [], []
+    Xs, ys = [[] for _ in feature_sets], []
     for sd in seeds:
         mesh, cfg = configs.bowl_humps(nq=nq, seed=int(sd), dt=dt, precision=precision)
-        P = Problem(cfg, mesh)
-        feat = torch.empty((P.ne, N_FEAT), dtype=torch.float32, device="cuda")
-        lab = torch.empty(P.ne, dtype=torch.uint8, device="cuda")
+        runs = []
+        for fs in feature_sets:
+            P = Problem(cfg, mesh)
+            P.set_indicator_features(fs)
+            runs.append((P, torch.empty((P.ne, N_FEAT), dtype=torch.float32, device="cuda"),
+                         torch.empty(P.ne, dtype=torch.uint8, device="cuda")))
+        ne = runs[0][0].ne
         for st in range(steps * cfg.rk_nstages):
-            P.stage_record(feat.data_ptr(), lab.data_ptr())
+            for P, feat, lab in runs:
+                P.stage_record(feat.data_ptr(), lab.data_ptr())
             if st % every:
                 continue
-            sel = (lab != 255) & (torch.rand(P.ne, generator=g, device="cuda") < keep)
-            Xs.append(feat[sel].clone())
+            lab = runs[0][2]
+            for _, _, other in runs[1:]:
+                assert torch.equal(other, lab), "lockstep runs diverged"
+            sel = (lab != 255) & (torch.rand(ne, generator=g, device="cuda") < keep)
+            for i, (_, feat, _) in enumerate(runs):
+                Xs[i].append(feat[sel].clone())
             ys.append(lab[sel].clone())
-        P.close()
-    return torch.cat(Xs), torch.cat(ys)
+        for P, _, _ in runs:
+            P.close()
+    return [torch.cat(x) for x in Xs], torch.cat(ys)
+
+
+def normalisation(X):
+    """Per-feature mean and standard deviation of a training set (FP64 sums; 1 for a constant feature)."""
+    torch = _torch()
+    Xd = X.double()
+    mu, sd = Xd.mean(0), Xd.std(0)
+    sd = torch.where(sd > 0, sd, torch.ones_like(sd))
+    return mu.float(), sd.float()
+
+
+def fold_normalisation(params, mu, sd):
+    """A network trained on (x - mu) / sd as a network on x: W1' = W1 / sd, b1' = b1 - W1' mu."""
+    P = np.asarray(params, np.float64).copy()
+    W1 = P[:N_H * N_FEAT].reshape(N_H, N_FEAT)
+    b1 = P[N_H * N_FEAT:N_H * N_FEAT + N_H]
+    mu = np.asarray(mu, np.float64)
+    sd = np.asarray(sd, np.float64)
+    W1n = W1 / sd[None, :]
+    P[:N_H * N_FEAT] = W1n.ravel()
+    P[N_H * N_FEAT:N_H * N_FEAT + N_H] = b1 - W1n @ mu
+    return P.astype(np.float32)
 
 
 def metrics(p, y, confidence=0.9):
@@ -170,7 +205,7 @@ def train(X, y, Xv=None, yv=None, epochs=8, batch=8192, lr=2e-3, seed=0, log=pri
     return T.params(), {"pos_weight": pos_weight, "history": hist, "train_cells": n}
 
 
-def evaluate(params, nq=1024, steps=200, dt=0.06, confidence=0.9, precision="fp32", warmup=3):
+def evaluate(params, nq=1024, steps=200, dt=0.06, confidence=0.9, precision="fp32", warmup=3, feature_set=0):
     """Config-4 inference: Thacker bowl on nq x nq quads (2 nq^2 triangles), p = 1, SSP-RK2, wetting and
     drying. Runs the same `steps` from t = 0 with no limiter, the plain limiter, the MLP-gated limiter and
     the shadow mode (plain decisions, gate misses counted); reports device time per step after `warmup`
@@ -182,6 +217,7 @@ def evaluate(params, nq=1024, steps=200, dt=0.06, confidence=0.9, precision="fp3
         cfg.slope_limiting = lim
         P = Problem(cfg, mesh)
         if mode:
+            P.set_indicator_features(feature_set)
             P.set_indicator(params, confidence=confidence, mode=mode)
         P.step_serial(warmup)
         if mode:
@@ -209,29 +245,50 @@ def main():
     ap.add_argument("cmd", choices=["train", "evaluate"])
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--nq", type=int, default=256)
-    ap.add_argument("--runs", type=int, default=12)
+    ap.add_argument("--runs", type=int, default=17)
     ap.add_argument("--steps", type=int, default=600)
-    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=16)
     ap.add_argument("--keep", type=float, default=0.035)
     ap.add_argument("--report", default=None)
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--eval-nq", type=int, default=1024)
     ap.add_argument("--eval-steps", type=int, default=200)
+    ap.add_argument("--compare-raw", action="store_true",
+                    help="also train on the raw feature set (same cells) and report both")
     a = ap.parse_args()
     if a.cmd == "evaluate":
         print(json.dumps(evaluate(load_weights(a.weights), nq=a.eval_nq, steps=a.eval_steps)), flush=True)
         return
+    torch = _torch()
+    sets = (0, 1) if a.compare_raw else (0,)
     t0 = time.time()
-    X, y = record(nq=a.nq, seeds=range(a.runs), steps=a.steps, keep=a.keep)
-    Xv, yv = record(nq=a.nq, seeds=range(1000, 1002), steps=a.steps, keep=a.keep, seed=1)
-    print(json.dumps({"train_cells": int(X.shape[0]), "val_cells": int(Xv.shape[0]),
-                      "record_seconds": time.time() - t0}), flush=True)
-    P, info = train(X, y, Xv, yv, epochs=a.epochs)
-    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
-    P.astype(np.float32).tofile(a.out)
+    Xs, y = record(nq=a.nq, seeds=range(a.runs), steps=a.steps, keep=a.keep, feature_sets=sets)
+    Xvs, yv = record(nq=a.nq, seeds=range(1000, 1002), steps=a.steps, keep=a.keep, seed=1, feature_sets=sets)
+    rep = {"train_cells": int(y.numel()), "val_cells": int(yv.numel()), "record_seconds": time.time() - t0}
+    print(json.dumps(rep), flush=True)
+    for fs, X, Xv in zip(sets, Xs, Xvs):
+        name = "characteristic" if fs == 0 else "raw"
+        if fs == 1:
+            # the raw set is trained on standardised inputs; the standardisation is then folded into the
+            # first layer so that the network reads the raw features
+            mu, sd = normalisation(X)
+            P, info = train((X - mu) / sd, y, (Xv - mu) / sd, yv, epochs=a.epochs)
+            P = fold_normalisation(P, mu.cpu().numpy(), sd.cpu().numpy())
+        else:
+            P, info = train(X, y, Xv, yv, epochs=a.epochs)
+        Pd = torch.from_numpy(P).cuda()
+        info["validation_fp32"] = metrics(forward(Xv, Pd, tensor_cores=False), yv)
+        info["validation_tensor_cores"] = metrics(forward(Xv, Pd, tensor_cores=True), yv)
+        rep[name] = info
+        out = a.out if fs == 0 else a.out.replace(".f32", "_raw.f32")
+        os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+        P.astype(np.float32).tofile(out)
+        rep[name]["weights"] = os.path.basename(out)
+        rep[name]["config4"] = evaluate(P, nq=a.eval_nq, steps=a.eval_steps, feature_set=fs)
+        print(json.dumps({name: {k: rep[name][k] for k in ("validation_fp32", "validation_tensor_cores")}}), flush=True)
     if a.report:
         with open(a.report, "w") as f:
-            json.dump(info, f, indent=1)
+            json.dump(rep, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -279,6 +279,11 @@ int32_t dgsw_rkdg_stage_record(dgsw_handle h, float* d_features, uint8_t* d_labe
  * the plain limiter). mode 2 (evaluation): the plain limiter decides every cell but writes back only
  * the cells mode 1 would visit, counting the misses. params: host FP32 array of DGSW_MLP_NPARAM. */
 int32_t dgsw_rkdg_set_indicator(dgsw_handle h, const float* params, double confidence, int32_t mode);
+/* the 18 features the indicator reads (dgsw_rkdg_indicator_features, dgsw_rkdg_stage_record and the gate):
+ * 0 (default) the scale-free characteristic set (fields in characteristic units, one common scale, TVB
+ * ratio, Froude numbers); 1 the raw set: the p = 1 modal coefficients of ze, qx, qy and the three
+ * neighbour cell means of each field (a network for it takes its input normalisation in its first layer) */
+int32_t dgsw_rkdg_set_indicator_features(dgsw_handle h, int32_t feature_set);
 /* accumulated counts since the last reset: [0] cells the limiter would look at, [1] cells sent to it,
  * [2] cells it changed, [3] cells it would have changed but the indicator skipped (mode 2) */
 int32_t dgsw_rkdg_indicator_stats(dgsw_handle h, int64_t* counts, int32_t reset);

@@ -20,6 +20,10 @@ and one scale s = max over the three fields of |b|, |c|, |d_f| (1 where that is 
 A cell takes part (ok) when it and its three neighbours are wet and each boundary face is land or
 function, the same condition under which the limiter looks at it.
 
+Feature set 1 ("raw", the learned-indicator workload's literal input list): [3 v + k] the modal
+coefficient k = 0, 1, 2 of field v (ze, qx, qy), then [9 + 3 f + v] the cell mean of field v in the
+neighbour across face f (the cell's own mean at a boundary face).
+
 Parameter vector (FP32 master copy, 5441 values): W1[64][18], b1[64], W2[64][64], b2[64], w3[64], b3.
 """
 import numpy as np
@@ -40,10 +44,10 @@ def unpack(P):
             P[OFF_B2:OFF_W3], P[OFF_W3:OFF_B3], P[OFF_B3])
 
 
-def features(q, wet, nbr, btype, node_xyz, elem_nodes, g, M):
+def features(q, wet, nbr, btype, node_xyz, elem_nodes, g, M, fset=0):
     """q [ne][3][nd] (ascending element ID), wet [ne], nbr [ne][3] (-1 at boundaries), btype [ne][3],
-    node_xyz [nn][3], elem_nodes [ne][3], gravity g, TVB constant M -> (features [ne][18] float32,
-    ok [ne] bool). Operation order matches the device code exactly (no fused multiply-adds)."""
+    node_xyz [nn][3], elem_nodes [ne][3], gravity g, TVB constant M, feature set -> (features [ne][18]
+    float32, ok [ne] bool). Operation order matches the device code exactly (no fused multiply-adds)."""
     q = np.asarray(q, np.float64)
     ne = q.shape[0]
     a = q[:, :, 0].copy()
@@ -51,6 +55,14 @@ def features(q, wet, nbr, btype, node_xyz, elem_nodes, g, M):
     c = q[:, :, 2].copy()
     has = nbr >= 0
     m = np.where(has[:, :, None], q[np.where(has, nbr, 0), :, 0], a[:, None, :])  # [ne][face][var]
+    w = np.asarray(wet) != 0
+    nbr_wet = np.where(has, w[np.where(has, nbr, 0)], btype <= 3)  # land, tide, flow, function objects
+    ok = w & nbr_wet.all(axis=1)
+    if fset == 1:
+        F = np.empty((ne, 18), np.float64)
+        F[:, 0:9] = q[:, :, 0:3].reshape(ne, 9)
+        F[:, 9:18] = m.reshape(ne, 9)
+        return F.astype(np.float32), ok
     d = m - a[:, None, :]
     X = node_xyz[elem_nodes]  # [ne][3][3]
     zb = X[:, 0, 2] * (1.0 / 3.0) + X[:, 1, 2] * (1.0 / 3.0) + X[:, 2, 2] * (1.0 / 3.0)
@@ -80,9 +92,6 @@ def features(q, wet, nbr, btype, node_xyz, elem_nodes, g, M):
         F[:, 4 + 5 * v] = c[:, v] * inv
         for f in range(3):
             F[:, 5 + 5 * v + f] = d[:, f, v] * inv
-    w = np.asarray(wet) != 0
-    nbr_wet = np.where(has, w[np.where(has, nbr, 0)], btype <= 3)  # land, tide, flow, function objects
-    ok = w & nbr_wet.all(axis=1)
     return F.astype(np.float32), ok
 
 

@@ -72,6 +72,11 @@ def test_oracle_features_by_hand():
     assert np.all(F[0, 13:] == 0)
     wet2 = np.array([1, 0, 1])
     assert list(mo.features(q, wet2, nbr, btype, xyz, en, g, M)[1]) == [False, False, True]
+    # the raw set: element 0's modes of ze, qx, qy, then per face the neighbour means (own at the land face)
+    R, okr = mo.features(q, wet, nbr, btype, xyz, en, g, M, fset=1)
+    assert np.array_equal(okr, ok)
+    assert np.allclose(R[0, :9], [1.0, 0.5, -0.2, 0.25, 0.0, 0.0, 0.0, 0.0, 0.0])
+    assert np.allclose(R[0, 9:], [1.5, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.25, 0.0])
 
 
 # ---------------------------------------------------------------------------------------------- GPU
@@ -89,18 +94,21 @@ def _bowl(nq=24, precision="fp32", seed=3):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_features_match_oracle_bit_exact(precision):
+@pytest.mark.parametrize("precision,fset", [("fp32", 0), ("fp64", 0), ("fp64", 1)])
+def test_features_match_oracle_bit_exact(precision, fset):
+    """Both feature sets: 0 the characteristic set, 1 the raw modal coefficients and neighbour means."""
     import torch
 
     mesh, cfg = _bowl(precision=precision)
     P = Problem(cfg, mesh)
     P.step_serial(30)
+    P.set_indicator_features(fset)
     feat = torch.empty((P.ne, 18), dtype=torch.float32, device="cuda")
     ok = torch.empty(P.ne, dtype=torch.uint8, device="cuda")
     P.indicator_features(feat.data_ptr(), ok.data_ptr())
     nbr, bt, _, _ = mesh_topology(mesh)
-    F, okr = mo.features(P.get_state(), P.get_wet(), nbr, bt, mesh.node_xyz, mesh.elem_nodes, cfg.g, cfg.sl_M)
+    F, okr = mo.features(P.get_state(), P.get_wet(), nbr, bt, mesh.node_xyz, mesh.elem_nodes, cfg.g, cfg.sl_M,
+                         fset=fset)
     assert okr.sum() > P.ne // 4 and (~okr).sum() > 0  # wet and dry cells both present
     assert np.array_equal(ok.cpu().numpy() != 0, okr)
     assert np.array_equal(feat.cpu().numpy(), F)
