@@ -14,6 +14,12 @@ Prints one JSON line per (configuration, precision): device ms per step after wa
 the handle's stream around graph-replayed steps), element-DOF updates per second per RK stage, the
 L2 error against the analytic solution at the end, and the host wall time of the handle's creation
 (topology, tiling, projections, uploads, initial state).
+
+Options for measuring single kernels (for instance under a profiler): --no-graphs launches every stage
+separately, --warmup sets the untimed steps, --tile fixes the tile size (default: the library's default,
+-1: the autotuner), --indicator 1 gates the limiter with the committed learned indicator (2: shadow
+mode), --trouble evaluates the KXRCF trouble indicator in each limiter pass, --postprocess computes the
+writers' output values once after the steps.
 """
 import argparse
 import json
@@ -43,21 +49,30 @@ def build(name, precision):
     raise ValueError(name)
 
 
-def measure(name, precision, steps, warmup=5):
+def measure(name, precision, steps, warmup=5, graphs=True, tile=0, indicator=0, trouble=False, postprocess=False):
     mesh, cfg = build(name, precision)
     t0 = time.perf_counter()
-    P = Problem(cfg, mesh)
+    P = Problem(cfg, mesh, use_graphs=graphs, tile=tile)
     create_s = time.perf_counter() - t0
+    if indicator:
+        from . import indicator as ind
+
+        P.set_indicator(ind.load_weights(), confidence=0.9, mode=indicator)
+    if trouble:
+        P.set_trouble(True)
     P.step_serial(warmup)
     P.step_serial(steps)
     ms, launches = P.last_step_timing()
     per_step = ms / steps
+    if postprocess:
+        P.postprocess()
     return {
         "config": name, "precision": precision, "elements": P.ne, "p": cfg.p, "stages": cfg.rk_nstages,
         "tile": P.info.tile, "steps": steps, "ms_per_step": per_step,
         "element_dof_per_s_per_stage": P.ne * P.nd * cfg.rk_nstages / (per_step * 1e-3),
         "kernel_launches_per_step": launches / steps, "l2_error": P.compute_residual_L2(),
-        "create_seconds": create_s,
+        "create_seconds": create_s, "occupancy": P.info.occupancy, "tile_order": P.info.tile_order,
+        "graphs": graphs, "indicator": indicator,
     }
 
 
@@ -66,11 +81,18 @@ def main():
     ap.add_argument("configs", nargs="*", default=["config1", "config2", "config3", "config3_nolim", "config4", "tidal_p1",
                                                    "tidal_p2", "levee_p1"])
     ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precisions", default="fp32,fp64")
+    ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--indicator", type=int, default=0, choices=[0, 1, 2])
+    ap.add_argument("--trouble", action="store_true")
+    ap.add_argument("--postprocess", action="store_true")
     a = ap.parse_args()
     for name in a.configs:
         for prec in a.precisions.split(","):
-            print(json.dumps(measure(name, prec, a.steps)), flush=True)
+            print(json.dumps(measure(name, prec, a.steps, a.warmup, graphs=not a.no_graphs, tile=a.tile,
+                                     indicator=a.indicator, trouble=a.trouble, postprocess=a.postprocess)), flush=True)
 
 
 if __name__ == "__main__":
