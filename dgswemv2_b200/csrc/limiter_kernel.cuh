@@ -108,11 +108,15 @@ template <int ND, typename Real>
 __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real>& L, int e, bool write) {
     const size_t P = (size_t)L.ne_pad;
     unsigned char lim = 0;
-    bool ok = L.wet[e] != 0;
+    // two rounds of loads: the own wet flag and the neighbours, then everything else at once (the
+    // neighbours' wet flags and means, the own modes, mean and geometry), before the decision to look
     int nb[3];
 #pragma unroll
+    for (int f = 0; f < 3; ++f) nb[f] = L.nbr[f * P + e];
+    if (!L.wet[e]) return 0;
+    bool ok = true;
+#pragma unroll
     for (int f = 0; f < 3; ++f) {
-        nb[f] = L.nbr[f * P + e];
         if (nb[f] >= 0) {
             ok = ok && (L.wet[nb[f]] != 0);
         } else {
@@ -123,7 +127,6 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
             ok = ok && (bt >= 0 && bt <= 3);  // DGSW_BC_LAND .. DGSW_BC_FUNCTION
         }
     }
-    if (!ok) return 0;
     // own vertex values (T_basis_linear) and derived barycentre / midpoint values
     double ql[3][3], qb[3], qm[3][3];
 #pragma unroll
@@ -152,6 +155,7 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
     for (int f = 0; f < 3; ++f)
 #pragma unroll
         for (int v = 0; v < 3; ++v) qnb[f][v] = nb[f] >= 0 ? L.baryctr[v * P + nb[f]] : qb[v];
+    if (!ok) return 0;
     const double zb = G[15];
     const double h = qb[0] + zb;
     const double u = qb[1] / h, vv = qb[2] / h;
@@ -248,17 +252,19 @@ __device__ __forceinline__ unsigned char cs_limit_element(const LimiterArgs<Real
 template <int ND, typename Real>
 __device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<Real>& L, int e, bool write) {
     const size_t P = (size_t)L.ne_pad;
-    bool ok = L.wet[e] != 0;
+    // two rounds of loads, as in cs_limit_element
     int nb[3];
 #pragma unroll
+    for (int f = 0; f < 3; ++f) nb[f] = L.nbr[f * P + e];
+    if (!L.wet[e]) return 0;
+    bool ok = true;
+#pragma unroll
     for (int f = 0; f < 3; ++f) {
-        nb[f] = L.nbr[f * P + e];
         if (nb[f] >= 0)
             ok = ok && (L.wet[nb[f]] != 0);
         else
             ok = ok && (-2 - nb[f] >= 0 && -2 - nb[f] <= 3);  // boundary objects: land .. function
     }
-    if (!ok) return 0;
     double md[3][3];  // modes 0..2 per variable
     float du[3][3], dn[3][3], nq[3];  // [bound][var] midpoint - barycentre, [face][var] neighbour - own, |ql|
     double qb[3];
@@ -285,6 +291,7 @@ __device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<
     } else {
         limiter_geometry(L, e, nb, G);
     }
+    if (!ok) return 0;
     const float h = (float)(qb[0] + G[15]);
     const float ih = 1.0f / h;
     const float u = (float)qb[1] * ih, vv = (float)qb[2] * ih;
@@ -386,17 +393,20 @@ __global__ void __launch_bounds__(256, MB) cs_limiter_kernel(const LimiterArgs<R
 
 // grid: one block per 256 elements, or a persistent grid of `list_blocks` blocks over a work list;
 // f32: the FP32-arithmetic form (the FP32 path)
+#ifndef DGSW_LIM_MB_BIG
+#define DGSW_LIM_MB_BIG 3
+#endif
 template <typename Real, bool F32>
 void launch_limiter_kernel_t(const LimiterArgs<Real>& L, int p, cudaStream_t s, int blocks) {
     const bool big = L.ne >= (1 << 18);
     if (p == 1) {
         if (big)
-            cs_limiter_kernel<3, Real, 3, F32><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<3, Real, DGSW_LIM_MB_BIG, F32><<<blocks, 256, 0, s>>>(L);
         else
             cs_limiter_kernel<3, Real, 2, F32><<<blocks, 256, 0, s>>>(L);
     } else {
         if (big)
-            cs_limiter_kernel<6, Real, 3, F32><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<6, Real, DGSW_LIM_MB_BIG, F32><<<blocks, 256, 0, s>>>(L);
         else
             cs_limiter_kernel<6, Real, 2, F32><<<blocks, 256, 0, s>>>(L);
     }
