@@ -333,6 +333,17 @@ __device__ __forceinline__ void sine_src_eval(const SineSrc<Real>& S, Real x, Re
     sine_src_terms<Real>(S, sx, cx, sy, cy, out);
 }
 
+// the sine set's source at one point, out of line; its constants are rebuilt from the set's parameters
+// (kernel parameter space) and the stage's time factors (shared memory), so no pointer to a local
+// value is taken
+template <typename Real>
+__device__ __noinline__ Val3<Real> sine_src_far(const double* params, const dgsw_fn_time* T, Real x, Real y) {
+    const SineSrc<Real> S = sine_src_prepare<Real>(params, *T);
+    Real out[3];
+    sine_src_eval<Real>(S, x, y, out);
+    return Val3<Real>{out[0], out[1], out[2]};
+}
+
 // ------------------------------------------------------------------------------------------------
 // wetting/drying of one p>=1 element on its vertex values, swe_post_wet_dry.hpp:6-145, in FP64.
 // qv: modal state (first three modes carry the linear part); returns the new wet flag and writes
@@ -811,7 +822,12 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                     const Real xg = xr0 * (Real)s0 + xr1 * (Real)s1 + xr2 * (Real)s2;
                     const Real yg = yr0 * (Real)s0 + yr1 * (Real)s1 + yr2 * (Real)s2;
                     Real fs[3];
-                    if (sine_set) {
+                    if (sine_set && sizeof(Real) == 8) {
+                        // FP64 elements large against the wavelength: out of line, so that this rarely
+                        // taken path keeps the kernel's hot code small
+                        const Val3<Real> r = sine_src_far<Real>(A.fn_params, &FT, xg, yg);
+                        fs[0] = r.v0, fs[1] = r.v1, fs[2] = r.v2;
+                    } else if (sine_set) {
                         sine_src_eval<Real>(SS, xg, yg, fs);
                     } else {
                         const Val3<Real> r = fn_eval_dev<Real>(A.fn_set, A.fn_params, &FT, 1, xg, yg);
