@@ -27,10 +27,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "element-DOF updates/s per RK stage, FP32+MLP vs FP64 plain on B200 at equal L2"
 UNIT = "element-DOF/s"
-# compulsory HBM bytes per element-DOF per RK stage (each array touched once): stage states read
-# (1 + the fraction of stages that also read q_0) and written, FP64 in both precisions; element
-# geometry and bathymetry (FP32 in the FP32 path) and the edge records. p = 2 SSP-RK3, p = 1 SSP-RK2.
-ALG_BYTES_PER_UNIT = {("fp32", 2): 77.0, ("fp64", 2): 87.0, ("fp32", 1): 82.0, ("fp64", 1): 99.0}
+# compulsory HBM bytes per element-DOF per RK stage (each array touched once), p = 2 SSP-RK3 and p = 1
+# SSP-RK2, keyed (precision, p, stage increments): element geometry and bathymetry (FP32 in the FP32 path)
+# and the edge records, plus the stage states. FP64 stage states: q_s read, q_{s+1} written, q_0 read by
+# the stages after the first. FP32 stage increments: the rounded carried state q0f (4 B) and the increment
+# d_s (4 B) read, d_{s+1} (4 B) written; the last stage reads the FP64 q_0 and writes q_0 + d_ns in FP64
+# and rounded (12 B).
+ALG_BYTES_PER_UNIT = {("fp32", 2, 0): 77.0, ("fp64", 2, 0): 87.0, ("fp32", 1, 0): 82.0, ("fp64", 1, 0): 99.0,
+                      ("fp32", 2, 1): 61.0, ("fp32", 1, 1): 76.0}
 
 
 def workload_name(nq, ne):
@@ -439,7 +443,7 @@ def run_ours(args):
         k64, n64 = P64.step_timed(args.steps)
         fp64 = {"value": job_value(units_per_step, args.steps, world, ms64), "ms_per_step": ms64 / args.steps,
                 "autotuned": autotuned(P64), "stage_kernel_ms": dist_max(k64 / max(1, n64), world)}
-        fp64["stage_kernel_frac_of_hbm"] = (ALG_BYTES_PER_UNIT[("fp64", cfg.p)] * ne * nd /
+        fp64["stage_kernel_frac_of_hbm"] = (ALG_BYTES_PER_UNIT[("fp64", cfg.p, 0)] * ne * nd /
                                             (fp64["stage_kernel_ms"] / 1e3) / 1e9 / load_peaks()[0])
         fp64["e2e"] = e2e_leg(P64, max(3, min(args.steps, 40)), world)
         # both paths advanced the same steps: warm-up, timed, kernel-timed and e2e
@@ -450,12 +454,13 @@ def run_ours(args):
         del P64
 
     peak, peak_kind = load_peaks()
-    alg = ALG_BYTES_PER_UNIT[(args.precision, cfg.p)] * ne * nd
+    alg = ALG_BYTES_PER_UNIT[(args.precision, cfg.p, P.info.stage_increments)] * ne * nd
     achieved = alg / (stage_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": load_traffic(args.precision), "peak_kind": peak_kind,
                 "kernel": "rkdg_stage_kernel<2,%s,...>" % ("float" if args.precision == "fp32" else "double"),
                 "stage_kernel_ms": stage_ms, "stage_kernel_launches_timed": int(klaunches),
+                "stage_states": "FP32 increments from the FP64 carried state" if P.info.stage_increments else "FP64",
                 "step_ms_over_stages": ms / (args.steps * ns), "algorithmic_bytes_per_launch": alg}
 
     out = {

@@ -16,7 +16,7 @@ __all__ = ["Problem", "ProblemConfig", "MeshArrays", "DgswError", "mesh_topology
 
 
 def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True, fp64_limiter=False, occupancy=0,
-                 tile_order=0):
+                 tile_order=0, fp64_stages=False):
     lib = _lib.load()
     c = _lib.Config()
     lib.dgsw_config_default(C.byref(c))
@@ -51,6 +51,7 @@ def _make_config(cfg, device=0, tile=0, renumber=True, use_graphs=True, fp64_lim
     c.fp64_limiter = int(fp64_limiter)
     c.occupancy = int(occupancy)
     c.tile_order = int(tile_order)
+    c.fp64_stages = int(fp64_stages)
     return c
 
 
@@ -111,14 +112,15 @@ def mesh_topology(mesh):
 
 
 def ensemble(cfg, meshes, member_params=None, device=0, tile=_lib.DGSW_TILE_AUTOTUNE, renumber=True,
-             use_graphs=True, init=True, occupancy=0, tile_order=0):
+             use_graphs=True, init=True, occupancy=0, tile_order=0, fp64_stages=False):
     """Ensemble batching (dgsw_ensemble_create): the members share `cfg` except their function-set
     parameters (member_params: one 16-value list per member, or None for cfg.fn_params). Returns a
     Problem whose state holds the members one after another (Problem.member_range)."""
     lib = _lib.load()
     P = Problem.__new__(Problem)
     P.cfg = cfg
-    P._c = _make_config(cfg, device, tile, renumber, use_graphs, occupancy=occupancy, tile_order=tile_order)
+    P._c = _make_config(cfg, device, tile, renumber, use_graphs, occupancy=occupancy, tile_order=tile_order,
+                        fp64_stages=fp64_stages)
     arr = (_lib.Mesh * len(meshes))()
     P._keep = []
     for k, m in enumerate(meshes):
@@ -147,10 +149,11 @@ class Problem:
     simulation.hpp:14-93)."""
 
     def __init__(self, cfg, mesh, device=0, tile=0, renumber=True, use_graphs=True, init=True, fp64_limiter=False,
-                 occupancy=0, tile_order=0):
+                 occupancy=0, tile_order=0, fp64_stages=False):
         lib = _lib.load()
         self.cfg = cfg
-        self._c = _make_config(cfg, device, tile, renumber, use_graphs, fp64_limiter, occupancy, tile_order)
+        self._c = _make_config(cfg, device, tile, renumber, use_graphs, fp64_limiter, occupancy, tile_order,
+                               fp64_stages)
         m, self._keep = _mesh_struct(mesh)
         h = C.c_void_p()
         _lib.check(lib.dgsw_rkdg_create(C.byref(self._c), C.byref(m), C.byref(h)))

@@ -66,7 +66,8 @@ class Config(C.Structure):
         ("fp64_limiter", C.c_int32),
         ("occupancy", C.c_int32),
         ("tile_order", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("fp64_stages", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -163,6 +164,8 @@ class Info(C.Structure):
         ("state_bytes", C.c_int64),
         ("occupancy", C.c_int32),
         ("tile_order", C.c_int32),
+        ("stage_increments", C.c_int32),
+        ("pad_", C.c_int32),
     ]
 
 

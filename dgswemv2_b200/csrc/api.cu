@@ -104,6 +104,14 @@ struct dgsw_rkdg_s {
     size_t real_size = 8;
     std::vector<void*> Q;    // ns+1 stage states
     std::vector<void*> SOL;  // stored stage solutions (only where needed)
+    // stage increments (FP32 precision without wetting/drying, limiter or levees, unless fp64_stages): the
+    // intermediate stage states live as FP32 increments D[s] = q_s - q_0 (s = 1 .. ns-1) and the stage
+    // inputs read the rounded carried state QF[qswap] (the copy of Q[0]); Q[1 .. ns-1] are filled only
+    // when the host API reads or writes a state in the middle of a step
+    bool split = false;
+    void* QF[2] = {nullptr, nullptr};
+    std::vector<void*> D;     // [ns], D[0] unused
+    std::vector<void*> DSOL;  // FP32 stored stage solutions (only where needed)
     void* bath = nullptr;  // [3][ne_pad] bathymetry modes of the linear part
     void* geo = nullptr;   // [5][ne_pad] J^-1 and |J|
     void* egeo = nullptr;  // [3][n_edges] edge normal and half length
@@ -208,6 +216,24 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
     A.store_sol = h->need_sol[s] ? 1 : 0;
     A.sol_out = (double*)h->SOL[s];
     A.q_out = (double*)h->Q[s + 1];
+    if (h->split) {
+        // the same terms as increments: q_0's term has none (d_0 = 0), q_k's is D[k]
+        int m = 0;
+        for (int k = 0; k < s; ++k)
+            if (h->rk.ark[s][k] != 0.0 || h->rk.brk[s][k] != 0.0) {
+                A.dk[m] = k ? (const Real*)h->D[k] : nullptr;
+                A.dsolk[m] = (const Real*)h->DSOL[k];
+                ++m;
+            }
+        A.dk[m] = s ? (const Real*)h->D[s] : nullptr;
+        A.dsolk[m] = nullptr;
+        A.q0f = (const Real*)h->QF[h->qswap];
+        A.q0 = (const double*)h->Q[0];
+        A.last = s + 1 == h->ns ? 1 : 0;
+        A.d_out = A.last ? nullptr : (Real*)h->D[s + 1];
+        A.q0f_out = A.last ? (Real*)h->QF[1 - h->qswap] : nullptr;
+        A.dsol_out = (Real*)h->DSOL[s];
+    }
     A.bath = (const Real*)h->bath;
     A.geo = (const Real*)h->geo;
     A.enodes = h->enodes.p;
@@ -261,6 +287,11 @@ cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<double>& A, int mod
 }
 cudaError_t launch_stage_any(dgsw_rkdg_s* h, const StageArgs<float>& A, int mode) {
     const int nt = (int)h->tiling.ntiles, mh = h->tiling.max_halo, me = h->tiling.max_edges;
+    if (h->split) {
+        const int m = mode | (h->occ ? STAGE_MODE_OCC : 0);
+        return h->cfg.p == 1 ? launch_stage_p1_f32_split(A, h->tile, nt, mh, me, m, h->stream)
+                             : launch_stage_p2_f32_split(A, h->tile, nt, mh, me, m, h->stream);
+    }
     if (h->occ)
         return h->cfg.p == 1 ? launch_stage_p1_f32_occ(A, h->tile, nt, mh, me, mode, h->stream)
                              : launch_stage_p2_f32_occ(A, h->tile, nt, mh, me, mode, h->stream);
@@ -381,6 +412,8 @@ __global__ void record_labels_kernel(const unsigned char* limited, const int* re
     labels[r] = labels[r] ? limited[d] : (uint8_t)255;
 }
 
+cudaError_t split_form(dgsw_rkdg_s* h, int s);
+
 // one RK stage: stage kernel, (clock on the last stage), indicator, limiter, wet flag buffer flip
 cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageRecord* rec = nullptr) {
     const bool timed = h->kt_on && h->kt_used + 2 <= h->kt_ev.size();
@@ -409,6 +442,8 @@ cudaError_t enqueue_stage(dgsw_rkdg_s* h, int s, int64_t& launches, const StageR
     }
     if (rec) {
         // features of the state the limiter is about to see; ok flags into the label buffer
+        e = split_form(h, s_out);
+        if (e != cudaSuccess) return e;
         e = launch_indicator_features<double>(feature_args<double>(h, s_out), h->ref_of_dev.p, rec->features,
                                               rec->labels, h->stream);
         if (e != cudaSuccess) return e;
@@ -515,6 +550,48 @@ int ensure_staging(dgsw_rkdg_s* h) {
     return DGSW_OK;
 }
 
+// Stage increments and the FP64 stage states, for the host API's reads and writes: a state written
+// through the API is turned into what the increment kernels read (the rounded carried state at stage 0,
+// the increment D[s] from q_0 after it), and a state read through the API in the middle of a step is
+// formed from them (Q[s] = q_0 + D[s], FP64)
+__global__ void split_absorb_kernel(const double* __restrict__ q, const double* __restrict__ q0,
+                                    float* __restrict__ out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = q0 ? (float)(q[i] - q0[i]) : (float)q[i];
+}
+
+__global__ void split_form_kernel(const double* __restrict__ q0, const float* __restrict__ d, double* __restrict__ out,
+                                  size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = q0[i] + (double)d[i];
+}
+
+unsigned split_grid(dgsw_rkdg_s* h, size_t n) {
+    return (unsigned)std::min<size_t>((n + 255) / 256, (size_t)8 * h->sm_count);
+}
+
+// after Q[h->stage] was written through the API
+cudaError_t split_absorb(dgsw_rkdg_s* h) {
+    if (!h->split) return cudaSuccess;
+    const size_t n = (size_t)3 * h->nd * h->ne_pad;
+    if (h->stage == 0)
+        split_absorb_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[0], nullptr,
+                                                                     (float*)h->QF[h->qswap], n);
+    else
+        split_absorb_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[h->stage],
+                                                                     (const double*)h->Q[0], (float*)h->D[h->stage], n);
+    return cudaGetLastError();
+}
+
+// before Q[s] is read outside the stage kernels (s = 0 is always current)
+cudaError_t split_form(dgsw_rkdg_s* h, int s) {
+    if (!h->split || s == 0) return cudaSuccess;
+    const size_t n = (size_t)3 * h->nd * h->ne_pad;
+    split_form_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[0], (const float*)h->D[s],
+                                                               (double*)h->Q[s], n);
+    return cudaGetLastError();
+}
+
 // host FP64 [ref][var][dof] -> one DMA into the staging buffer -> device permute + convert
 int upload_state(dgsw_rkdg_s* h, const double* q) {
     int rc = ensure_staging(h);
@@ -523,6 +600,7 @@ int upload_state(dgsw_rkdg_s* h, const double* q) {
     CUDA_TRY(cudaMemcpyAsync(h->staging.p, q, bytes, cudaMemcpyHostToDevice, h->stream));
     cudaError_t e = launch_permute_in<double, double>(h->staging.p, (double*)h->Q[h->stage], h->ref_of_dev.p,
                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    if (e == cudaSuccess) e = split_absorb(h);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("set_state: ") + cudaGetErrorString(e));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return DGSW_OK;
@@ -531,8 +609,10 @@ int upload_state(dgsw_rkdg_s* h, const double* q) {
 int download_state(dgsw_rkdg_s* h, double* q) {
     int rc = ensure_staging(h);
     if (rc) return rc;
-    cudaError_t e = launch_permute_out<double, double>((const double*)h->Q[h->stage], h->staging.p, h->ref_of_dev.p,
-                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    cudaError_t e = split_form(h, h->stage);
+    if (e == cudaSuccess)
+        e = launch_permute_out<double, double>((const double*)h->Q[h->stage], h->staging.p, h->ref_of_dev.p,
+                                               (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("get_state: ") + cudaGetErrorString(e));
     const size_t bytes = (size_t)h->ne * 3 * h->nd * sizeof(double);
     CUDA_TRY(cudaMemcpyAsync(q, h->staging.p, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -552,6 +632,10 @@ template <typename Real>
 int run_reduction(dgsw_rkdg_s* h, int what, double* out) {
     ReduceArgs<Real> R;
     std::memset(&R, 0, sizeof(R));
+    if (what != 0) {
+        cudaError_t ef = split_form(h, h->stage);
+        if (ef != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("reduction: ") + cudaGetErrorString(ef));
+    }
     // the L2 error reads state[0] (swe_post_comp_res_l2.hpp:12), the mass the current stage state
     R.q = (const double*)h->Q[what == 0 ? 0 : h->stage];
     R.bath = (const Real*)h->bath;
@@ -913,6 +997,29 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         limiter_geometry_kernel<double><<<(unsigned)((h->ne + 255) / 256), 256, 0, h->stream>>>(L, h->lgeo.p);
         if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cleanup_fail("limiter geometry", e);
     }
+    // stage increments: FP32 arithmetic on a configuration whose stage states only the stage kernel reads
+    // (no wetting/drying, slope limiter or levee pass, which work on the FP64 states)
+    h->split = h->fp32 && !cfg->fp64_stages && !cfg->wetting_drying && !cfg->slope_limiting && h->n_levee == 0;
+    if (h->split) {
+        const size_t nval = (size_t)3 * h->nd * h->ne_pad;
+        h->D.assign(h->ns, nullptr);
+        h->DSOL.assign(h->ns, nullptr);
+        for (int i = 0; i < 2; ++i) {
+            if ((e = cudaMalloc(&h->QF[i], nval * sizeof(float))) != cudaSuccess) return cleanup_fail("state alloc", e);
+            cudaMemset(h->QF[i], 0, nval * sizeof(float));
+            h->device_bytes += nval * sizeof(float);
+        }
+        for (int s = 1; s < h->ns; ++s) {
+            if ((e = cudaMalloc(&h->D[s], nval * sizeof(float))) != cudaSuccess) return cleanup_fail("state alloc", e);
+            cudaMemset(h->D[s], 0, nval * sizeof(float));
+            h->device_bytes += nval * sizeof(float);
+        }
+        for (int s = 0; s < h->ns; ++s)
+            if (h->need_sol[s]) {
+                if ((e = cudaMalloc(&h->DSOL[s], nval * sizeof(float))) != cudaSuccess) return cleanup_fail("sol alloc", e);
+                h->device_bytes += nval * sizeof(float);
+            }
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return cleanup_fail("setup", e);
     *out = h;
     return DGSW_OK;
@@ -1232,6 +1339,12 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
         if (p) cudaFree(p);
     for (void* p : h->SOL)
         if (p) cudaFree(p);
+    for (void* p : h->D)
+        if (p) cudaFree(p);
+    for (void* p : h->DSOL)
+        if (p) cudaFree(p);
+    for (void* p : h->QF)
+        if (p) cudaFree(p);
     if (h->bath) cudaFree(h->bath);
     if (h->geo) cudaFree(h->geo);
     if (h->egeo) cudaFree(h->egeo);
@@ -1303,6 +1416,7 @@ int32_t dgsw_rkdg_info(dgsw_handle h, dgsw_info* o) {
     o->state_bytes = (int64_t)3 * h->nd * h->ne_pad * (int64_t)sizeof(double);
     o->occupancy = h->occ;
     o->tile_order = h->order;
+    o->stage_increments = h->split ? 1 : 0;
     return DGSW_OK;
 }
 
@@ -1370,7 +1484,8 @@ int32_t dgsw_rkdg_postprocess(dgsw_handle h, double* point_data, double* cell_da
         A.nd = h->nd;
         return launch_postprocess<R>(A, h->stream);
     };
-    e = h->fp32 ? run((const float*)h->bath) : run((const double*)h->bath);
+    e = split_form(h, h->stage);
+    if (e == cudaSuccess) e = h->fp32 ? run((const float*)h->bath) : run((const double*)h->bath);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("postprocess: ") + cudaGetErrorString(e));
     CUDA_TRY(cudaMemcpyAsync(point_data, h->post.p, (size_t)h->ne * 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaMemcpyAsync(cell_data, h->post.p + (size_t)h->ne * 12, (size_t)h->ne * 4 * sizeof(double),
@@ -1420,8 +1535,10 @@ int32_t dgsw_rkdg_indicator_features(dgsw_handle h, float* d_features, uint8_t* 
     if (!h || !d_features) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     if (h->cfg.p != 1) return fail(DGSW_ERR_UNSUPPORTED, "the troubled-cell indicator is defined for p = 1");
     cudaSetDevice(h->device);
-    cudaError_t e = launch_indicator_features<double>(feature_args<double>(h, h->stage), h->ref_of_dev.p, d_features,
-                                                      d_ok, h->stream);
+    cudaError_t e = split_form(h, h->stage);
+    if (e == cudaSuccess)
+        e = launch_indicator_features<double>(feature_args<double>(h, h->stage), h->ref_of_dev.p, d_features, d_ok,
+                                              h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("indicator features: ") + cudaGetErrorString(e));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return DGSW_OK;
@@ -1551,6 +1668,7 @@ int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
     cudaSetDevice(h->device);
     cudaError_t e = launch_permute_in<double, double>((const double*)d_q, (double*)h->Q[h->stage], h->ref_of_dev.p,
                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    if (e == cudaSuccess) e = split_absorb(h);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("set_state_device: ") + cudaGetErrorString(e));
     return DGSW_OK;
 }
@@ -1558,8 +1676,10 @@ int32_t dgsw_rkdg_set_state_device(dgsw_handle h, const void* d_q) {
 int32_t dgsw_rkdg_get_state_device(dgsw_handle h, void* d_q) {
     if (!h || !d_q) return fail(DGSW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(h->device);
-    cudaError_t e = launch_permute_out<double, double>((const double*)h->Q[h->stage], (double*)d_q, h->ref_of_dev.p,
-                                                       (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
+    cudaError_t e = split_form(h, h->stage);
+    if (e == cudaSuccess)
+        e = launch_permute_out<double, double>((const double*)h->Q[h->stage], (double*)d_q, h->ref_of_dev.p,
+                                               (int)h->ne, (int)h->ne_pad, 3 * h->nd, h->stream);
     if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("get_state_device: ") + cudaGetErrorString(e));
     return DGSW_OK;
 }

@@ -104,7 +104,9 @@ __global__ void __launch_bounds__(kBlock) l2_static_finish(double* __restrict__ 
     if (threadIdx.x == 0) scratch[kResultSlot] = s;
 }
 
-// once per device, with that device current: fill the rule and look up the scratch address
+// once per device, with that device current: fill the rule and look up the scratch address. The result is
+// kept for the life of the process: after a cudaDeviceReset the saved address and the constant-memory rule
+// would be stale, so a reset between calls is not supported.
 int setup_device(int dev, double** out, std::string& err) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (g_scratch_ptr[dev]) {

@@ -113,6 +113,20 @@ struct StageArgs {
     const double* levF;
     unsigned char* went_dry;  // [ne] wet_dry_state.went_completely_dry of the last wet/dry pass, or null
     int reverse;              // visit the tiles in reverse order (grid = one CTA per tile)
+    // Stage increments (the SPLIT kernels, FP32 arithmetic without wetting/drying, limiter or levees): the
+    // carried state q_0 stays FP64 (q0) with a rounded copy (q0f) for the stage inputs, and each
+    // intermediate stage state is kept as its increment d_s = q_s - q_0 in Real. With sum_k a_sk = 1 the
+    // combination q_{s+1} = sum_k a_sk q_k + dt b_sk L(q_k) becomes d_{s+1} = sum_k a_sk d_k + dt b_sk L(q_k)
+    // (d_0 = 0): q_0 leaves it, so the increments round relative to their own small size and the carried
+    // state q_0 + d_ns is formed in FP64 at the last stage only.
+    const Real* dk[DGSW_RK_MAX_STAGES];     // increments of the combination's terms (null for q_0), d_s last
+    const Real* dsolk[DGSW_RK_MAX_STAGES];  // stored stage solutions of the earlier terms, in Real
+    const Real* q0f;                        // rounded carried state: stage input q_s = q0f + d_s
+    const double* q0;                       // FP64 carried state (read by the last stage)
+    Real* d_out;                            // d_{s+1} (intermediate stages)
+    Real* dsol_out;                         // this stage's solution, when a later stage reads it
+    Real* q0f_out;                          // rounding of the new carried state (last stage; q_out holds it)
+    int last;                               // this is the step's last stage
 };
 
 constexpr int FORCE_STRIDE_DEV = 9;
@@ -586,9 +600,10 @@ struct TileCap {
     static constexpr int edges = TILE + TILE / 2 + TILE / 4 + 16;  // 240 for 128, 464 for 256
 };
 
-template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, bool CAPPED, int OCC = 0>
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, bool CAPPED, int OCC = 0, bool SPLIT = false>
 __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::value))
     rkdg_stage_kernel(const __grid_constant__ StageArgs<Real> A, int max_halo_rt, int max_edges_rt) {
+    static_assert(!SPLIT || (!WD && sizeof(Real) == 4), "stage increments: FP32 arithmetic without wetting/drying");
     const int max_halo = CAPPED ? TileCap<TILE>::halo : max_halo_rt;
     const int max_edges = CAPPED ? TileCap<TILE>::edges : max_edges_rt;
     constexpr int ND = MT<P>::ND, NQ = MT<P>::NQ, NG = MT<P>::NG;
@@ -669,19 +684,52 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     int2 hrec = make_int2(0, -1);
     if (CAPPED && tid < nh) hrec = A.halo[hoff + tid];
     bool hwet = false;
+    // stage increments: the halo staging holds q0f in its first 3 ND Real rows and d_s in the next 3 ND
+    // (the same bytes as 3 ND doubles)
+    Real* shf = reinterpret_cast<Real*>(shq);
     auto issue_halo_copies = [&]() {
+        if constexpr (SPLIT) {
 #pragma unroll
-        for (int c = 0; c < 3 * ND; ++c) cp_async_value<double>(&shq[c * max_halo + tid], &qs[c * P_ + hrec.x]);
+            for (int c = 0; c < 3 * ND; ++c) cp_async_value<Real>(&shf[c * max_halo + tid], &A.q0f[c * P_ + hrec.x]);
+            if (A.dk[A.nterms - 1]) {
+#pragma unroll
+                for (int c = 0; c < 3 * ND; ++c)
+                    cp_async_value<Real>(&shf[(3 * ND + c) * max_halo + tid], &A.dk[A.nterms - 1][c * P_ + hrec.x]);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3 * ND; ++c) cp_async_value<double>(&shq[c * max_halo + tid], &qs[c * P_ + hrec.x]);
+        }
 #pragma unroll
         for (int k = 0; k < 3; ++k) cp_async_value<Real>(&shb[k * max_halo + tid], &A.bath[k * P_ + hrec.x]);
         hwet = A.wet_in[hrec.x] != 0;
+    };
+    // an element's stage state in Real: q_s (FP64 stage states) or q0f + d_s (stage increments)
+    auto load_state = [&](Real (&q)[3][ND], int e) {
+        if constexpr (SPLIT) {
+            const Real* __restrict__ ds = A.dk[A.nterms - 1];
+            if (ds) {
+                Real a[3 * ND], b[3 * ND];
+#pragma unroll
+                for (int c = 0; c < 3 * ND; ++c) a[c] = A.q0f[c * P_ + e];
+#pragma unroll
+                for (int c = 0; c < 3 * ND; ++c) b[c] = ds[c * P_ + e];
+#pragma unroll
+                for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = a[c] + b[c];
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = A.q0f[c * P_ + e];
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)qs[c * P_ + e];
+        }
     };
 
     // ---------------- phase 1: volume + source integrals, face traces ----------------
     if (active) {
         Real q[3][ND], b[3];
-#pragma unroll
-        for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)qs[c * P_ + d];
+        load_state(q, d);
         if (CAPPED && hrec.y >= 0) issue_halo_copies();
 #pragma unroll
         for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + d];
@@ -866,8 +914,19 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
             const int h = tid;
             cp_async_commit_and_wait();  // this thread's own copies
             Real q[3][ND], b[3], t[4][NG];
+            if constexpr (SPLIT) {
+                if (A.dk[A.nterms - 1]) {
 #pragma unroll
-            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)shq[c * max_halo + h];
+                    for (int c = 0; c < 3 * ND; ++c)
+                        q[c / ND][c % ND] = shf[c * max_halo + h] + shf[(3 * ND + c) * max_halo + h];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = shf[c * max_halo + h];
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)shq[c * max_halo + h];
+            }
 #pragma unroll
             for (int k = 0; k < 3; ++k) b[k] = shb[k * max_halo + h];
             if (hrec.y == 0)
@@ -889,8 +948,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
             const int2 it = A.halo[hoff + h];
             const int e = it.x;
             Real q[3][ND], b[3], t[4][NG];
-#pragma unroll
-            for (int c = 0; c < 3 * ND; ++c) q[c / ND][c % ND] = (Real)qs[c * P_ + e];
+            load_state(q, e);
 #pragma unroll
             for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + e];
             if (it.y == 0)
@@ -1017,11 +1075,47 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     // the edge gather below (one dependent load per value at the end of the CTA cost a global-memory
     // latency per value, per wave)
     double comb[3][ND];
+    // stage increments: the combination's increment terms sum_k a_k d_k + dt b_k sol_k in Real
+    Real dcomb[3][ND];
+    if constexpr (SPLIT) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int k = 0; k < ND; ++k) dcomb[v][k] = Real(0);
+        for (int j = 0; j < A.nterms; ++j) {
+            const Real* __restrict__ dj = A.dk[j];
+            if (dj) {
+                const Real aj = (Real)A.a[j];
+                Real t[3][ND];
+#pragma unroll
+                for (int v = 0; v < 3; ++v)
+#pragma unroll
+                    for (int k = 0; k < ND; ++k) t[v][k] = dj[(v * ND + k) * P_ + d];
+#pragma unroll
+                for (int v = 0; v < 3; ++v)
+#pragma unroll
+                    for (int k = 0; k < ND; ++k) dcomb[v][k] += aj * t[v][k];
+            }
+            if (j < A.nterms - 1 && A.bdt[j] != 0.0) {
+                const Real* __restrict__ sj = A.dsolk[j];
+                const Real bj = (Real)A.bdt[j];
+                Real u[3][ND];
+#pragma unroll
+                for (int v = 0; v < 3; ++v)
+#pragma unroll
+                    for (int k = 0; k < ND; ++k) u[v][k] = sj[(v * ND + k) * P_ + d];
+#pragma unroll
+                for (int v = 0; v < 3; ++v)
+#pragma unroll
+                    for (int k = 0; k < ND; ++k) dcomb[v][k] += bj * u[v][k];
+            }
+        }
+    }
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < ND; ++k) comb[v][k] = 0.0;
-    for (int j = 0; j < A.nterms; ++j) {
+    for (int j = 0; j < (SPLIT ? 0 : A.nterms); ++j) {
         const double* __restrict__ qj = A.qk[j];
         const double aj = A.a[j];
         double t[3][ND];
@@ -1102,6 +1196,56 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     }
     // M^-1 (the diagonal master mass inverse; 1 / |J| is already in) and the SSP-RK stage combination
     const double bdt_s = A.bdt[A.nterms - 1];
+    if constexpr (SPLIT) {
+        const Real bs = (Real)bdt_s;
+        Real dn[3][ND];
+        sfor<0, ND>([&](auto K) {
+            constexpr int k = decltype(K)::value;
+            const Real mk = (Real)MT<P>::minv(k);
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                const Real sol = rhs[v][k] * mk;
+                if (A.store_sol) A.dsol_out[(v * ND + k) * P_ + d] = sol;
+                dn[v][k] = dcomb[v][k] + bs * sol;
+            }
+        });
+        bool has_nan = false;
+        if (A.last) {
+            // the new carried state q_0 + d_ns in FP64, and its rounding for the next step's stage inputs
+            // (q_0 is loaded here rather than with the increments: held across the edge gather, its 36
+            // registers would spill)
+            double q0v[3][ND];
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int k = 0; k < ND; ++k) q0v[v][k] = A.q0[(v * ND + k) * P_ + d];
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int k = 0; k < ND; ++k) {
+                    const int idx = (v * ND + k) * P_ + d;
+                    const double qv = q0v[v][k] + (double)dn[v][k];
+                    has_nan |= isnan(qv);
+                    A.q_out[idx] = qv;
+                    A.q0f_out[idx] = (Real)qv;
+                }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int k = 0; k < ND; ++k) {
+                    has_nan |= isnan(dn[v][k]);
+                    A.d_out[(v * ND + k) * P_ + d] = dn[v][k];
+                }
+        }
+        A.wet_out[d] = wet ? 1 : 0;
+        if (has_nan) {
+            const unsigned long long counter = (unsigned long long)A.clock->step * A.nstages + A.stage_index;
+            atomicOr(&A.status->nan_flag, 1u);
+            atomicMin(&A.status->nan_key, (counter << 32) | (unsigned int)A.ref_of_dev[d]);
+        }
+        return;
+    }
     double qn[3][ND];
     sfor<0, ND>([&](auto K) {
         constexpr int k = decltype(K)::value;
@@ -1167,12 +1311,17 @@ cudaError_t launch_stage_p2_f64_occ(const StageArgs<double>& A, int tile, int nt
                                     int mode, cudaStream_t s);
 cudaError_t launch_stage_p2_f32_occ(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
                                     int mode, cudaStream_t s);
+// stage increments (StageArgs::dk ...): the default budget, or the alternative one with bit 3 of `mode`
+cudaError_t launch_stage_p1_f32_split(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                      int mode, cudaStream_t s);
+cudaError_t launch_stage_p2_f32_split(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                      int mode, cudaStream_t s);
 
-template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, int OCC>
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, int OCC, bool SPLIT = false>
 cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo, int max_edges, cudaStream_t s) {
     const bool capped = max_halo <= TileCap<TILE>::halo && max_edges <= TileCap<TILE>::edges;
-    auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, true, OCC>
-                       : rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, false, OCC>;
+    auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, true, OCC, SPLIT>
+                       : rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, false, OCC, SPLIT>;
     const size_t smem = capped ? Smem<P, Real, WD>::bytes(TILE, TileCap<TILE>::halo, TileCap<TILE>::edges)
                                : Smem<P, Real, WD>::bytes(TILE, max_halo, max_edges);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1181,14 +1330,14 @@ cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo
     return cudaGetLastError();
 }
 
-template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int OCC>
+template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int OCC, bool SPLIT = false>
 cudaError_t launch_stage_tile(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges,
                               cudaStream_t s) {
     switch (tile) {
         case 128:
-            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 128, OCC>(A, ntiles, max_halo, max_edges, s);
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 128, OCC, SPLIT>(A, ntiles, max_halo, max_edges, s);
         case 256:
-            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 256, OCC>(A, ntiles, max_halo, max_edges, s);
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 256, OCC, SPLIT>(A, ntiles, max_halo, max_edges, s);
         default:
             return cudaErrorInvalidValue;
     }
@@ -1207,6 +1356,20 @@ cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles
         case 5: return launch_stage_tile<P, Real, true, false, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
         case 6: return launch_stage_tile<P, Real, false, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
         default: return launch_stage_tile<P, Real, true, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+    }
+}
+
+// the stage-increment kernels (FP32, no wetting/drying): function source and bottom friction select the
+// instantiation (bits 1 and 2 of `mode`; bit 0, wetting/drying, must be clear)
+template <int P, int OCC>
+cudaError_t launch_stage_split_dispatch(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
+                                        int mode, cudaStream_t s) {
+    switch (mode & 7) {
+        case 0: return launch_stage_tile<P, float, false, false, false, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
+        case 2: return launch_stage_tile<P, float, false, true, false, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
+        case 4: return launch_stage_tile<P, float, false, false, true, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
+        case 6: return launch_stage_tile<P, float, false, true, true, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
+        default: return cudaErrorInvalidValue;
     }
 }
 

@@ -19,7 +19,8 @@ Options for measuring single kernels (for instance under a profiler): --no-graph
 separately, --warmup sets the untimed steps, --tile fixes the tile size (default: the library's default,
 -1: the autotuner), --indicator 1 gates the limiter with the committed learned indicator (2: shadow
 mode), --trouble evaluates the KXRCF trouble indicator in each limiter pass, --postprocess computes the
-writers' output values once after the steps.
+writers' output values once after the steps, --fp64-stages keeps the FP32 path's intermediate stage states
+in FP64 instead of FP32 increments.
 """
 import argparse
 import json
@@ -49,10 +50,11 @@ def build(name, precision):
     raise ValueError(name)
 
 
-def measure(name, precision, steps, warmup=5, graphs=True, tile=0, indicator=0, trouble=False, postprocess=False):
+def measure(name, precision, steps, warmup=5, graphs=True, tile=0, indicator=0, trouble=False, postprocess=False,
+            fp64_stages=False):
     mesh, cfg = build(name, precision)
     t0 = time.perf_counter()
-    P = Problem(cfg, mesh, use_graphs=graphs, tile=tile)
+    P = Problem(cfg, mesh, use_graphs=graphs, tile=tile, fp64_stages=fp64_stages)
     create_s = time.perf_counter() - t0
     if indicator:
         from . import indicator as ind
@@ -72,7 +74,7 @@ def measure(name, precision, steps, warmup=5, graphs=True, tile=0, indicator=0, 
         "element_dof_per_s_per_stage": P.ne * P.nd * cfg.rk_nstages / (per_step * 1e-3),
         "kernel_launches_per_step": launches / steps, "l2_error": P.compute_residual_L2(),
         "create_seconds": create_s, "occupancy": P.info.occupancy, "tile_order": P.info.tile_order,
-        "graphs": graphs, "indicator": indicator,
+        "graphs": graphs, "indicator": indicator, "stage_increments": P.info.stage_increments,
     }
 
 
@@ -88,11 +90,13 @@ def main():
     ap.add_argument("--indicator", type=int, default=0, choices=[0, 1, 2])
     ap.add_argument("--trouble", action="store_true")
     ap.add_argument("--postprocess", action="store_true")
+    ap.add_argument("--fp64-stages", action="store_true")
     a = ap.parse_args()
     for name in a.configs:
         for prec in a.precisions.split(","):
             print(json.dumps(measure(name, prec, a.steps, a.warmup, graphs=not a.no_graphs, tile=a.tile,
-                                     indicator=a.indicator, trouble=a.trouble, postprocess=a.postprocess)), flush=True)
+                                     indicator=a.indicator, trouble=a.trouble, postprocess=a.postprocess,
+                                     fp64_stages=a.fp64_stages)), flush=True)
 
 
 if __name__ == "__main__":

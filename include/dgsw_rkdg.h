@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define DGSW_ABI_VERSION 2
+#define DGSW_ABI_VERSION 3
 #define DGSW_TILE_AUTOTUNE (-1)
 
 typedef enum {
@@ -84,7 +84,12 @@ typedef struct {
                                   the autotuner when tile = DGSW_TILE_AUTOTUNE */
     int32_t tile_order;        /* 0 alternate the tile order from stage to stage (each stage starts where
                                   the previous one ended), 1 always ascending; set by the autotuner too */
-    int32_t reserved[5];
+    int32_t fp64_stages;       /* FP32 precision only: 1 keeps every intermediate stage state in FP64; 0
+                                  (default) keeps them as FP32 increments from the FP64 carried state
+                                  (q_s = q_0 + d_s; the carried state q_0 + d_ns is formed in FP64 at each
+                                  step's last stage) wherever only the stage kernel reads them: without
+                                  wetting/drying, slope limiter or levees */
+    int32_t reserved[4];
 } dgsw_config;
 
 /* One tide or flow block of the `.bcis` file (SWE::Inputs::read_bcis, problem_input/swe_inputs.cpp:211-
@@ -138,6 +143,8 @@ typedef struct {
     int64_t device_bytes;      /* bytes of device memory held by the handle */
     int64_t state_bytes;       /* bytes of one stage state array */
     int32_t occupancy, tile_order;  /* the stage kernel's register budget and tile order in use */
+    int32_t stage_increments;  /* 1 when the intermediate stage states are FP32 increments (fp64_stages) */
+    int32_t pad_;
 } dgsw_info;
 
 typedef struct dgsw_rkdg_s* dgsw_handle;
@@ -228,8 +235,10 @@ int32_t dgsw_rkdg_mass(dgsw_handle h, double* out);
  * function_set / fn_params (16 values, NULL = zeros) / t select true_q. Work is queued on `stream`
  * (NULL = default stream) and the call returns after it completes, with the result in *out (host).
  * The first call on a device does a one-time set-up (copies the quadrature table to the device and
- * looks up the scratch address); make that first call before any stream capture. All calls on one
- * device share the scratch array: calls that overlap on the GPU race and may return wrong values. */
+ * looks up the scratch address); make that first call before any stream capture. The set-up is kept
+ * for the life of the process, so a cudaDeviceReset between calls is not supported (the saved address and
+ * the device-side table would be stale). All calls on one device share the scratch array: calls that
+ * overlap on the GPU race and may return wrong values. */
 #define DGSW_L2_STATIC_MAX_ELEMS 1048576
 int32_t dgsw_l2_error_static(int32_t p, int64_t n_elems, const double* d_q, const int32_t* d_elem_nodes,
                              const double* d_node_xyz, int32_t function_set, const double* fn_params, double t,

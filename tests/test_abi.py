@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = _lib.load()
-    assert lib.dgsw_abi_version() == 2
+    assert lib.dgsw_abi_version() == 3
     assert lib.dgsw_status_string(0) == b"ok"
     assert lib.dgsw_status_string(4) == b"NaN in solution"
 
