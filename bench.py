@@ -34,7 +34,7 @@ UNIT = "element-DOF/s"
 # d_s (4 B) read, d_{s+1} (4 B) written; the last stage reads the FP64 q_0 and writes q_0 + d_ns in FP64
 # and rounded (12 B).
 ALG_BYTES_PER_UNIT = {("fp32", 2, 0): 77.0, ("fp64", 2, 0): 87.0, ("fp32", 1, 0): 82.0, ("fp64", 1, 0): 99.0,
-                      ("fp32", 2, 1): 61.0, ("fp32", 1, 1): 76.0}
+                      ("fp32", 2, 1): 61.0}
 
 
 def workload_name(nq, ne):
@@ -224,12 +224,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def load_traffic(precision):
-    """DRAM bytes per stage-kernel launch from the committed ncu summary of this workload, if any."""
+def load_traffic(key):
+    """DRAM bytes per stage-kernel launch (read + write, mean over the stages of one step) from the
+    committed ncu summary of this workload, if any; key "fp32_increments", "fp32" or "fp64"."""
     try:
         with open(os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")) as f:
             d = json.load(f)
-        return d.get(precision)
+        return d.get(key)
     except Exception:
         return None
 
@@ -457,7 +458,8 @@ def run_ours(args):
     alg = ALG_BYTES_PER_UNIT[(args.precision, cfg.p, P.info.stage_increments)] * ne * nd
     achieved = alg / (stage_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": load_traffic(args.precision), "peak_kind": peak_kind,
+                "traffic": load_traffic(args.precision + ("_increments" if P.info.stage_increments else "")),
+                "peak_kind": peak_kind,
                 "kernel": "rkdg_stage_kernel<2,%s,...>" % ("float" if args.precision == "fp32" else "double"),
                 "stage_kernel_ms": stage_ms, "stage_kernel_launches_timed": int(klaunches),
                 "stage_states": "FP32 increments from the FP64 carried state" if P.info.stage_increments else "FP64",
@@ -468,8 +470,8 @@ def run_ours(args):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
         "config": {"workload": workload_name(args.nq, ne), "elements": ne, "p": 2, "rk": "SSP(3,3)",
-                   "l2_cache": "no flush: the per-step working set (%d MB of stage states, bathymetry and mesh "
-                               "arrays) exceeds the 126 MB L2" % int(P.info.device_bytes / 2 ** 20)},
+                   "l2_cache": "no flush: each step moves %d MB of stage states, bathymetry and mesh arrays "
+                            "(algorithmic bytes), more than the 126 MB L2" % int(alg * ns / 1e6)},
         "precision": args.precision, "parallelism": "replicas" if world > 1 else "single GPU",
         "autotuned": autotuned(P),
         "gpu_launches": int(launches),

@@ -142,6 +142,7 @@ struct dgsw_rkdg_s {
     DBuf<int> nbr;     // neighbours per face, device order (limiter)
     DBuf<double> baryctr;  // barycentre values of the newest state (limiter)
     DBuf<double> lgeo;     // limiter geometry per element, [16][ne_pad]
+    DBuf<float> lgeo_f;    // its first 15 rows in FP32 (the FP32 limiter form)
     // trouble indicator (computed in each limiter pass only when asked for)
     int trouble_on = 0;
     DBuf<signed char> nbr_face;  // [3][ne_pad] the neighbour's face across each face
@@ -346,6 +347,7 @@ cudaError_t launch_limiter(dgsw_rkdg_s* h, int s_out) {
     L.status = h->status.p;
     L.ref_of_dev = h->ref_of_dev.p;
     L.lgeo = h->lgeo.p;
+    L.lgeo_f = h->lgeo_f.p;
     // the FP32 path limits in FP32 arithmetic (FP64 differences, decisions free of rounding noise)
     const bool f32 = h->fp32 && !h->cfg.fp64_limiter;
     if (h->ind_mode == 1) {
@@ -994,12 +996,20 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         L.nz = h->nz.p;
         L.ne = (int)h->ne;
         L.ne_pad = (int)h->ne_pad;
-        limiter_geometry_kernel<double><<<(unsigned)((h->ne + 255) / 256), 256, 0, h->stream>>>(L, h->lgeo.p);
+        if (h->fp32 && !cfg->fp64_limiter) {
+            if ((e = h->lgeo_f.alloc((size_t)(LIM_GEO - 1) * h->ne_pad)) != cudaSuccess) return cleanup_fail("alloc", e);
+            h->device_bytes += (int64_t)(LIM_GEO - 1) * h->ne_pad * 4;
+        }
+        limiter_geometry_kernel<double><<<(unsigned)((h->ne + 255) / 256), 256, 0, h->stream>>>(L, h->lgeo.p,
+                                                                                                h->lgeo_f.p);
         if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cleanup_fail("limiter geometry", e);
     }
     // stage increments: FP32 arithmetic on a configuration whose stage states only the stage kernel reads
-    // (no wetting/drying, slope limiter or levee pass, which work on the FP64 states)
-    h->split = h->fp32 && !cfg->fp64_stages && !cfg->wetting_drying && !cfg->slope_limiting && h->n_levee == 0;
+    // (no wetting/drying, slope limiter or levee pass, which work on the FP64 states), with at least three
+    // stages (measured on 524,288 triangles: p = 2 SSP-RK3 1.6-2.5 % faster per step; p = 1 SSP-RK2, where
+    // only one intermediate state exists, 2-3 % slower)
+    h->split = h->fp32 && !cfg->fp64_stages && !cfg->wetting_drying && !cfg->slope_limiting && h->n_levee == 0 &&
+               h->ns >= 3;
     if (h->split) {
         const size_t nval = (size_t)3 * h->nd * h->ne_pad;
         h->D.assign(h->ns, nullptr);
@@ -1377,6 +1387,7 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     h->nbr.release();
     h->baryctr.release();
     h->lgeo.release();
+    h->lgeo_f.release();
     h->nbr_face.release();
     h->tI.release();
     h->tflag.release();

@@ -37,6 +37,7 @@ struct LimiterArgs {
     const unsigned char* gate;       // write back only where gate[e] != 0 (NULL: everywhere)
     unsigned long long* counters;    // [IND_LIMITED], [IND_MISSED] accumulators (NULL: none)
     const double* lgeo;              // precomputed limiter geometry [16][ne_pad] (NULL: computed here)
+    const float* lgeo_f;             // its first 15 rows rounded to FP32, for the FP32 form (NULL: lgeo)
 };
 
 // Limiter geometry of element e (swe_pre_init_data.hpp:252-326): per median b (from the centroid to the
@@ -88,9 +89,12 @@ __device__ __forceinline__ void limiter_geometry(const LimiterArgs<Real>& L, int
     G[15] = L.nz[n0] * (1.0 / 3.0) + L.nz[n1] * (1.0 / 3.0) + L.nz[n2] * (1.0 / 3.0);
 }
 
-// once per handle: the geometry of every element into lgeo [LIM_GEO][ne_pad]
+// once per handle: the geometry of every element into lgeo [LIM_GEO][ne_pad], and, for the FP32 form, the
+// medians' coefficients, directions and squared lengths rounded to FP32 into lgeo_f [LIM_GEO - 1][ne_pad]
+// (the FP32 form does that arithmetic in FP32; the bathymetry at the barycentre stays FP64)
 template <typename Real>
-__global__ void __launch_bounds__(256) limiter_geometry_kernel(const LimiterArgs<Real> L, double* __restrict__ lgeo) {
+__global__ void __launch_bounds__(256) limiter_geometry_kernel(const LimiterArgs<Real> L, double* __restrict__ lgeo,
+                                                               float* __restrict__ lgeo_f) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= L.ne) return;
     const size_t P = (size_t)L.ne_pad;
@@ -101,6 +105,10 @@ __global__ void __launch_bounds__(256) limiter_geometry_kernel(const LimiterArgs
     limiter_geometry(L, e, nb, G);
 #pragma unroll
     for (int i = 0; i < LIM_GEO; ++i) lgeo[i * P + e] = G[i];
+    if (lgeo_f) {
+#pragma unroll
+        for (int i = 0; i < LIM_GEO - 1; ++i) lgeo_f[i * P + e] = (float)G[i];
+    }
 }
 
 // the limiter decision for element e (1 if its state changes); the new state is written only if `write`
@@ -284,15 +292,26 @@ __device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<
     for (int f = 0; f < 3; ++f)
 #pragma unroll
         for (int v = 0; v < 3; ++v) dn[f][v] = nb[f] >= 0 ? (float)(L.baryctr[v * P + nb[f]] - qb[v]) : 0.0f;
-    double G[LIM_GEO];
-    if (L.lgeo) {
+    float G[LIM_GEO - 1];
+    double zb;
+    if (L.lgeo_f) {
 #pragma unroll
-        for (int i = 0; i < LIM_GEO; ++i) G[i] = L.lgeo[i * P + e];
+        for (int i = 0; i < LIM_GEO - 1; ++i) G[i] = L.lgeo_f[i * P + e];
+        zb = L.lgeo[(LIM_GEO - 1) * P + e];
     } else {
-        limiter_geometry(L, e, nb, G);
+        double Gd[LIM_GEO];
+        if (L.lgeo) {
+#pragma unroll
+            for (int i = 0; i < LIM_GEO; ++i) Gd[i] = L.lgeo[i * P + e];
+        } else {
+            limiter_geometry(L, e, nb, Gd);
+        }
+#pragma unroll
+        for (int i = 0; i < LIM_GEO - 1; ++i) G[i] = (float)Gd[i];
+        zb = Gd[LIM_GEO - 1];
     }
     if (!ok) return 0;
-    const float h = (float)(qb[0] + G[15]);
+    const float h = (float)(qb[0] + zb);
     const float ih = 1.0f / h;
     const float u = (float)qb[1] * ih, vv = (float)qb[2] * ih;
     const float c = sqrtf((float)L.g * h), i2c = 0.5f / c;
@@ -301,8 +320,7 @@ __device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
         const int e1 = b, e2 = (b + 1) % 3;
-        const float al0 = (float)G[5 * b], al1 = (float)G[5 * b + 1], nx = (float)G[5 * b + 2], ny = (float)G[5 * b + 3],
-                    rsq = (float)G[5 * b + 4];
+        const float al0 = G[5 * b], al1 = G[5 * b + 1], nx = G[5 * b + 2], ny = G[5 * b + 3], rsq = G[5 * b + 4];
         const float un = u * nx + vv * ny;
         const float iR[3][3] = {{(c + un) * i2c, -nx * i2c, -ny * i2c},
                                 {u * ny - vv * nx, -ny, nx},

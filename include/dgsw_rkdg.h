@@ -88,7 +88,7 @@ typedef struct {
                                   (default) keeps them as FP32 increments from the FP64 carried state
                                   (q_s = q_0 + d_s; the carried state q_0 + d_ns is formed in FP64 at each
                                   step's last stage) wherever only the stage kernel reads them: without
-                                  wetting/drying, slope limiter or levees */
+                                  wetting/drying, slope limiter or levees, and with three or more stages */
     int32_t reserved[4];
 } dgsw_config;
 

@@ -130,10 +130,11 @@ def test_fp32_l2_stays_within_5_percent_over_2000_steps():
     assert l2["fp32"] <= 1.05 * l2["fp64"], l2
 
 
-@pytest.mark.parametrize("p,rk,tile", [(2, (3, 3), 256), (1, (2, 2), 128), (2, (5, 4), 128)])
+@pytest.mark.parametrize("p,rk,tile", [(2, (3, 3), 256), (1, (3, 3), 128), (2, (5, 4), 128)])
 def test_fp32_stage_increments(p, rk, tile):
     """FP32 arithmetic keeps the intermediate stage states as FP32 increments from the FP64 carried state
-    wherever only the stage kernel reads them (no wetting/drying, limiter or levees). Against the same
+    wherever only the stage kernel reads them (no wetting/drying, limiter or levees; three or more stages;
+    a two-stage scheme keeps FP64 stage states). Against the same
     FP32 path with FP64 stage states (fp64_stages), on the config-2 discretisation at 24 x 24 quads for 300
     steps: each variable within 1e-5 of its scale and the L2 errors within 0.1 %. Graph-replayed steps,
     plain launches and stage-by-stage calls give the same bits, and a state read and written back through
@@ -145,6 +146,8 @@ def test_fp32_stage_increments(p, rk, tile):
     A = Problem(cfg, mesh, tile=tile)
     B = Problem(cfg, mesh, tile=tile, fp64_stages=True)
     assert A.info.stage_increments == 1 and B.info.stage_increments == 0
+    m2, c2 = configs.manufactured(8, p=p, rk=(2, 2), dt=2.0, precision="fp32")
+    assert Problem(c2, m2).info.stage_increments == 0
     A.step_serial(300)
     B.step_serial(300)
     assert rel_err(A.get_state(), B.get_state()) <= 1e-5
