@@ -1154,6 +1154,13 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
 #pragma unroll
             for (int k = 0; k < ND; ++k) comb[v][k] += aj * t[v][k];
     }
+    // wetting/drying: the element's vertex depths, loaded now (two dependent loads) so that their latency
+    // overlaps the edge gather instead of opening the wet/dry pass
+    double bv[3] = {0.0, 0.0, 0.0};
+    if (WD) {
+        const int n0 = A.enodes[d], n1 = A.enodes[P_ + d], n2 = A.enodes[2 * P_ + d];
+        bv[0] = A.nz[n0], bv[1] = A.nz[n1], bv[2] = A.nz[n2];
+    }
     const Real iaJ = Real(1) / aJ;
     const int roles = es.y & 7;
     const int ord = es.y >> 3;
@@ -1273,7 +1280,6 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     });
     bool wet_new = wet;
     if (WD) {
-        const double bv[3] = {A.nz[A.enodes[d]], A.nz[A.enodes[P_ + d]], A.nz[A.enodes[2 * P_ + d]]};
         const double bmin = fmin(bv[0], fmin(bv[1], bv[2]));
         bool went_dry = false;
         wet_new = wetting_drying<ND, double>(qn, bv, bmin, A.h_o, A.h_o_thr, wet, went_dry);
