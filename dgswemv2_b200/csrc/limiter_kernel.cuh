@@ -273,14 +273,12 @@ __device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<
         else
             ok = ok && (-2 - nb[f] >= 0 && -2 - nb[f] <= 3);  // boundary objects: land .. function
     }
-    double md[3][3];  // modes 0..2 per variable
     float du[3][3], dn[3][3], nq[3];  // [bound][var] midpoint - barycentre, [face][var] neighbour - own, |ql|
     double qb[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
         const double a = (double)L.q[(v * ND + 0) * P + e], b = (double)L.q[(v * ND + 1) * P + e],
                      c = (double)L.q[(v * ND + 2) * P + e];
-        md[v][0] = a, md[v][1] = b, md[v][2] = c;
         const double l0 = a - b - c, l1 = a - b + c, l2 = a + 2.0 * b;
         qb[v] = L.baryctr[v * P + e];
         du[0][v] = (float)((l1 * 0.5 + l2 * 0.5) - qb[v]);
@@ -372,8 +370,10 @@ __device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<
         if (sqrtf(x0 * x0 + x1 * x1 + x2 * x2) > 1.0e-12f * nq[v]) {
             lim = 1;
             if (!write) continue;
-            L.q[(v * ND + 1) * P + e] = (Real)(md[v][1] + (double)((-x0 - x1 + 2.0f * x2) * (1.0f / 6.0f)));
-            L.q[(v * ND + 2) * P + e] = (Real)(md[v][2] + (double)((-x0 + x1) * 0.5f));
+            // the slope modes are read again here (L1 hits) rather than held in registers across the pass
+            const double m1 = (double)L.q[(v * ND + 1) * P + e], m2 = (double)L.q[(v * ND + 2) * P + e];
+            L.q[(v * ND + 1) * P + e] = (Real)(m1 + (double)((-x0 - x1 + 2.0f * x2) * (1.0f / 6.0f)));
+            L.q[(v * ND + 2) * P + e] = (Real)(m2 + (double)((-x0 + x1) * 0.5f));
 #pragma unroll
             for (int k = 3; k < ND; ++k) L.q[(v * ND + k) * P + e] = Real(0);
         }
@@ -382,8 +382,9 @@ __device__ __forceinline__ unsigned char cs_limit_element_f32(const LimiterArgs<
 }
 
 // One thread per visited element (every element, or the indicator's work list with a grid-stride loop).
-// MB resident 256-thread blocks per SM: 2 (128 registers) or 3 (80 registers and a few hundred bytes of
-// spills); measured on the bowl, 3 is 13 % faster at 524,288 triangles and 2 is faster at 131,072
+// MB resident 256-thread blocks per SM: 2 (128 registers), 3 (80 registers and a few hundred bytes of
+// spills) or 4 (64 registers, the FP32 form); measured on the bowl, 3 is 13 % faster than 2 at 524,288
+// triangles and 2 is faster at 131,072
 template <int ND, typename Real, int MB, bool F32 = false>
 __global__ void __launch_bounds__(256, MB) cs_limiter_kernel(const LimiterArgs<Real> L) {
     const int n = L.list ? *L.list_count : L.ne;
@@ -410,21 +411,28 @@ __global__ void __launch_bounds__(256, MB) cs_limiter_kernel(const LimiterArgs<R
 }
 
 // grid: one block per 256 elements, or a persistent grid of `list_blocks` blocks over a work list;
-// f32: the FP32-arithmetic form (the FP32 path)
+// f32: the FP32-arithmetic form (the FP32 path). Large meshes run more blocks per SM with fewer registers:
+// 3 (80 registers) for the FP64 form, 4 (64 registers) for the FP32 form, whose slope modes are re-read
+// at write-back instead of held (measured on the 2.1 M-triangle bowl: FP32 step 0.520 -> 0.499 ms at 4
+// against 3; FP64 0.757 -> 0.765 ms, so it stays at 3)
 #ifndef DGSW_LIM_MB_BIG
 #define DGSW_LIM_MB_BIG 3
+#endif
+#ifndef DGSW_LIM_MB_BIG_F32
+#define DGSW_LIM_MB_BIG_F32 4
 #endif
 template <typename Real, bool F32>
 void launch_limiter_kernel_t(const LimiterArgs<Real>& L, int p, cudaStream_t s, int blocks) {
     const bool big = L.ne >= (1 << 18);
+    constexpr int MB = F32 ? DGSW_LIM_MB_BIG_F32 : DGSW_LIM_MB_BIG;
     if (p == 1) {
         if (big)
-            cs_limiter_kernel<3, Real, DGSW_LIM_MB_BIG, F32><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<3, Real, MB, F32><<<blocks, 256, 0, s>>>(L);
         else
             cs_limiter_kernel<3, Real, 2, F32><<<blocks, 256, 0, s>>>(L);
     } else {
         if (big)
-            cs_limiter_kernel<6, Real, DGSW_LIM_MB_BIG, F32><<<blocks, 256, 0, s>>>(L);
+            cs_limiter_kernel<6, Real, MB, F32><<<blocks, 256, 0, s>>>(L);
         else
             cs_limiter_kernel<6, Real, 2, F32><<<blocks, 256, 0, s>>>(L);
     }
