@@ -105,11 +105,12 @@ struct dgsw_rkdg_s {
     std::vector<void*> Q;    // ns+1 stage states
     std::vector<void*> SOL;  // stored stage solutions (only where needed)
     // stage increments (FP32 precision without wetting/drying, limiter or levees, unless fp64_stages): the
-    // intermediate stage states live as FP32 increments D[s] = q_s - q_0 (s = 1 .. ns-1) and the stage
-    // inputs read the rounded carried state QF[qswap] (the copy of Q[0]); Q[1 .. ns-1] are filled only
-    // when the host API reads or writes a state in the middle of a step
+    // carried state lives as two FP32 parts QF[qswap] + QL[qswap] (leading and trailing), the intermediate
+    // stage states as FP32 increments D[s] = q_s - q_0 (s = 1 .. ns-1); the FP64 arrays Q[s] are formed only
+    // when the host API reads a state, and split again after it writes one
     bool split = false;
-    void* QF[2] = {nullptr, nullptr};
+    void* QF[2] = {nullptr, nullptr};  // the carried state's leading FP32 part (ping-pong pair)
+    void* QL[2] = {nullptr, nullptr};  // and its trailing part
     std::vector<void*> D;     // [ns], D[0] unused
     std::vector<void*> DSOL;  // FP32 stored stage solutions (only where needed)
     void* bath = nullptr;  // [3][ne_pad] bathymetry modes of the linear part
@@ -229,10 +230,11 @@ void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
         A.dk[m] = s ? (const Real*)h->D[s] : nullptr;
         A.dsolk[m] = nullptr;
         A.q0f = (const Real*)h->QF[h->qswap];
-        A.q0 = (const double*)h->Q[0];
+        A.q0lo = (const Real*)h->QL[h->qswap];
         A.last = s + 1 == h->ns ? 1 : 0;
         A.d_out = A.last ? nullptr : (Real*)h->D[s + 1];
         A.q0f_out = A.last ? (Real*)h->QF[1 - h->qswap] : nullptr;
+        A.q0lo_out = A.last ? (Real*)h->QL[1 - h->qswap] : nullptr;
         A.dsol_out = (Real*)h->DSOL[s];
     }
     A.bath = (const Real*)h->bath;
@@ -553,19 +555,30 @@ int ensure_staging(dgsw_rkdg_s* h) {
 }
 
 // Stage increments and the FP64 stage states, for the host API's reads and writes: a state written
-// through the API is turned into what the increment kernels read (the rounded carried state at stage 0,
-// the increment D[s] from q_0 after it), and a state read through the API in the middle of a step is
-// formed from them (Q[s] = q_0 + D[s], FP64)
-__global__ void split_absorb_kernel(const double* __restrict__ q, const double* __restrict__ q0,
-                                    float* __restrict__ out, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        out[i] = q0 ? (float)(q[i] - q0[i]) : (float)q[i];
+// through the API is turned into what the increment kernels read (the carried state's two FP32 parts at
+// stage 0, the increment D[s] from q_0 after it), and a state read through the API is formed from them
+// (Q[s] = q0f + q0lo + D[s], FP64; q0f + q0lo is exact in FP64)
+__global__ void split_carry_kernel(const double* __restrict__ q, float* __restrict__ hi, float* __restrict__ lo,
+                                   size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float h = (float)q[i];
+        hi[i] = h;
+        lo[i] = (float)(q[i] - (double)h);
+    }
 }
 
-__global__ void split_form_kernel(const double* __restrict__ q0, const float* __restrict__ d, double* __restrict__ out,
-                                  size_t n) {
+__global__ void split_incr_kernel(const double* __restrict__ q, const float* __restrict__ hi,
+                                  const float* __restrict__ lo, float* __restrict__ d, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        out[i] = q0[i] + (double)d[i];
+        d[i] = (float)(q[i] - ((double)hi[i] + (double)lo[i]));
+}
+
+__global__ void split_form_kernel(const float* __restrict__ hi, const float* __restrict__ lo,
+                                  const float* __restrict__ d, double* __restrict__ out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double q0 = (double)hi[i] + (double)lo[i];
+        out[i] = d ? q0 + (double)d[i] : q0;
+    }
 }
 
 unsigned split_grid(dgsw_rkdg_s* h, size_t n) {
@@ -576,20 +589,23 @@ unsigned split_grid(dgsw_rkdg_s* h, size_t n) {
 cudaError_t split_absorb(dgsw_rkdg_s* h) {
     if (!h->split) return cudaSuccess;
     const size_t n = (size_t)3 * h->nd * h->ne_pad;
+    float* hi = (float*)h->QF[h->qswap];
+    float* lo = (float*)h->QL[h->qswap];
     if (h->stage == 0)
-        split_absorb_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[0], nullptr,
-                                                                     (float*)h->QF[h->qswap], n);
+        split_carry_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[0], hi, lo, n);
     else
-        split_absorb_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[h->stage],
-                                                                     (const double*)h->Q[0], (float*)h->D[h->stage], n);
+        split_incr_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[h->stage], hi, lo,
+                                                                   (float*)h->D[h->stage], n);
     return cudaGetLastError();
 }
 
-// before Q[s] is read outside the stage kernels (s = 0 is always current)
+// before Q[s] is read outside the stage kernels
 cudaError_t split_form(dgsw_rkdg_s* h, int s) {
-    if (!h->split || s == 0) return cudaSuccess;
+    if (!h->split) return cudaSuccess;
     const size_t n = (size_t)3 * h->nd * h->ne_pad;
-    split_form_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const double*)h->Q[0], (const float*)h->D[s],
+    split_form_kernel<<<split_grid(h, n), 256, 0, h->stream>>>((const float*)h->QF[h->qswap],
+                                                               (const float*)h->QL[h->qswap],
+                                                               s ? (const float*)h->D[s] : nullptr,
                                                                (double*)h->Q[s], n);
     return cudaGetLastError();
 }
@@ -634,8 +650,8 @@ template <typename Real>
 int run_reduction(dgsw_rkdg_s* h, int what, double* out) {
     ReduceArgs<Real> R;
     std::memset(&R, 0, sizeof(R));
-    if (what != 0) {
-        cudaError_t ef = split_form(h, h->stage);
+    {
+        cudaError_t ef = split_form(h, what == 0 ? 0 : h->stage);
         if (ef != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("reduction: ") + cudaGetErrorString(ef));
     }
     // the L2 error reads state[0] (swe_post_comp_res_l2.hpp:12), the mass the current stage state
@@ -1016,8 +1032,10 @@ static int32_t create_impl(const dgsw_config* cfg, const dgsw_mesh* mesh, const 
         h->DSOL.assign(h->ns, nullptr);
         for (int i = 0; i < 2; ++i) {
             if ((e = cudaMalloc(&h->QF[i], nval * sizeof(float))) != cudaSuccess) return cleanup_fail("state alloc", e);
+            if ((e = cudaMalloc(&h->QL[i], nval * sizeof(float))) != cudaSuccess) return cleanup_fail("state alloc", e);
             cudaMemset(h->QF[i], 0, nval * sizeof(float));
-            h->device_bytes += nval * sizeof(float);
+            cudaMemset(h->QL[i], 0, nval * sizeof(float));
+            h->device_bytes += 2 * nval * sizeof(float);
         }
         for (int s = 1; s < h->ns; ++s) {
             if ((e = cudaMalloc(&h->D[s], nval * sizeof(float))) != cudaSuccess) return cleanup_fail("state alloc", e);
@@ -1354,6 +1372,8 @@ int32_t dgsw_rkdg_destroy(dgsw_handle h) {
     for (void* p : h->DSOL)
         if (p) cudaFree(p);
     for (void* p : h->QF)
+        if (p) cudaFree(p);
+    for (void* p : h->QL)
         if (p) cudaFree(p);
     if (h->bath) cudaFree(h->bath);
     if (h->geo) cudaFree(h->geo);

@@ -114,18 +114,20 @@ struct StageArgs {
     unsigned char* went_dry;  // [ne] wet_dry_state.went_completely_dry of the last wet/dry pass, or null
     int reverse;              // visit the tiles in reverse order (grid = one CTA per tile)
     // Stage increments (the SPLIT kernels, FP32 arithmetic without wetting/drying, limiter or levees): the
-    // carried state q_0 stays FP64 (q0) with a rounded copy (q0f) for the stage inputs, and each
-    // intermediate stage state is kept as its increment d_s = q_s - q_0 in Real. With sum_k a_sk = 1 the
-    // combination q_{s+1} = sum_k a_sk q_k + dt b_sk L(q_k) becomes d_{s+1} = sum_k a_sk d_k + dt b_sk L(q_k)
-    // (d_0 = 0): q_0 leaves it, so the increments round relative to their own small size and the carried
-    // state q_0 + d_ns is formed in FP64 at the last stage only.
+    // carried state q_0 is kept compensated, as the unevaluated sum q0f + q0lo of two Real values (q0f the
+    // rounding of q_0, q0lo the rounding of the remainder: a 48-bit significand), and each intermediate
+    // stage state as its increment d_s = q_s - q_0 in Real. With sum_k a_sk = 1 the combination
+    // q_{s+1} = sum_k a_sk q_k + dt b_sk L(q_k) becomes d_{s+1} = sum_k a_sk d_k + dt b_sk L(q_k) (d_0 = 0):
+    // q_0 leaves it, so the increments round relative to their own small size. The last stage forms
+    // q0f + q0lo + d_ns in FP64 and splits it again.
     const Real* dk[DGSW_RK_MAX_STAGES];     // increments of the combination's terms (null for q_0), d_s last
     const Real* dsolk[DGSW_RK_MAX_STAGES];  // stored stage solutions of the earlier terms, in Real
-    const Real* q0f;                        // rounded carried state: stage input q_s = q0f + d_s
-    const double* q0;                       // FP64 carried state (read by the last stage)
+    const Real* q0f;                        // carried state, leading part: stage input q_s = q0f + d_s
+    const Real* q0lo;                       // carried state, trailing part (read by the last stage)
     Real* d_out;                            // d_{s+1} (intermediate stages)
     Real* dsol_out;                         // this stage's solution, when a later stage reads it
-    Real* q0f_out;                          // rounding of the new carried state (last stage; q_out holds it)
+    Real* q0f_out;                          // new carried state, leading part (last stage)
+    Real* q0lo_out;                         // new carried state, trailing part (last stage)
     int last;                               // this is the step's last stage
 };
 
@@ -719,13 +721,14 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
             if (e16 > b16) prefetch(A.egeo + b16, (unsigned)(e16 - b16) * (unsigned)sizeof(Real));
         }
     }
-    // stage increments, last stage: the FP64 carried state q_0 is read only in the epilogue; one thread
-    // asks L2 for this tile's rows now, so that those loads start on L2 hits
+    // stage increments, last stage: the carried state's trailing part is read only in the epilogue; one
+    // thread asks L2 for this tile's rows now, so that those loads start on L2 hits
     if constexpr (SPLIT) {
         if (A.last && tid == 0) {
-            const unsigned rowb = (unsigned)((nloc + 1) & ~1) * 8u;
+            const unsigned rowb = (unsigned)((nloc + 3) & ~3) * 4u;
             for (int c = 0; c < 3 * ND; ++c)
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.q0 + (size_t)c * P_ + e0), "r"(rowb)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.q0lo + (size_t)c * P_ + e0),
+                             "r"(rowb)
                              : "memory");
         }
     }
@@ -1259,23 +1262,28 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
         });
         bool has_nan = false;
         if (A.last) {
-            // the new carried state q_0 + d_ns in FP64, and its rounding for the next step's stage inputs
-            // (q_0 is loaded here rather than with the increments: held across the edge gather, its 36
-            // registers would spill)
-            double q0v[3][ND];
+            // the new carried state q0f + q0lo + d_ns in FP64 (q0f + q0lo is exact there), split again into
+            // its leading and trailing Real parts; q_0 is loaded here rather than with the increments (held
+            // across the edge gather its registers would spill; its leading part is an L1 or L2 hit from
+            // phase 1)
+            Real hi[3][ND], lo[3][ND];
 #pragma unroll
             for (int v = 0; v < 3; ++v)
 #pragma unroll
-                for (int k = 0; k < ND; ++k) q0v[v][k] = A.q0[(v * ND + k) * P_ + d];
+                for (int k = 0; k < ND; ++k) {
+                    hi[v][k] = A.q0f[(v * ND + k) * P_ + d];
+                    lo[v][k] = A.q0lo[(v * ND + k) * P_ + d];
+                }
 #pragma unroll
             for (int v = 0; v < 3; ++v)
 #pragma unroll
                 for (int k = 0; k < ND; ++k) {
                     const int idx = (v * ND + k) * P_ + d;
-                    const double qv = q0v[v][k] + (double)dn[v][k];
+                    const double qv = ((double)hi[v][k] + (double)lo[v][k]) + (double)dn[v][k];
                     has_nan |= isnan(qv);
-                    A.q_out[idx] = qv;
-                    A.q0f_out[idx] = (Real)qv;
+                    const Real h2 = (Real)qv;
+                    A.q0f_out[idx] = h2;
+                    A.q0lo_out[idx] = (Real)(qv - (double)h2);
                 }
         } else {
 #pragma unroll

@@ -85,8 +85,8 @@ typedef struct {
     int32_t tile_order;        /* 0 alternate the tile order from stage to stage (each stage starts where
                                   the previous one ended), 1 always ascending; set by the autotuner too */
     int32_t fp64_stages;       /* FP32 precision only: 1 keeps every intermediate stage state in FP64; 0
-                                  (default) keeps them as FP32 increments from the FP64 carried state
-                                  (q_s = q_0 + d_s; the carried state q_0 + d_ns is formed in FP64 at each
+                                  (default) keeps them as FP32 increments from the carried state, itself
+                                  kept as two FP32 parts (q_s = q_0 + d_s; q_0 + d_ns is formed in FP64 at each
                                   step's last stage) wherever only the stage kernel reads them: without
                                   wetting/drying, slope limiter or levees, and with three or more stages */
     int32_t reserved[4];

@@ -132,7 +132,8 @@ def test_fp32_l2_stays_within_5_percent_over_2000_steps():
 
 @pytest.mark.parametrize("p,rk,tile", [(2, (3, 3), 256), (1, (3, 3), 128), (2, (5, 4), 128)])
 def test_fp32_stage_increments(p, rk, tile):
-    """FP32 arithmetic keeps the intermediate stage states as FP32 increments from the FP64 carried state
+    """FP32 arithmetic keeps the intermediate stage states as FP32 increments from the carried state (two FP32
+    parts)
     wherever only the stage kernel reads them (no wetting/drying, limiter or levees; three or more stages;
     a two-stage scheme keeps FP64 stage states). Against the same
     FP32 path with FP64 stage states (fp64_stages), on the config-2 discretisation at 24 x 24 quads for 300
@@ -171,6 +172,22 @@ def test_fp32_stage_increments(p, rk, tile):
     assert rel_err(R.get_state(), mid) <= 1e-7
     R.step_serial(1)
     assert rel_err(R.get_state(), A.get_state()) <= 1e-6
+
+
+def test_fp32_l2_on_a_limited_p2_bowl():
+    """FP32 at equal L2 on a limited p = 2 run: Thacker's bowl with wetting/drying and the Cockburn-Shu
+    limiter at p = 2 (SSP-RK3, 96 x 96 quads, dt = 0.25 s, 1,344 steps: half a period), where a flipped
+    write-back decision zeroes an element's p = 2 modes. The FP32 path's L2 error against the analytic
+    surface stays within 1.05x of the FP64 path's."""
+    l2 = {}
+    for prec in ("fp32", "fp64"):
+        mesh, cfg = configs.config3(nq=96, dt=0.25, precision=prec)
+        cfg.p, cfg.rk_nstages, cfg.rk_order = 2, 3, 3
+        P = Problem(cfg, mesh)
+        P.step_serial(1344)
+        l2[prec] = P.compute_residual_L2()
+        assert np.isfinite(P.get_state()).all()
+    assert l2["fp32"] <= 1.05 * l2["fp64"], l2
 
 
 def test_fp32_limiter_against_the_fp64_limiter():
