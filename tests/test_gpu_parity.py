@@ -132,12 +132,10 @@ def test_fp32_l2_stays_within_5_percent_over_2000_steps():
 
 @pytest.mark.parametrize("p,rk,tile", [(2, (3, 3), 256), (1, (3, 3), 128), (2, (5, 4), 128)])
 def test_fp32_stage_increments(p, rk, tile):
-    """FP32 arithmetic keeps the intermediate stage states as FP32 increments from the carried state (two FP32
-    parts)
-    wherever only the stage kernel reads them (no wetting/drying, limiter or levees; three or more stages;
-    a two-stage scheme keeps FP64 stage states). Against the same
-    FP32 path with FP64 stage states (fp64_stages), on the config-2 discretisation at 24 x 24 quads for 300
-    steps: each variable within 1e-5 of its scale and the L2 errors within 0.1 %. Graph-replayed steps,
+    """FP32 arithmetic keeps the intermediate stage states as FP32 increments from the carried state (kept
+    as two FP32 parts) wherever only the stage kernel reads them: no wetting/drying, limiter or levees, and
+    three or more stages (a two-stage scheme keeps FP64 stage states). Against the same FP32 path with FP64
+    stage states (fp64_stages), on the config-2 discretisation at 24 x 24 quads for 300 steps: each variable within 1e-5 of its scale and the L2 errors within 0.1 %. Graph-replayed steps,
     plain launches and stage-by-stage calls give the same bits, and a state read and written back through
     the host API in the middle of a step (Q_s = q_0 + d_s formed in FP64, then split again) continues
     within 1e-6 of the undisturbed run. SSP(5,4) covers combinations with several increment terms and a
