@@ -172,19 +172,21 @@ def test_fp32_stage_increments(p, rk, tile):
     assert rel_err(R.get_state(), A.get_state()) <= 1e-6
 
 
-def test_fp32_l2_on_a_limited_p2_bowl():
-    """FP32 at equal L2 on a limited p = 2 run: Thacker's bowl with wetting/drying and the Cockburn-Shu
-    limiter at p = 2 (SSP-RK3, 96 x 96 quads, dt = 0.25 s, 1,344 steps: half a period), where a flipped
-    write-back decision zeroes an element's p = 2 modes. The FP32 path's L2 error against the analytic
-    surface stays within 1.05x of the FP64 path's."""
+def test_fp32_l2_on_a_limited_p2_run():
+    """FP32 at equal L2 on a limited p = 2 run: the config-2 discretisation (manufactured solution, p = 2,
+    SSP-RK3, jittered) at 32 x 32 quads with the Cockburn-Shu limiter (M = 1e-8), 500 steps of dt = 2 s. The
+    limiter acts on about 7 % of the elements per stage and a flipped write-back decision zeroes an
+    element's p = 2 modes; the FP32 path's L2 error against the analytic solution stays within 1.05x of the
+    FP64 path's. (Thacker's bowl at p = 2 with wetting/drying and the limiter is no test case: the FP64
+    oracle itself produces a NaN there after 120-150 s of simulated time, at every time step tried.)"""
     l2 = {}
     for prec in ("fp32", "fp64"):
-        mesh, cfg = configs.config3(nq=96, dt=0.25, precision=prec)
-        cfg.p, cfg.rk_nstages, cfg.rk_order = 2, 3, 3
+        mesh, cfg = configs.manufactured(32, p=2, rk=(3, 3), dt=2.0, jitter=0.2, precision=prec)
+        cfg.slope_limiting = True
         P = Problem(cfg, mesh)
-        P.step_serial(1344)
+        P.step_serial(500)
         l2[prec] = P.compute_residual_L2()
-        assert np.isfinite(P.get_state()).all()
+        assert 0.02 <= float(np.mean(P.get_limited())) <= 0.2, np.mean(P.get_limited())
     assert l2["fp32"] <= 1.05 * l2["fp64"], l2
 
 
