@@ -518,6 +518,40 @@ __device__ __forceinline__ void face_trace(const Real (&q)[3][MT<P>::ND], const 
     });
 }
 
+// the same trace for a face known only at run time, with the face's basis values from a [mode][gp] table:
+// the halo faces of a warp belong to different faces, and one compile-time copy per face would split the
+// warp. Entries that are zero on this face but not on another add a zero product (the sum is unchanged), so
+// the values equal face_trace's bit for bit.
+template <int P, typename Real>
+__device__ __forceinline__ void face_trace_rt(const Real (&q)[3][MT<P>::ND], const Real (&b)[3], const Real* cf,
+                                              Real (&t)[4][MT<P>::NG]) {
+    constexpr int ND = MT<P>::ND, NG = MT<P>::NG;
+    sfor<0, NG>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        sfor<0, 3>([&](auto V) {
+            constexpr int v = decltype(V)::value;
+            Real s = Real(0);
+            sfor<0, ND>([&](auto K) {
+                constexpr int k = decltype(K)::value;
+                constexpr bool used = MT<P>::fphi((0 * ND + k) * NG + g) != 0.0 ||
+                                      MT<P>::fphi((1 * ND + k) * NG + g) != 0.0 ||
+                                      MT<P>::fphi((2 * ND + k) * NG + g) != 0.0;
+                if constexpr (used) s += q[v][k] * cf[k * NG + g];
+            });
+            t[v][g] = s;
+        });
+        Real sb = Real(0);
+        sfor<0, 3>([&](auto K) {
+            constexpr int k = decltype(K)::value;
+            constexpr bool used = MT<P>::fphi((0 * ND + k) * NG + g) != 0.0 ||
+                                  MT<P>::fphi((1 * ND + k) * NG + g) != 0.0 ||
+                                  MT<P>::fphi((2 * ND + k) * NG + g) != 0.0;
+            if constexpr (used) sb += b[k] * cf[k * NG + g];
+        });
+        t[3][g] = sb;
+    });
+}
+
 // shared-memory layout of the stage kernel
 template <int P, typename Real, bool WD>
 struct Smem {
@@ -635,6 +669,21 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     // the stage's time factors, once per CTA in shared memory (the out-of-line helpers read them there)
     __shared__ dgsw_fn_time sFT;
     if (threadIdx.x == 0) sFT = dgsw_fn_prepare(A.fn_set, A.fn_params, t_stage);
+    // the face traces' basis values at the edge Gauss points, [face][mode][gp], for phase 3's lift and the
+    // halo traces: the elements of a warp visit their faces in different orders, and compile-time tables per
+    // face split the warp into one branch per face. Measured per step (bit-identical results): FP32 at p = 2
+    // -0.6 to -0.9 %; FP64 at p = 2 -0.6 to +0.5 %, p = 1 +1 to +4 % (the shared-memory loads cost more than
+    // the divergence there), so only FP32 at p = 2 uses it
+    constexpr bool rt_face = P == 2 && sizeof(Real) == 4;
+    __shared__ Real sfphi[3 * ND * NG];
+    if (rt_face && threadIdx.x < 3 * ND * NG) {
+        Real c = Real(0);
+        sfor<0, 3 * ND * NG>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            if (threadIdx.x == i) c = (Real)MT<P>::fphi(i);
+        });
+        sfphi[threadIdx.x] = c;
+    }
     __syncthreads();
     const dgsw_fn_time& FT = sFT;
     // the manufactured sine set's source inline, in both precisions; other sets go through fn_eval_dev
@@ -990,12 +1039,15 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
             }
 #pragma unroll
             for (int k = 0; k < 3; ++k) b[k] = shb[k * max_halo + h];
-            if (hrec.y == 0)
+            if constexpr (rt_face) {
+                face_trace_rt<P, Real>(q, b, sfphi + hrec.y * ND * NG, t);
+            } else if (hrec.y == 0) {
                 face_trace<P, 0, Real>(q, b, t);
-            else if (hrec.y == 1)
+            } else if (hrec.y == 1) {
                 face_trace<P, 1, Real>(q, b, t);
-            else
+            } else {
                 face_trace<P, 2, Real>(q, b, t);
+            }
             const int slot = 3 * TILE + h;
 #pragma unroll
             for (int c = 0; c < 4; ++c)
@@ -1012,12 +1064,15 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
             load_state(q, e);
 #pragma unroll
             for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + e];
-            if (it.y == 0)
+            if constexpr (rt_face) {
+                face_trace_rt<P, Real>(q, b, sfphi + it.y * ND * NG, t);
+            } else if (it.y == 0) {
                 face_trace<P, 0, Real>(q, b, t);
-            else if (it.y == 1)
+            } else if (it.y == 1) {
                 face_trace<P, 1, Real>(q, b, t);
-            else
+            } else {
                 face_trace<P, 2, Real>(q, b, t);
+            }
             const int slot = 3 * TILE + h;
 #pragma unroll
             for (int c = 0; c < 4; ++c)
@@ -1220,8 +1275,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                     F[v][gp] = WD ? sF[((3 + v) * NG + ga) * max_edges + slot] : -sF[(v * NG + ga) * max_edges + slot];
             }
         }
-        auto contrib = [&](auto FF) {
-            constexpr int fc = decltype(FF)::value;
+        if constexpr (rt_face) {
+            // rhs -= sum_gp F phi_k w |e|/2 / |J| with the face's basis values from shared memory (a value
+            // that is zero on this face but not on another subtracts a zero product: the sum is unchanged)
+            const Real* __restrict__ cf = sfphi + f * ND * NG;
             sfor<0, NG>([&](auto GP) {
                 constexpr int gp = decltype(GP)::value;
                 const Real wsJ = (Real)MT<P>::gw(gp) * sJe;
@@ -1230,20 +1287,42 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                 for (int v = 0; v < 3; ++v) T[v] = F[v][gp] * wsJ;
                 sfor<0, ND>([&](auto K) {
                     constexpr int k = decltype(K)::value;
-                    constexpr double c = MT<P>::fphi((fc * ND + k) * NG + gp);
-                    if constexpr (c != 0.0) {
+                    constexpr bool used = MT<P>::fphi((0 * ND + k) * NG + gp) != 0.0 ||
+                                          MT<P>::fphi((1 * ND + k) * NG + gp) != 0.0 ||
+                                          MT<P>::fphi((2 * ND + k) * NG + gp) != 0.0;
+                    if constexpr (used) {
+                        const Real c = cf[k * NG + gp];
 #pragma unroll
-                        for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * (Real)c;
+                        for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * c;
                     }
                 });
             });
-        };
-        if (f == 0)
-            contrib(IC<0>{});
-        else if (f == 1)
-            contrib(IC<1>{});
-        else
-            contrib(IC<2>{});
+        } else {
+            auto contrib = [&](auto FF) {
+                constexpr int fc = decltype(FF)::value;
+                sfor<0, NG>([&](auto GP) {
+                    constexpr int gp = decltype(GP)::value;
+                    const Real wsJ = (Real)MT<P>::gw(gp) * sJe;
+                    Real T[3];
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) T[v] = F[v][gp] * wsJ;
+                    sfor<0, ND>([&](auto K) {
+                        constexpr int k = decltype(K)::value;
+                        constexpr double c = MT<P>::fphi((fc * ND + k) * NG + gp);
+                        if constexpr (c != 0.0) {
+#pragma unroll
+                            for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * (Real)c;
+                        }
+                    });
+                });
+            };
+            if (f == 0)
+                contrib(IC<0>{});
+            else if (f == 1)
+                contrib(IC<1>{});
+            else
+                contrib(IC<2>{});
+        }
     }
     // M^-1 (the diagonal master mass inverse; 1 / |J| is already in) and the SSP-RK stage combination
     const double bdt_s = A.bdt[A.nterms - 1];
