@@ -900,8 +900,22 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
 #pragma unroll
                     for (int v = 0; v < 3; ++v) Fx[v] = sp * Fx[v];
                 }
-                // bathymetry-slope source, swe_source.hpp:15-21 (the analytic source follows in its own loop)
+                // bathymetry-slope source, swe_source.hpp:15-21 (the analytic source follows in its own loop,
+                // except the manufactured sine set in FP32, added here: its sum then shares the phi w products)
                 Real S[3] = {Real(0), g * (dbx * qg[0]), g * (dby * qg[0])};
+                if constexpr (FSRC && sizeof(Real) == 4) {
+                    if (sine_set) {
+                        constexpr double s0 = MT<P>::psi(0 * NQ + gp), s1 = MT<P>::psi(1 * NQ + gp),
+                                         s2 = MT<P>::psi(2 * NQ + gp);
+                        const Real xg = (Real)x0 * (Real)s0 + (Real)x1 * (Real)s1 + (Real)x2 * (Real)s2;
+                        const Real yg = (Real)y0 * (Real)s0 + (Real)y1 * (Real)s1 + (Real)y2 * (Real)s2;
+                        Real fs[3];
+                        sine_src_eval<Real>(SS, xg, yg, fs);
+                        S[0] = fs[0];
+                        S[1] += fs[1];
+                        S[2] += fs[2];
+                    }
+                }
                 // bottom friction, swe_source.hpp:29-51: S(qx, qy) -= Cf |u| / h (qx, qy), Cf the Chezy
                 // coefficient or, for Manning, max(g n^2 / h^(1/3), Cf); |u| as sqrt(u^2 + v^2) and / h as
                 // * (1 / h) where the reference has hypot and a division (each within an ulp; velocities
@@ -969,7 +983,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                     });
                 }
             }
-            if (FSRC && !near) {
+            if (FSRC && !near && !(sizeof(Real) == 4 && sine_set)) {
                 const Real xr0 = (Real)x0, xr1 = (Real)x1, xr2 = (Real)x2;
                 const Real yr0 = (Real)y0, yr1 = (Real)y1, yr2 = (Real)y2;
                 sfor<0, NQ>([&](auto GP) {
