@@ -1,5 +1,6 @@
 // Stage-kernel instantiations for polynomial order 2, FP32 arithmetic with the intermediate stage states
-// kept as FP32 increments from the FP64 carried state (both register budgets; compiled as a separate unit).
+// kept as FP32 increments from a carried state held as two FP32 parts (both register budgets; compiled as a
+// separate unit).
 #include "stage_kernel.cuh"
 
 namespace dgsw {
