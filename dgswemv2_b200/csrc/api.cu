@@ -157,6 +157,10 @@ struct dgsw_rkdg_s {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    // graphs of GRAPH_MULTI consecutive steps, same keys (for batches of many steps: one graph launch, and
+    // no gap between graphs, per GRAPH_MULTI steps; small meshes are launch-bound)
+    cudaGraphExec_t graph_multi[4] = {nullptr, nullptr, nullptr, nullptr};
+    int64_t graph_multi_launches[4] = {0, 0, 0, 0};
     int qswap = 0;  // parity of the q_0 <-> q_ns swaps so far
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // per-launch timing of the stage kernel (dgsw_rkdg_step_timed): event pairs, recorded while kt_on
@@ -195,6 +199,9 @@ struct dgsw_rkdg_s {
 };
 
 namespace {
+
+// steps per multi-step graph
+constexpr int GRAPH_MULTI = 8;
 
 template <typename Real>
 void fill_stage_args(dgsw_rkdg_s* h, int s, StageArgs<Real>& A) {
@@ -539,11 +546,16 @@ int check_status(dgsw_rkdg_s* h) {
 }
 
 void destroy_graphs(dgsw_rkdg_s* h) {
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i) {
         if (h->graph[i]) {
             cudaGraphExecDestroy(h->graph[i]);
             h->graph[i] = nullptr;
         }
+        if (h->graph_multi[i]) {
+            cudaGraphExecDestroy(h->graph_multi[i]);
+            h->graph_multi[i] = nullptr;
+        }
+    }
 }
 
 int ensure_staging(dgsw_rkdg_s* h) {
@@ -1738,46 +1750,52 @@ int32_t dgsw_rkdg_step(dgsw_handle h, int32_t nsteps) {
         advance_host_stepper(h);
         if (h->stage == 0) --nsteps;
     }
-    for (int32_t n = 0; n < nsteps; ++n) {
+    for (int32_t n = 0; n < nsteps;) {
         // a captured step bakes in the buffer pointers: key the graphs by the parity of the
         // q_0 <-> q_ns swaps and by which wet-flag buffer is current
         const int key = h->qswap + 2 * h->wet_cur;
         if (h->cfg.use_graphs) {
-            if (!h->graph[key]) {
+            const int m = nsteps - n >= GRAPH_MULTI ? GRAPH_MULTI : 1;  // steps in this graph
+            cudaGraphExec_t& gx = m > 1 ? h->graph_multi[key] : h->graph[key];
+            int64_t& gl = m > 1 ? h->graph_multi_launches[key] : h->graph_launches[key];
+            if (!gx) {
                 cudaGraph_t g;
                 std::vector<void*> Qsave = h->Q;
                 const int wsave = h->wet_cur, qsave = h->qswap;
                 CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
                 int64_t l2 = 0;
                 cudaError_t ce = cudaSuccess;
-                for (int s = 0; s < h->ns && ce == cudaSuccess; ++s) ce = enqueue_stage(h, s, l2);
+                for (int s = 0; s < m * h->ns && ce == cudaSuccess; ++s) ce = enqueue_stage(h, s % h->ns, l2);
                 cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
                 h->Q = Qsave;
                 h->wet_cur = wsave;
                 h->qswap = qsave;
                 if (ce != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
                 if (ee != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("capture end: ") + cudaGetErrorString(ee));
-                CUDA_TRY(cudaGraphInstantiate(&h->graph[key], g, 0));
+                CUDA_TRY(cudaGraphInstantiate(&gx, g, 0));
                 cudaGraphDestroy(g);
-                h->graph_launches[key] = l2;
+                gl = l2;
             }
-            CUDA_TRY(cudaGraphLaunch(h->graph[key], h->stream));
-            launches += h->graph_launches[key];
-            // replay the host-side buffer rotation of one step
-            for (int s = 0; s < h->ns; ++s) {
+            CUDA_TRY(cudaGraphLaunch(gx, h->stream));
+            launches += gl;
+            // replay the host-side buffer rotation of the graph's steps
+            for (int s = 0; s < m * h->ns; ++s) {
                 h->wet_cur = 1 - h->wet_cur;
-                if (s + 1 == h->ns) {
+                if ((s + 1) % h->ns == 0) {
                     std::swap(h->Q[0], h->Q[h->ns]);
                     h->qswap ^= 1;
                 }
             }
+            for (int s = 0; s < m * h->ns; ++s) advance_host_stepper(h);
+            n += m;
         } else {
             for (int s = 0; s < h->ns; ++s) {
                 cudaError_t e = enqueue_stage(h, s, launches);
                 if (e != cudaSuccess) return fail(DGSW_ERR_CUDA, std::string("stage: ") + cudaGetErrorString(e));
             }
+            for (int s = 0; s < h->ns; ++s) advance_host_stepper(h);
+            ++n;
         }
-        for (int s = 0; s < h->ns; ++s) advance_host_stepper(h);
     }
     CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
     int rc = check_status(h);
