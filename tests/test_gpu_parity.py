@@ -195,6 +195,43 @@ def test_fp32_stage_increments(p, rk, tile):
     assert rel_err(R.get_state(), A.get_state()) <= 1e-6
 
 
+def test_fp32_stage_increments_behind_the_host_api():
+    """Every host-API read of a state in the middle of a step forms it from the stage increments, and every
+    write splits it again: after one stage of step 41 the handle with stage increments and the one with
+    FP64 stage states agree on the mass (the current stage's state), the L2 error (the carried state), the
+    writers' values and the state copied device to device, within the FP32 path's rounding; a state
+    written device to device mid-step reads back unchanged up to the increment's FP32 rounding."""
+    import torch
+
+    mesh, cfg = configs.manufactured(16, p=2, rk=(3, 3), dt=2.0, jitter=0.2, precision="fp32")
+    A = Problem(cfg, mesh)
+    B = Problem(cfg, mesh, fp64_stages=True)
+    assert A.info.stage_increments == 1 and B.info.stage_increments == 0
+    for P in (A, B):
+        P.step_serial(40)
+        P.stage_serial()
+    assert A.time() == B.time() and A.time()[2] == 1
+    assert abs(A.mass() - B.mass()) <= 1e-7 * abs(B.mass())
+    la, lb = A.compute_residual_L2(), B.compute_residual_L2()
+    assert abs(la - lb) <= 1e-4 * lb, (la, lb)
+    pa, ca, _, _ = A.postprocess()
+    pb, cb, _, _ = B.postprocess()
+    assert np.abs(pa - pb).max() <= 1e-5 * np.abs(pb).max()
+    assert np.abs(ca - cb).max() <= 1e-5 * np.abs(cb).max()
+    d = torch.empty((A.ne, 3, A.nd), dtype=torch.float64, device="cuda")
+    A.get_state_device(d.data_ptr())
+    torch.cuda.synchronize()
+    qa = d.cpu().numpy()
+    assert rel_err(qa, A.get_state()) == 0.0
+    assert rel_err(qa, B.get_state()) <= 1e-5
+    A.set_state_device(d.data_ptr())
+    torch.cuda.synchronize()
+    assert rel_err(A.get_state(), qa) <= 1e-7
+    A.step_serial(5)
+    B.step_serial(5)
+    assert rel_err(A.get_state(), B.get_state()) <= 1e-5
+
+
 def test_fp32_l2_on_a_limited_p2_run():
     """FP32 at equal L2 on a limited p = 2 run: the config-2 discretisation (manufactured solution, p = 2,
     SSP-RK3, jittered) at 32 x 32 quads with the Cockburn-Shu limiter (M = 1e-8), 500 steps of dt = 2 s. The
