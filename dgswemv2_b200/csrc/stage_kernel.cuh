@@ -44,6 +44,23 @@ __device__ __forceinline__ void sfor(F&& f) {
     }
 }
 
+// packed FP32 arithmetic of sm_100 (one FFMA2 issue for two FMAs): a0 += x0 c0 and a1 += x1 c1. Each lane is
+// an IEEE fma with the scalar fma's rounding. The kernels pair variables (ze with qx; qy with the bathymetry
+// or alone) so that both lanes share one coefficient. Z0 / Z1 mark terms whose coefficient is a compile-time
+// zero; they are left out, as the scalar loops leave them out.
+template <bool Z0 = false, bool Z1 = false>
+__device__ __forceinline__ void fma_pair(float& a0, float& a1, float x0, float x1, float c0, float c1) {
+    if constexpr (!Z0 && !Z1) {
+        const float2 r = __ffma2_rn(make_float2(x0, x1), make_float2(c0, c1), make_float2(a0, a1));
+        a0 = r.x;
+        a1 = r.y;
+    } else if constexpr (!Z0) {
+        a0 = __fmaf_rn(x0, c0, a0);
+    } else if constexpr (!Z1) {
+        a1 = __fmaf_rn(x1, c1, a1);
+    }
+}
+
 // NaN scrutiny (scrutinize_solution after every stage, rkdg_swe_proc_serial_step.hpp:59-65): the reference
 // stops at the first stage whose state holds a NaN and reports the first element (ascending ID) there.
 // nan_key = (stage counter << 32) | reference element index, stage counter = step * stages + stage, kept
@@ -492,10 +509,30 @@ using MT = ct::Master<P>;
 
 // trace of an element's face F at the edge Gauss points: ze, qx, qy and bathymetry,
 // sum over the modes in ascending order (same arithmetic for tile and halo elements)
-template <int P, int F, typename Real>
+template <int P, int F, typename Real, bool PK = false>
 __device__ __forceinline__ void face_trace(const Real (&q)[3][MT<P>::ND], const Real (&b)[3],
                                            Real (&t)[4][MT<P>::NG]) {
     constexpr int ND = MT<P>::ND, NG = MT<P>::NG;
+    if constexpr (PK) {
+        // packed FP32: (ze, qx) and (qy, bathymetry) share each mode's coefficient
+        sfor<0, NG>([&](auto G) {
+            constexpr int g = decltype(G)::value;
+            Real s0 = Real(0), s1 = Real(0), s2 = Real(0), sb = Real(0);
+            sfor<0, ND>([&](auto K) {
+                constexpr int k = decltype(K)::value;
+                constexpr double c = MT<P>::fphi((F * ND + k) * NG + g);
+                if constexpr (c != 0.0) {
+                    fma_pair(s0, s1, q[0][k], q[1][k], (Real)c, (Real)c);
+                    if constexpr (k < 3)
+                        fma_pair(s2, sb, q[2][k], b[k], (Real)c, (Real)c);
+                    else
+                        s2 = __fmaf_rn(q[2][k], (Real)c, s2);
+                }
+            });
+            t[0][g] = s0, t[1][g] = s1, t[2][g] = s2, t[3][g] = sb;
+        });
+        return;
+    }
     sfor<0, NG>([&](auto G) {
         constexpr int g = decltype(G)::value;
         sfor<0, 3>([&](auto V) {
@@ -522,10 +559,32 @@ __device__ __forceinline__ void face_trace(const Real (&q)[3][MT<P>::ND], const 
 // the halo faces of a warp belong to different faces, and one compile-time copy per face would split the
 // warp. Entries that are zero on this face but not on another add a zero product (the sum is unchanged), so
 // the values equal face_trace's bit for bit.
-template <int P, typename Real>
+template <int P, typename Real, bool PK = false>
 __device__ __forceinline__ void face_trace_rt(const Real (&q)[3][MT<P>::ND], const Real (&b)[3], const Real* cf,
                                               Real (&t)[4][MT<P>::NG]) {
     constexpr int ND = MT<P>::ND, NG = MT<P>::NG;
+    if constexpr (PK) {
+        sfor<0, NG>([&](auto G) {
+            constexpr int g = decltype(G)::value;
+            Real s0 = Real(0), s1 = Real(0), s2 = Real(0), sb = Real(0);
+            sfor<0, ND>([&](auto K) {
+                constexpr int k = decltype(K)::value;
+                constexpr bool used = MT<P>::fphi((0 * ND + k) * NG + g) != 0.0 ||
+                                      MT<P>::fphi((1 * ND + k) * NG + g) != 0.0 ||
+                                      MT<P>::fphi((2 * ND + k) * NG + g) != 0.0;
+                if constexpr (used) {
+                    const Real c = cf[k * NG + g];
+                    fma_pair(s0, s1, q[0][k], q[1][k], c, c);
+                    if constexpr (k < 3)
+                        fma_pair(s2, sb, q[2][k], b[k], c, c);
+                    else
+                        s2 = __fmaf_rn(q[2][k], c, s2);
+                }
+            });
+            t[0][g] = s0, t[1][g] = s1, t[2][g] = s2, t[3][g] = sb;
+        });
+        return;
+    }
     sfor<0, NG>([&](auto G) {
         constexpr int g = decltype(G)::value;
         sfor<0, 3>([&](auto V) {
@@ -675,6 +734,11 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     // -0.6 to -0.9 %; FP64 at p = 2 -0.6 to +0.5 %, p = 1 +1 to +4 % (the shared-memory loads cost more than
     // the divergence there), so only FP32 at p = 2 uses it
     constexpr bool rt_face = P == 2 && sizeof(Real) == 4;
+    // packed FP32 FMAs (fma_pair) in the Gauss-point state evaluation, the face traces, the volume integral and
+    // the lift. Measured per step against the scalar FMAs: config 2 -4.5 %, the tidal channel -3.6 % (p = 2)
+    // and -2 % (p = 1); warp instructions per config-2 stage -8 %. With wetting/drying (p = 1 bowl) the
+    // scalar form stays: packed, the bowl step took 6 % longer.
+    constexpr bool packed = sizeof(Real) == 4 && !WD;
     __shared__ Real sfphi[3 * ND * NG];
     if (rt_face && threadIdx.x < 3 * ND * NG) {
         Real c = Real(0);
@@ -866,22 +930,38 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
             sfor<0, NQ>([&](auto GP) {
                 constexpr int gp = decltype(GP)::value;
                 Real qg[3];
-                sfor<0, 3>([&](auto V) {
-                    constexpr int v = decltype(V)::value;
-                    Real s = Real(0);
+                Real bg = Real(0);
+                if constexpr (packed) {
+                    // packed FP32: (ze, qx) and (qy, bathymetry) share each mode's coefficient
+                    qg[0] = qg[1] = qg[2] = Real(0);
                     sfor<0, ND>([&](auto K) {
                         constexpr int k = decltype(K)::value;
                         constexpr double c = MT<P>::phi(k * NQ + gp);
-                        if constexpr (c != 0.0) s += q[v][k] * (Real)c;
+                        if constexpr (c != 0.0) {
+                            fma_pair(qg[0], qg[1], q[0][k], q[1][k], (Real)c, (Real)c);
+                            if constexpr (k < 3)
+                                fma_pair(qg[2], bg, q[2][k], b[k], (Real)c, (Real)c);
+                            else
+                                qg[2] = __fmaf_rn(q[2][k], (Real)c, qg[2]);
+                        }
                     });
-                    qg[v] = s;
-                });
-                Real bg = Real(0);
-                sfor<0, 3>([&](auto K) {
-                    constexpr int k = decltype(K)::value;
-                    constexpr double c = MT<P>::phi(k * NQ + gp);
-                    if constexpr (c != 0.0) bg += b[k] * (Real)c;
-                });
+                } else {
+                    sfor<0, 3>([&](auto V) {
+                        constexpr int v = decltype(V)::value;
+                        Real s = Real(0);
+                        sfor<0, ND>([&](auto K) {
+                            constexpr int k = decltype(K)::value;
+                            constexpr double c = MT<P>::phi(k * NQ + gp);
+                            if constexpr (c != 0.0) s += q[v][k] * (Real)c;
+                        });
+                        qg[v] = s;
+                    });
+                    sfor<0, 3>([&](auto K) {
+                        constexpr int k = decltype(K)::value;
+                        constexpr double c = MT<P>::phi(k * NQ + gp);
+                        if constexpr (c != 0.0) bg += b[k] * (Real)c;
+                    });
+                }
                 // physical flux, swe_flux.hpp:5-25
                 const Real h = qg[0] + bg;
                 const Real ih = Real(1) / h;
@@ -928,6 +1008,35 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                     S[2] -= tau * qg[2];
                 }
                 // int F . grad(phi) = sum_gp sum_z (F_x J^-1(z,x) + F_y J^-1(z,y)) dphi_z w
+                if constexpr (packed) {
+                    // packed FP32: ze and qx share each mode's coefficients (qy alone), each mode's terms in the
+                    // scalar loop's order
+                    Real G0[3], G1[3];
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) {
+                        G0[v] = Fx[v] * Ji00 + Fy[v] * Ji01;
+                        G1[v] = Fx[v] * Ji10 + Fy[v] * Ji11;
+                    }
+                    sfor<0, ND>([&](auto K) {
+                        constexpr int k = decltype(K)::value;
+                        constexpr double m0 = MT<P>::mz((0 * NQ + gp) * ND + k);
+                        constexpr double m1 = MT<P>::mz((1 * NQ + gp) * ND + k);
+                        constexpr double pw = MT<P>::phiw(gp * ND + k);
+                        if constexpr (m0 != 0.0) {
+                            fma_pair(rhs[0][k], rhs[1][k], G0[0], G0[1], (Real)m0, (Real)m0);
+                            rhs[2][k] = __fmaf_rn(G0[2], (Real)m0, rhs[2][k]);
+                        }
+                        if constexpr (m1 != 0.0) {
+                            fma_pair(rhs[0][k], rhs[1][k], G1[0], G1[1], (Real)m1, (Real)m1);
+                            rhs[2][k] = __fmaf_rn(G1[2], (Real)m1, rhs[2][k]);
+                        }
+                        if constexpr (pw != 0.0) {
+                            fma_pair(rhs[0][k], rhs[1][k], S[0], S[1], (Real)pw, (Real)pw);
+                            rhs[2][k] = __fmaf_rn(S[2], (Real)pw, rhs[2][k]);
+                        }
+                    });
+                    return;
+                }
                 sfor<0, 3>([&](auto V) {
                     constexpr int v = decltype(V)::value;
                     const Real G0 = Fx[v] * Ji00 + Fy[v] * Ji01;
@@ -1022,7 +1131,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
         sfor<0, 3>([&](auto FF) {
             constexpr int f = decltype(FF)::value;
             Real t[4][NG];
-            face_trace<P, f, Real>(q, b, t);
+            face_trace<P, f, Real, packed>(q, b, t);
             const int slot = 3 * tid + f;
 #pragma unroll
             for (int c = 0; c < 4; ++c)
@@ -1054,13 +1163,13 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
 #pragma unroll
             for (int k = 0; k < 3; ++k) b[k] = shb[k * max_halo + h];
             if constexpr (rt_face) {
-                face_trace_rt<P, Real>(q, b, sfphi + hrec.y * ND * NG, t);
+                face_trace_rt<P, Real, packed>(q, b, sfphi + hrec.y * ND * NG, t);
             } else if (hrec.y == 0) {
-                face_trace<P, 0, Real>(q, b, t);
+                face_trace<P, 0, Real, packed>(q, b, t);
             } else if (hrec.y == 1) {
-                face_trace<P, 1, Real>(q, b, t);
+                face_trace<P, 1, Real, packed>(q, b, t);
             } else {
-                face_trace<P, 2, Real>(q, b, t);
+                face_trace<P, 2, Real, packed>(q, b, t);
             }
             const int slot = 3 * TILE + h;
 #pragma unroll
@@ -1079,13 +1188,13 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
 #pragma unroll
             for (int k = 0; k < 3; ++k) b[k] = A.bath[k * P_ + e];
             if constexpr (rt_face) {
-                face_trace_rt<P, Real>(q, b, sfphi + it.y * ND * NG, t);
+                face_trace_rt<P, Real, packed>(q, b, sfphi + it.y * ND * NG, t);
             } else if (it.y == 0) {
-                face_trace<P, 0, Real>(q, b, t);
+                face_trace<P, 0, Real, packed>(q, b, t);
             } else if (it.y == 1) {
-                face_trace<P, 1, Real>(q, b, t);
+                face_trace<P, 1, Real, packed>(q, b, t);
             } else {
-                face_trace<P, 2, Real>(q, b, t);
+                face_trace<P, 2, Real, packed>(q, b, t);
             }
             const int slot = 3 * TILE + h;
 #pragma unroll
@@ -1306,8 +1415,14 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                                           MT<P>::fphi((2 * ND + k) * NG + gp) != 0.0;
                     if constexpr (used) {
                         const Real c = cf[k * NG + gp];
+                        if constexpr (packed) {
+                            // packed FP32: ze and qx share the coefficient (qy alone), as fma(-T, c, rhs)
+                            fma_pair(rhs[0][k], rhs[1][k], -T[0], -T[1], c, c);
+                            rhs[2][k] = __fmaf_rn(-T[2], c, rhs[2][k]);
+                        } else {
 #pragma unroll
-                        for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * c;
+                            for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * c;
+                        }
                     }
                 });
             });
@@ -1324,6 +1439,12 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                         constexpr int k = decltype(K)::value;
                         constexpr double c = MT<P>::fphi((fc * ND + k) * NG + gp);
                         if constexpr (c != 0.0) {
+                            if constexpr (packed) {
+                                // packed FP32: ze and qx share the coefficient (qy alone), as fma(-T, c, rhs)
+                                fma_pair(rhs[0][k], rhs[1][k], -T[0], -T[1], (Real)c, (Real)c);
+                                rhs[2][k] = __fmaf_rn(-T[2], (Real)c, rhs[2][k]);
+                                return;
+                            }
 #pragma unroll
                             for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * (Real)c;
                         }
