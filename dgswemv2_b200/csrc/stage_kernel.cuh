@@ -778,10 +778,18 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                 for (int v = 0; v < 3; ++v)
 #pragma unroll
                     for (int k = 0; k < ND; ++k) t[v][k] = dj[(v * ND + k) * P_ + d];
+                if constexpr (packed) {
 #pragma unroll
-                for (int v = 0; v < 3; ++v)
+                    for (int k = 0; k < ND; ++k) {
+                        fma_pair(dcomb[0][k], dcomb[1][k], t[0][k], t[1][k], aj, aj);
+                        dcomb[2][k] = __fmaf_rn(t[2][k], aj, dcomb[2][k]);
+                    }
+                } else {
 #pragma unroll
-                    for (int k = 0; k < ND; ++k) dcomb[v][k] += aj * t[v][k];
+                    for (int v = 0; v < 3; ++v)
+#pragma unroll
+                        for (int k = 0; k < ND; ++k) dcomb[v][k] += aj * t[v][k];
+                }
             }
             if (j < A.nterms - 1 && A.bdt[j] != 0.0) {
                 const Real* __restrict__ sj = A.dsolk[j];
@@ -791,10 +799,18 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                 for (int v = 0; v < 3; ++v)
 #pragma unroll
                     for (int k = 0; k < ND; ++k) u[v][k] = sj[(v * ND + k) * P_ + d];
+                if constexpr (packed) {
 #pragma unroll
-                for (int v = 0; v < 3; ++v)
+                    for (int k = 0; k < ND; ++k) {
+                        fma_pair(dcomb[0][k], dcomb[1][k], u[0][k], u[1][k], bj, bj);
+                        dcomb[2][k] = __fmaf_rn(u[2][k], bj, dcomb[2][k]);
+                    }
+                } else {
 #pragma unroll
-                    for (int k = 0; k < ND; ++k) dcomb[v][k] += bj * u[v][k];
+                    for (int v = 0; v < 3; ++v)
+#pragma unroll
+                        for (int k = 0; k < ND; ++k) dcomb[v][k] += bj * u[v][k];
+                }
             }
         }
     };
@@ -1463,16 +1479,19 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     const double bdt_s = A.bdt[A.nterms - 1];
     if constexpr (SPLIT) {
         const Real bs = (Real)bdt_s;
-        Real dn[3][ND];
+        // dn = dcomb + dt b_s (rhs M^-1), ze and qx packed (each lane the scalar mul and fma)
+        Real (&dn)[3][ND] = dcomb;
         sfor<0, ND>([&](auto K) {
             constexpr int k = decltype(K)::value;
             const Real mk = (Real)MT<P>::minv(k);
+            const float2 s01 = __fmul2_rn(make_float2(rhs[0][k], rhs[1][k]), make_float2(mk, mk));
+            const Real sol[3] = {s01.x, s01.y, rhs[2][k] * mk};
+            if (A.store_sol) {
 #pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                const Real sol = rhs[v][k] * mk;
-                if (A.store_sol) A.dsol_out[(v * ND + k) * P_ + d] = sol;
-                dn[v][k] = dcomb[v][k] + bs * sol;
+                for (int v = 0; v < 3; ++v) A.dsol_out[(v * ND + k) * P_ + d] = sol[v];
             }
+            fma_pair(dn[0][k], dn[1][k], sol[0], sol[1], bs, bs);
+            dn[2][k] = __fmaf_rn(sol[2], bs, dn[2][k]);
         });
         bool has_nan = false;
         if (A.last) {
