@@ -183,6 +183,31 @@ __device__ __forceinline__ void llf_flux(Real gravity, const Real qin[3], const 
     F[2] = Real(0.5) * (f2 + e2 + lam * (qin[2] - qex[2]));
 }
 
+// the same flux in packed FP32 (FFMA2 / FMUL2 / FADD2): the in side in lane x, the ex side in lane y, each
+// lane the scalar formula above with its terms in the same order (sp on the in lane only)
+__device__ __forceinline__ void llf_flux_packed(float gravity, const float qin[3], const float qex[3], float bath,
+                                                float sp, float nx, float ny, float F[3]) {
+    const float2 q0 = make_float2(qin[0], qex[0]), q1 = make_float2(qin[1], qex[1]), q2 = make_float2(qin[2], qex[2]);
+    const float2 N = make_float2(nx, nx), M = make_float2(ny, ny), B = make_float2(bath, bath);
+    const float2 h = __fadd2_rn(q0, B);
+    const float2 ih = make_float2(1.0f / h.x, 1.0f / h.y);
+    const float2 u = __fmul2_rn(q1, ih), v = __fmul2_rn(q2, ih);
+    const float2 un = __ffma2_rn(v, M, __fmul2_rn(u, N));
+    const float spc = (nx * sp) * (nx * sp) + ny * ny;
+    const float2 gh = __fmul2_rn(make_float2(gravity, gravity), h);
+    const float lam = fmaxf(fabsf(un.x) + sqrtf(gh.x * spc), fabsf(un.y) + sqrtf(gh.y * spc));
+    const float2 pe = __fmul2_rn(make_float2(gravity, gravity),
+                                 __ffma2_rn(q0, B, __fmul2_rn(__fmul2_rn(q0, q0), make_float2(0.5f, 0.5f))));
+    const float2 uuh = __fmul2_rn(u, q1), vvh = __fmul2_rn(v, q2), uvh = __fmul2_rn(u, q2);
+    const float2 spv = make_float2(sp, 1.0f);
+    const float2 f0 = __ffma2_rn(q2, M, __fmul2_rn(__fmul2_rn(spv, q1), N));
+    const float2 f1 = __ffma2_rn(uvh, M, __fmul2_rn(__fmul2_rn(spv, __fadd2_rn(uuh, pe)), N));
+    const float2 f2 = __ffma2_rn(__fadd2_rn(vvh, pe), M, __fmul2_rn(__fmul2_rn(spv, uvh), N));
+    F[0] = 0.5f * (f0.x + f0.y + lam * (qin[0] - qex[0]));
+    F[1] = 0.5f * (f1.x + f1.y + lam * (qin[1] - qex[1]));
+    F[2] = 0.5f * (f2.x + f2.y + lam * (qin[2] - qex[2]));
+}
+
 // land boundary ghost state (normal momentum mirrored) + LLF, rkdg_swe_bc_land.hpp:68-86
 template <typename Real>
 __device__ __forceinline__ void land_flux(Real g, Real nx, Real ny, const Real qin[3], Real bath, Real sp, Real F[3]) {
@@ -705,7 +730,28 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
     using SM = Smem<P, Real, WD>;
     const int NS = SM::nslot(TILE, max_halo);  // trace slots: 3 per tile element, then halo faces
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real* str = reinterpret_cast<Real*>(smem_raw + SM::off_tr(TILE));               // [4*NG][NS]
+    // trace slots: FP32 at p = 2 [NS][NG][ze, qx, qy, b], one 16-byte shared access per Gauss point (a slot is
+    // 36 words, so the 8 threads of a quarter-warp that write consecutive slots hit distinct banks);
+    // otherwise [4*NG][NS]. Measured per step against [4*NG][NS] (same bits): config 2 -1.9 %, tidal p = 2
+    // -1.4 %; at p = 1 (24-word slots, two-way bank conflicts) +1.3 to +1.5 %, so p = 1 keeps the old layout
+    Real* str = reinterpret_cast<Real*>(smem_raw + SM::off_tr(TILE));
+    constexpr bool tr_vec = sizeof(Real) == 4 && P == 2;
+    auto tr_at = [&](int c, int gp, int slot) -> Real& {
+        return tr_vec ? str[(slot * NG + gp) * 4 + c] : str[(c * NG + gp) * NS + slot];
+    };
+    // a face's traces into its slot
+    auto put_trace = [&](int slot, const Real (&t)[4][NG]) {
+        if constexpr (tr_vec) {
+#pragma unroll
+            for (int gg = 0; gg < NG; ++gg)
+                *reinterpret_cast<float4*>(str + (slot * NG + gg) * 4) = make_float4(t[0][gg], t[1][gg], t[2][gg], t[3][gg]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int gg = 0; gg < NG; ++gg) str[(c * NG + gg) * NS + slot] = t[c][gg];
+        }
+    };
     Real* sF = reinterpret_cast<Real*>(smem_raw + SM::off_F(TILE, max_halo));       // [NFC][max_edges]
     Real* ssJ = reinterpret_cast<Real*>(smem_raw + SM::off_sJ(TILE, max_halo, max_edges));
     unsigned char* swet = smem_raw + SM::off_wet(TILE, max_halo, max_edges);        // [NS]
@@ -1149,10 +1195,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
             Real t[4][NG];
             face_trace<P, f, Real, packed>(q, b, t);
             const int slot = 3 * tid + f;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-#pragma unroll
-                for (int gg = 0; gg < NG; ++gg) str[(c * NG + gg) * NS + slot] = t[c][gg];
+            put_trace(slot, t);
             swet[slot] = wet ? 1 : 0;
         });
     }
@@ -1188,10 +1231,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                 face_trace<P, 2, Real, packed>(q, b, t);
             }
             const int slot = 3 * TILE + h;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-#pragma unroll
-                for (int gg = 0; gg < NG; ++gg) str[(c * NG + gg) * NS + slot] = t[c][gg];
+            put_trace(slot, t);
             swet[slot] = hwet ? 1 : 0;
         }
     } else {
@@ -1213,10 +1253,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                 face_trace<P, 2, Real, packed>(q, b, t);
             }
             const int slot = 3 * TILE + h;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-#pragma unroll
-                for (int gg = 0; gg < NG; ++gg) str[(c * NG + gg) * NS + slot] = t[c][gg];
+            put_trace(slot, t);
             swet[slot] = A.wet_in[e] != 0 ? 1 : 0;
         }
     }
@@ -1272,7 +1309,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
 #pragma unroll
                 for (int c = 0; c < 3 * NG; ++c) sF[c * max_edges + le] = (Real)Fl[c];
 #pragma unroll
-                for (int c = 0; c < 3 * NG; ++c) str[c * NS + sb] = (Real)Fl[3 * NG + c];
+                for (int c = 0; c < 3 * NG; ++c) tr_at(c / NG, c % NG, sb) = (Real)Fl[3 * NG + c];
                 continue;
             }
             Real sp = Real(1);
@@ -1290,15 +1327,26 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                 // BoundaryToMasterCoordinates + LocalToGlobalCoordinates on a straight edge
                 constexpr double wa_ = MT<P>::fpsi((0 * 3 + 1) * NG + gp), wb_ = MT<P>::fpsi((0 * 3 + 2) * NG + gp);
                 if (A.spherical) sp = (Real)(A.sp_cos_lat0 / cos((ya * wa_ + yb * wb_) / A.sp_R));
-                const Real qi[3] = {str[(0 * NG + gp) * NS + sa], str[(1 * NG + gp) * NS + sa],
-                                    str[(2 * NG + gp) * NS + sa]};
-                const Real bi = str[(3 * NG + gp) * NS + sa];
+                Real qi[3], bi;
+                if constexpr (tr_vec) {
+                    const float4 a = *reinterpret_cast<const float4*>(str + (sa * NG + gp) * 4);
+                    qi[0] = a.x, qi[1] = a.y, qi[2] = a.z, bi = a.w;
+                } else {
+                    qi[0] = str[(0 * NG + gp) * NS + sa], qi[1] = str[(1 * NG + gp) * NS + sa];
+                    qi[2] = str[(2 * NG + gp) * NS + sa], bi = str[(3 * NG + gp) * NS + sa];
+                }
                 Real qe[3], be = Real(0);
                 if (kind == 0) {
-                    qe[0] = str[(0 * NG + ge) * NS + sb];
-                    qe[1] = str[(1 * NG + ge) * NS + sb];
-                    qe[2] = str[(2 * NG + ge) * NS + sb];
-                    if (WD) be = str[(3 * NG + ge) * NS + sb];
+                    if constexpr (tr_vec) {
+                        const float4 e = *reinterpret_cast<const float4*>(str + (sb * NG + ge) * 4);
+                        qe[0] = e.x, qe[1] = e.y, qe[2] = e.z;
+                        if (WD) be = e.w;
+                    } else {
+                        qe[0] = str[(0 * NG + ge) * NS + sb];
+                        qe[1] = str[(1 * NG + ge) * NS + sb];
+                        qe[2] = str[(2 * NG + ge) * NS + sb];
+                        if (WD) be = str[(3 * NG + ge) * NS + sb];
+                    }
                 } else if (kind == 1) {
                     // BC::Land ghost state: normal momentum mirrored (rkdg_swe_bc_land.hpp:44-56)
                     const Real tx = -ny, ty = nx;
@@ -1316,7 +1364,12 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                     qe[0] = r.v0, qe[1] = r.v1, qe[2] = r.v2;
                 }
                 Real Fi[3];
-                llf_flux<Real>(g, qi, qe, bi, sp, nx, ny, Fi);
+                // packed at p = 1 only: measured per step, the p = 1 tidal channel -1.7 %; at p = 2 the kernel
+                // spilled and the config-2 step took 2 % longer
+                if constexpr (packed && P == 1)
+                    llf_flux_packed(g, qi, qe, bi, sp, nx, ny, Fi);
+                else
+                    llf_flux<Real>(g, qi, qe, bi, sp, nx, ny, Fi);
                 if (WD && kind == 0) {
                     Real Fe[3] = {-Fi[0], -Fi[1], -Fi[2]};
                     if (!(wa && wb)) {
@@ -1406,7 +1459,7 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                 for (int v = 0; v < 3; ++v) F[v][gp] = sF[(v * NG + gp) * max_edges + slot];
             } else if (sfl == 2) {  // levee ex side: its own flux, left in its face's trace slot
 #pragma unroll
-                for (int v = 0; v < 3; ++v) F[v][gp] = str[(v * NG + (NG - 1 - gp)) * NS + 3 * tid + f];
+                for (int v = 0; v < 3; ++v) F[v][gp] = tr_at(v, NG - 1 - gp, 3 * tid + f);
             } else {
                 const int ga = NG - 1 - gp;
 #pragma unroll
