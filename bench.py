@@ -319,9 +319,10 @@ def run_reference(args):
 
 
 def autotuned(P):
-    """The autotuner's choice and its timed candidates (tile, occupancy, tile order, ms per step)."""
+    """The autotuner's choice and its timed candidates (tile, occupancy, tile order, ms per step; each the
+    faster of the capped and the run-time-stride kernel where the mesh fits the caps)."""
     return {"tile": P.info.tile, "occupancy": P.info.occupancy, "tile_order": P.info.tile_order,
-            "candidates": [list(c) for c in P.tuning()]}
+            "smem_capped": P.info.smem_capped, "candidates": [list(c) for c in P.tuning()]}
 
 
 def time_steps(P, K):

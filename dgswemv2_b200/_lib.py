@@ -165,7 +165,7 @@ class Info(C.Structure):
         ("occupancy", C.c_int32),
         ("tile_order", C.c_int32),
         ("stage_increments", C.c_int32),
-        ("pad_", C.c_int32),
+        ("smem_capped", C.c_int32),
     ]
 
 

@@ -1512,10 +1512,10 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
                                 // packed FP32: ze and qx share the coefficient (qy alone), as fma(-T, c, rhs)
                                 fma_pair(rhs[0][k], rhs[1][k], -T[0], -T[1], (Real)c, (Real)c);
                                 rhs[2][k] = __fmaf_rn(-T[2], (Real)c, rhs[2][k]);
-                                return;
-                            }
+                            } else {
 #pragma unroll
-                            for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * (Real)c;
+                                for (int v = 0; v < 3; ++v) rhs[v][k] -= T[v] * (Real)c;
+                            }
                         }
                     });
                 });
@@ -1636,6 +1636,8 @@ __global__ void __launch_bounds__(TILE, (MinBlocks<P, Real, TILE, WD, OCC>::valu
 // launchers, one translation unit per (order, precision, register budget); bit 3 of `mode` selects the
 // alternative budget (OCC = 1)
 constexpr int STAGE_MODE_OCC = 8;
+// bit 4 of `mode`: the kernel with run-time shared-memory strides even where the mesh fits the caps
+constexpr int STAGE_MODE_UNCAPPED = 16;
 cudaError_t launch_stage_p1_f64(const StageArgs<double>& A, int tile, int ntiles, int max_halo, int max_edges,
                                 int mode, cudaStream_t s);
 cudaError_t launch_stage_p1_f32(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
@@ -1658,9 +1660,19 @@ cudaError_t launch_stage_p1_f32_split(const StageArgs<float>& A, int tile, int n
 cudaError_t launch_stage_p2_f32_split(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
                                       int mode, cudaStream_t s);
 
+// whether every tile of a mesh fits the compile-time shared-memory capacities of the capped kernels
+inline bool stage_fits_caps(int tile, int max_halo, int max_edges) {
+    return tile == 128 ? max_halo <= TileCap<128>::halo && max_edges <= TileCap<128>::edges
+                       : max_halo <= TileCap<256>::halo && max_edges <= TileCap<256>::edges;
+}
+
+// with `allow_capped` false the kernel with run-time strides runs even where the mesh fits the caps: its
+// shared memory is sized to the mesh's largest tile, and with less shared memory per SM the L1 cache that
+// shares its storage is larger (the autotuner times both)
 template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int TILE, int OCC, bool SPLIT = false>
-cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo, int max_edges, cudaStream_t s) {
-    const bool capped = max_halo <= TileCap<TILE>::halo && max_edges <= TileCap<TILE>::edges;
+cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo, int max_edges, bool allow_capped,
+                              cudaStream_t s) {
+    const bool capped = allow_capped && max_halo <= TileCap<TILE>::halo && max_edges <= TileCap<TILE>::edges;
     auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, true, OCC, SPLIT>
                        : rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, false, OCC, SPLIT>;
     const size_t smem = capped ? Smem<P, Real, WD>::bytes(TILE, TileCap<TILE>::halo, TileCap<TILE>::edges)
@@ -1672,13 +1684,16 @@ cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo
 }
 
 template <int P, typename Real, bool WD, bool FSRC, bool FRIC, int OCC, bool SPLIT = false>
-cudaError_t launch_stage_tile(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges,
+cudaError_t launch_stage_tile(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges, int mode,
                               cudaStream_t s) {
+    const bool allow_capped = !(mode & STAGE_MODE_UNCAPPED);
     switch (tile) {
         case 128:
-            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 128, OCC, SPLIT>(A, ntiles, max_halo, max_edges, s);
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 128, OCC, SPLIT>(A, ntiles, max_halo, max_edges,
+                                                                                allow_capped, s);
         case 256:
-            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 256, OCC, SPLIT>(A, ntiles, max_halo, max_edges, s);
+            return launch_stage_impl<P, Real, WD, FSRC, FRIC, 256, OCC, SPLIT>(A, ntiles, max_halo, max_edges,
+                                                                                allow_capped, s);
         default:
             return cudaErrorInvalidValue;
     }
@@ -1689,14 +1704,14 @@ template <int P, typename Real, int OCC>
 cudaError_t launch_stage_dispatch(const StageArgs<Real>& A, int tile, int ntiles, int max_halo, int max_edges,
                                   int mode, cudaStream_t s) {
     switch (mode & 7) {
-        case 0: return launch_stage_tile<P, Real, false, false, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
-        case 1: return launch_stage_tile<P, Real, true, false, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
-        case 2: return launch_stage_tile<P, Real, false, true, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
-        case 3: return launch_stage_tile<P, Real, true, true, false, OCC>(A, tile, ntiles, max_halo, max_edges, s);
-        case 4: return launch_stage_tile<P, Real, false, false, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
-        case 5: return launch_stage_tile<P, Real, true, false, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
-        case 6: return launch_stage_tile<P, Real, false, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
-        default: return launch_stage_tile<P, Real, true, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, s);
+        case 0: return launch_stage_tile<P, Real, false, false, false, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 1: return launch_stage_tile<P, Real, true, false, false, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 2: return launch_stage_tile<P, Real, false, true, false, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 3: return launch_stage_tile<P, Real, true, true, false, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 4: return launch_stage_tile<P, Real, false, false, true, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 5: return launch_stage_tile<P, Real, true, false, true, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 6: return launch_stage_tile<P, Real, false, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        default: return launch_stage_tile<P, Real, true, true, true, OCC>(A, tile, ntiles, max_halo, max_edges, mode, s);
     }
 }
 
@@ -1706,10 +1721,10 @@ template <int P, int OCC>
 cudaError_t launch_stage_split_dispatch(const StageArgs<float>& A, int tile, int ntiles, int max_halo, int max_edges,
                                         int mode, cudaStream_t s) {
     switch (mode & 7) {
-        case 0: return launch_stage_tile<P, float, false, false, false, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
-        case 2: return launch_stage_tile<P, float, false, true, false, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
-        case 4: return launch_stage_tile<P, float, false, false, true, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
-        case 6: return launch_stage_tile<P, float, false, true, true, OCC, true>(A, tile, ntiles, max_halo, max_edges, s);
+        case 0: return launch_stage_tile<P, float, false, false, false, OCC, true>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 2: return launch_stage_tile<P, float, false, true, false, OCC, true>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 4: return launch_stage_tile<P, float, false, false, true, OCC, true>(A, tile, ntiles, max_halo, max_edges, mode, s);
+        case 6: return launch_stage_tile<P, float, false, true, true, OCC, true>(A, tile, ntiles, max_halo, max_edges, mode, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -75,6 +75,7 @@ def measure(name, precision, steps, warmup=5, graphs=True, tile=0, indicator=0, 
         "kernel_launches_per_step": launches / steps, "l2_error": P.compute_residual_L2(),
         "create_seconds": create_s, "occupancy": P.info.occupancy, "tile_order": P.info.tile_order,
         "graphs": graphs, "indicator": indicator, "stage_increments": P.info.stage_increments,
+        "smem_capped": P.info.smem_capped,
     }
 
 

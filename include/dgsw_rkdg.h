@@ -144,7 +144,9 @@ typedef struct {
     int64_t state_bytes;       /* bytes of one stage state array */
     int32_t occupancy, tile_order;  /* the stage kernel's register budget and tile order in use */
     int32_t stage_increments;  /* 1 when the intermediate stage states are FP32 increments (fp64_stages) */
-    int32_t pad_;
+    int32_t smem_capped;       /* 1 when the stage kernel's shared memory has the compile-time capacities;
+                                  0 when it is sized to the mesh's largest tile (the autotuner's choice, or a
+                                  tile beyond the capacities) */
 } dgsw_info;
 
 typedef struct dgsw_rkdg_s* dgsw_handle;
