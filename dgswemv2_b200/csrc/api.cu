@@ -1083,8 +1083,8 @@ static std::mutex g_tune_mutex;
 static std::map<std::string, TuneRecord> g_tune_cache;
 
 // One tile size of the autotuner: a handle built with that tile, then each (occupancy, tile order) pair
-// timed on it, 4 graph-replayed steps after 2 warm-up steps, from the initial state each time. Returns
-// the handle (in *keep, left at the last variant) or destroys it.
+// timed on it from the initial state: 2 warm-up steps, then graph-replayed steps worth about 2 ms (at
+// least 4). Returns the handle (in *keep, left at the last variant) or destroys it.
 
 static int32_t time_tile(const dgsw_config* cfg, const dgsw_mesh* mesh, const int32_t* group, int32_t ng,
                          const double* gp, int tile, std::vector<TuneRecord>& rec, dgsw_handle* keep) {
@@ -1093,18 +1093,27 @@ static int32_t time_tile(const dgsw_config* cfg, const dgsw_mesh* mesh, const in
     dgsw_handle h = nullptr;
     int32_t rc = create_impl(&c, mesh, group, ng, gp, &h);
     if (rc) return rc;
-    const int warm = 2, timed = 4;
+    const int warm = 2;
     for (int occ = 0; occ < 2; ++occ)
         for (int order = 0; order < 2; ++order) {
             destroy_graphs(h);  // the step graphs hold the kernel and its arguments
             h->occ = occ;
             h->order = order;
-            if ((rc = dgsw_rkdg_init_state(h)) || (rc = dgsw_rkdg_step(h, warm)) || (rc = dgsw_rkdg_step(h, timed))) {
+            if ((rc = dgsw_rkdg_init_state(h)) || (rc = dgsw_rkdg_step(h, warm))) {
                 dgsw_rkdg_destroy(h);
                 return rc;
             }
+            // about 2 ms of timed steps (at least 4): on small meshes a few steps are launch-latency noise.
+            // A batch of 8 or more replays 8-step graphs, captured here before the timed batch.
             double ms = 0;
             int64_t nl = 0;
+            dgsw_rkdg_last_step_timing(h, &ms, &nl);
+            const double est = ms / warm;
+            const int timed = est > 0.0 ? std::max(4, std::min(256, (int)std::ceil(2.0 / est))) : 4;
+            if ((timed >= 8 && (rc = dgsw_rkdg_step(h, 8))) || (rc = dgsw_rkdg_step(h, timed))) {
+                dgsw_rkdg_destroy(h);
+                return rc;
+            }
             dgsw_rkdg_last_step_timing(h, &ms, &nl);
             rec.push_back({tile, occ, order, ms / timed, 0});
         }
