@@ -1675,8 +1675,10 @@ cudaError_t launch_stage_impl(const StageArgs<Real>& A, int ntiles, int max_halo
     const bool capped = allow_capped && max_halo <= TileCap<TILE>::halo && max_edges <= TileCap<TILE>::edges;
     auto kern = capped ? rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, true, OCC, SPLIT>
                        : rkdg_stage_kernel<P, Real, WD, FSRC, FRIC, TILE, false, OCC, SPLIT>;
+    // the run-time-stride kernel loads its halo faces' elements straight from global memory and never
+    // touches the halo staging area (every use of it is under CAPPED), so its allocation ends there
     const size_t smem = capped ? Smem<P, Real, WD>::bytes(TILE, TileCap<TILE>::halo, TileCap<TILE>::edges)
-                               : Smem<P, Real, WD>::bytes(TILE, max_halo, max_edges);
+                               : Smem<P, Real, WD>::off_halo(TILE, max_halo, max_edges);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)ntiles, TILE, smem, s>>>(A, max_halo, max_edges);
