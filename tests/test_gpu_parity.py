@@ -119,6 +119,20 @@ def test_register_budget_and_tile_order_do_not_change_results(precision):
             assert np.abs(q1 - q0).max() <= 1e-15 * np.abs(q0).max()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_autotuned_shared_memory_choice_does_not_change_results(precision):
+    """The autotuner also chooses between the stage kernel with compile-time shared-memory capacities and the
+    one sized to the mesh's largest tile (dgsw_info.smem_capped). Both do the same arithmetic in the same
+    order: an autotuned handle gives the same bits as a handle built with its tile, budget and order, which
+    takes the capped kernel wherever the mesh fits the caps."""
+    mesh, cfg = configs.manufactured(128, p=2, rk=(3, 3), dt=1.0, jitter=0.2, precision=precision)
+    A = Problem(cfg, mesh, tile=-1)
+    B = Problem(cfg, mesh, tile=A.info.tile, occupancy=A.info.occupancy, tile_order=A.info.tile_order)
+    A.step_serial(12)
+    B.step_serial(12)
+    assert np.array_equal(A.get_state(), B.get_state())
+
+
 def test_renumbering_does_not_change_results(oracle):
     mesh, cfg = configs.manufactured(12, p=2, rk=(2, 2), dt=5.0, jitter=0.15)
     A = Problem(cfg, mesh, renumber=True)
